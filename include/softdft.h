@@ -1,0 +1,161 @@
+/*
+ * softdft.h -- C ABI of the B200 iDFT self-consistent solve.
+ *
+ * The library replaces the bodies of the reference's inhomogeneous solve loop:
+ *   solver_dft(dft_system)                 src/iDFT/evaluation/objective/solver_dft.jl:5-25
+ *   solver_function(::AndersonMixing, ...) src/NonlinearSolvers/fixed_point/AndersonMixing.jl:56-169
+ *   objective_dft(problem_data)            src/iDFT/evaluation/objective/objective_dft.jl:6-30
+ *   grand_potential(dft_system)            src/iDFT/evaluation/analysis/grand_potential.jl:4-28
+ *   get_num_species(...)                   src/iDFT/evaluation/analysis/num_species.jl:1-38
+ * Setup (input.yaml, molecular system, bulk iLST state, geometry) stays on the
+ * host; the host fills a sdft_system_desc and the library builds every grid
+ * field, k-space weight and FFT plan on the device.
+ *
+ * Conventions
+ *  - Plain C types only.  Input pointers are borrowed for the duration of the
+ *    call; the library copies what it needs.  Output pointers are caller-owned
+ *    host memory.
+ *  - Grid arrays use the reference's column-major layout with the grid index
+ *    fastest:  mu_ex_K[K + NP*j]          (NP, NB)
+ *              lng_K[K + NP*(e + 2*b)]    (NP, 2, MB)   e = bond end 0/1
+ *              Psi[K]                     (NP)
+ *              rho_segments_u[K + NP*(s + S_u*g)]  (NP, S_u, N_u)
+ *  - Indices (bead types, bonds, segments, grid points) are 0-based.
+ *  - Every function returns an sdft_status; sdft_last_error() gives the text of
+ *    the most recent failure on the calling thread.  SDFT_MAX_ITERS is returned
+ *    by the solve when max_iters is reached; it is not an error (the reference
+ *    returns normally in that case) and the state is valid.
+ *  - Handles are independent; each owns one CUDA stream.  A handle must not be
+ *    used from two threads at once.
+ */
+#ifndef SOFTDFT_H
+#define SOFTDFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDFT_ABI_VERSION 1
+
+typedef enum sdft_status {
+  SDFT_OK = 0,
+  SDFT_MAX_ITERS = 1,        /* solve stopped at max_iters (state valid) */
+  SDFT_ERR_ARG = 2,          /* invalid descriptor or argument */
+  SDFT_ERR_UNSUPPORTED = 3,  /* feature outside the device solve */
+  SDFT_ERR_CUDA = 4,         /* CUDA runtime error or no device */
+  SDFT_ERR_OOM = 5,          /* device memory exhausted / admission refused */
+  SDFT_ERR_NORM = 6,         /* chain normalisation lambda <= 0 or not finite */
+  SDFT_ERR_NONFINITE = 7,    /* NaN/Inf in the fixed-point residual */
+  SDFT_ERR_TIMEOUT = 8       /* a bounded device wait gave up */
+} sdft_status;
+
+/* functional set (bitmask): the `model:` list of input.yaml minus `ideal`;
+ * registry src/iDFT/functionals/Abstract_Types/functional_registry.jl:53-70 */
+#define SDFT_FUNC_MFMT      0x1u   /* White-Bear FMT                 functionals/excluded_volume/mfmt.jl */
+#define SDFT_FUNC_TPT1MFMT  0x2u   /* White-Bear FMT + TPT1 bonding  functionals/excluded_volume/TPT1mfmt.jl */
+#define SDFT_FUNC_MSA       0x4u   /* MSA electrostatic correlations functionals/electrostaticcorrelations/msa.jl */
+#define SDFT_FUNC_TPT1MSA   0x8u   /* MSA + TPT1 bonding             functionals/electrostaticcorrelations/TPT1msa.jl */
+
+/* arithmetic of the solve */
+#define SDFT_PREC_FP64   0   /* every stage in FP64 (the plain form) */
+#define SDFT_PREC_MIXED  1   /* FP32 convolutions/propagators; FP64 Anderson,
+                                state sums, functional pointwise terms, residual */
+
+/* One species (configuration): src/molecular_system/structures/ConfigurationStruct.jl:41-47
+ * plus its fixed (grafted) segments, src/iDFT/structures/FixedSpecies.jl:20-39. */
+typedef struct sdft_species_desc {
+  int32_t n_seg;                 /* segments N_u */
+  int32_t max_states;            /* S_u = max over segments of the state count */
+  const int32_t* parent;         /* [n_seg] parent segment, -1 for the root (segment 0) */
+  const int32_t* n_states;       /* [n_seg] states of each segment */
+  const int32_t* states;         /* [n_seg*max_states] bead type of (segment, state slot) */
+  const int32_t* fixed_coord;    /* [n_seg] 0-based grid index of a fixed segment, -1 if free; may be NULL */
+  double fixed_density;          /* grafting density (chains per unit area) */
+  const double* max_distance;    /* [n_seg*n_seg] row-major path-length matrix; may be NULL without fixed segments */
+  double mu_species;             /* bulk chemical potential of the species */
+} sdft_species_desc;
+
+/* One inhomogeneous system (request). */
+typedef struct sdft_system_desc {
+  int32_t abi_version;           /* SDFT_ABI_VERSION */
+  int32_t np;                    /* grid points NP = cld(H, dz) + 1 */
+  double bin_width;              /* dz */
+  double length;                 /* slit width H (wall positions 0 and H) */
+  int32_t hard_walls;            /* nonzero: hard walls at 0 and H */
+  int32_t charged_walls;         /* nonzero: surface charges at 0 and H */
+  double wall_charge[2];         /* (qL, qR), e per area */
+  double bjerrum_length;         /* in units of the length scale */
+  int32_t nb;                    /* bead types */
+  const double* diameter;        /* [nb] */
+  const double* valence;         /* [nb] */
+  const double* delta_muH;       /* [nb] */
+  int32_t mb;                    /* bond types */
+  const int32_t* bond_types;     /* [mb*2] (min, max) bead-type pairs */
+  int32_t n_species;
+  const sdft_species_desc* species;
+  uint32_t functionals;          /* SDFT_FUNC_* */
+  const double* mu_ex_bulk;      /* [nb] bulk excess chemical potential (initial guess) */
+  const double* lng_bulk;        /* [mb] bulk ln g (initial guess) */
+} sdft_system_desc;
+
+/* Anderson controls: numerical section of input.yaml,
+ * src/NonlinearSolvers/fixed_point/AndersonMixing.jl:74-79 */
+typedef struct sdft_numerics {
+  int32_t max_iters;             /* default 100000 */
+  int32_t anderm;                /* history depth m, default 5 */
+  double damping;                /* default 0.5 */
+  double mixing_max;             /* default 1.0 */
+  double switch_tole;            /* default 1e-3 */
+  double tole;                   /* default 1e-6 */
+} sdft_numerics;
+
+typedef struct sdft_request* sdft_handle;
+
+/* Library / device */
+int32_t sdft_abi_version(void);
+const char* sdft_last_error(void);
+int sdft_device_count(int32_t* count);
+void sdft_numerics_default(sdft_numerics* out);
+
+/* Request lifecycle.  Builds Ext, trapez, k-space weights, the surface charge
+ * spectrum and the initial guess of process_guess
+ * (src/iDFT/setup/setup_steps/process_guess.jl:5-54) on the device. */
+int sdft_request_create(const sdft_system_desc* desc, int32_t precision, sdft_handle* out);
+int sdft_request_destroy(sdft_handle h);
+/* sizes: n = NP*(NB + 2*MB + 1) + 1 (Anderson vector length) */
+int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* device_bytes);
+
+/* Unknowns x = (mu_ex_K, lng_K, Psi, PsiC), solver_dft.jl:13 */
+int sdft_set_state(sdft_handle h, const double* mu_ex_K, const double* lng_K,
+                   const double* Psi, const double* PsiC);
+int sdft_get_state(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC);
+
+/* One fixed-point map evaluation G(x) (objective_dft), without changing x.
+ * Any output pointer may be NULL. */
+int sdft_objective(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC);
+
+/* Anderson-mixing solve from the current state; x is updated in place. */
+int sdft_solve(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err);
+
+/* Densities of the last G(x) evaluation.  rho_segments: array of n_species host
+ * pointers (entries may be NULL).  Any argument may be NULL. */
+int sdft_get_densities(sdft_handle h, double* const* rho_segments, double* rho_beads_K,
+                       double* rho_bonds_K);
+
+/* Grand potential (grand_potential.jl:4-28) from the current x and the densities
+ * of the last evaluation; chains per species (num_species.jl:1-38). */
+int sdft_grand_potential(sdft_handle h, double* omega);
+int sdft_num_species(sdft_handle h, double* num_species);
+
+/* Batched solve: every request of the batch runs in one launch (one persistent
+ * CTA per request).  status[i] receives the per-request sdft_status. */
+int sdft_solve_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num,
+                     int32_t* iters, double* errs, int32_t* status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOFTDFT_H */
