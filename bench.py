@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark: converged iDFT solves/s (max-norm fixed-point residual < 1e-8).
+
+One step = solving one batch of B independent requests to convergence in one
+device launch sequence (one persistent CTA per request).  The default
+workload is the plain slit request (NP=1024, dz=0.02, N=20 weak-polyacid
+chain pKa 4.5 at pH 7, 1:1 salt 0.1 M, hard-sphere solvent, packing 0.3, hard
+walls, Anderson m=5) in FP64; B defaults to two requests per SM.
+
+  value      device-timed solves/s over all ranks (CUDA events on the launch
+             stream, inputs resident, max time over ranks)
+  e2e        the same through the C ABI with host buffers: per step the
+             initial state of every request is copied host->device and the
+             bead densities device->host
+  roofline   algorithmic HBM bytes (softdft_b200/roofline.py) / device time
+             of the solve kernel vs the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (FP64 restatement of the reference; the Julia
+             reference cannot run on this machine) solving the same request
+             on the host cores, one solve per thread
+
+--impl reference runs only the CPU oracle (rank 0) on the same workload.
+Multi-GPU (torchrun): every rank solves its own batch (replicas, no exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import copy
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "converged iDFT solves/s at residual 1e-8, batched vs plain FP64; p50/p99 ms"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=0, help="requests per GPU (0: two per SM)")
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per request-iteration of the solve kernel from the committed
+    ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "sdft_k_solve_traffic.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh)
+    return None
+
+
+def workload():
+    from softdft_b200 import workloads
+    return "plain_slit", workloads.plain_slit()
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def all_max(v: float, ws: int) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(dft, num, threads: int):
+    """Oracle solves of the request on `threads` host threads, one solve each."""
+    from oracle.oracle import OracleSystem, max_threads, solve_many
+    if threads <= 0:
+        threads = min(max_threads(), 32)
+    systems = [OracleSystem(dft.descriptor) for _ in range(threads)]
+    t = time.perf_counter()
+    iters, errs, status = solve_many(systems, num, threads)
+    dt = time.perf_counter() - t
+    ok = int((status == 0).sum())
+    return {"value": ok / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{threads} full FP64 oracle solves of the request in parallel ({dt:.1f} s, "
+                      f"iterations {int(iters.min())}-{int(iters.max())}, {ok} converged)"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from softdft_b200.api import setup_request
+    from softdft_b200.host.descriptor import numerics_from_dict
+    name, ds = workload()
+    dft = setup_request(copy.deepcopy(ds))
+    num = numerics_from_dict(ds["numerical"])
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(dft, num, args.cpu_threads)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median([r["value"] for r in vals])
+    base = dict(vals[-1])
+    base["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * base["cores"] / v if v else None,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": name, "np": dft.NP, "n_chain": dft.descriptor.n_seg[0],
+                      "reference": "CPU oracle (FP64 restatement; Julia reference unavailable on this box)"},
+           "cpu_baseline": base,
+           "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+
+    from softdft_b200 import native
+    from softdft_b200.api import setup_request
+    from softdft_b200.host.descriptor import numerics_from_dict
+    from softdft_b200.roofline import algorithmic_bytes_per_iteration
+
+    if ws > 1:
+        import torch
+        torch.cuda.set_device(local)
+    name, ds = workload()
+    dft = setup_request(copy.deepcopy(ds))
+    num = numerics_from_dict(ds["numerical"])
+    import torch
+    sms = torch.cuda.get_device_properties(local if ws > 1 else 0).multi_processor_count
+    B = args.batch if args.batch > 0 else 2 * sms
+    systems = [native.DeviceSystem(dft.descriptor) for _ in range(B)]
+    x0 = systems[0].get_x()
+    n = x0.size
+    P, NB = dft.NP, dft.descriptor.nb
+
+    def reset():
+        for s in systems:
+            s.set_x(x0)
+
+    # plain FP64 form: one request per launch
+    plain = native.DeviceSystem(dft.descriptor)
+    plain.solve(num)  # warm-up
+    plain.set_x(x0)
+    plain_it, _, _ = plain.solve(num)
+    plain_ms, _, _ = native.last_batch_stats(1)
+    for _ in range(args.warmup):
+        reset()
+        native.solve_batch(systems, num)
+    barrier(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    dev_ms = []
+    launches = 0
+    iters_all, lat_all = [], []
+    for _ in range(args.steps):
+        reset()
+        barrier(ws)
+        iters, errs, status = native.solve_batch(systems, num)
+        ms, nl, lat = native.last_batch_stats(B)
+        dev_ms.append(ms)
+        launches += nl
+        iters_all.append(iters.copy())
+        lat_all.extend(lat.tolist())
+        if not np.all(status == 0):
+            raise RuntimeError(f"solve status {np.unique(status)}")
+    clk = clocks.stop()
+    total_s = all_max(sum(dev_ms) / 1000.0, ws)
+    value = ws * B * args.steps / total_s
+    # end to end: host buffers through the C ABI, copies inside the timed region
+    dens = np.zeros(P * NB)
+    e2e_t = []
+    for _ in range(args.steps):
+        barrier(ws)
+        t = time.perf_counter()
+        for s in systems:
+            s.set_x(x0)
+        native.solve_batch(systems, num)
+        for s in systems:
+            native.lib().sdft_get_densities(s.h, None, native._p(dens), None)
+        e2e_t.append(time.perf_counter() - t)
+    e2e_s = all_max(sum(e2e_t), ws)
+    e2e_value = ws * B * args.steps / e2e_s
+    # roofline of the solve kernel
+    bpi = algorithmic_bytes_per_iteration(dft.descriptor, num.anderm, 8)
+    it_sum = float(np.sum(iters_all))
+    alg_bytes = bpi * it_sum
+    achieved = alg_bytes / (sum(dev_ms) / 1000.0) / 1e9
+    peak, peak_kind = measured_peaks()
+    prof = profile_traffic()
+    traffic = None
+    if prof and prof.get("workload") == name:
+        traffic = prof["dram_bytes_per_request_iteration"] * it_sum / max(launches, 1)
+    lat = np.asarray(lat_all)
+    out = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(dev_ms), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": name, "np": P, "n_chain": dft.descriptor.n_seg[0], "batch_per_gpu": B,
+                   "anderm": num.anderm, "tole": num.tole, "parallelism": f"replicas x{ws}",
+                   "l2": f"inputs larger than L2 ({B} requests x {plain.device_bytes/1e6:.1f} MB device state)"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "iterations": {"min": int(np.min(iters_all)), "max": int(np.max(iters_all)),
+                       "mean": float(np.mean(iters_all))},
+        "plain_fp64": {"value": 1000.0 / plain_ms, "unit": "solves/s", "ms_per_solve": plain_ms,
+                       "iterations": plain_it, "form": "one request per launch"},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": B * n * 8,
+                "d2h_bytes_per_step": B * P * NB * 8},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "kernel": "sdft_k_solve", "alg_bytes_per_request_iteration": bpi},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(dft, num, args.cpu_threads)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    for s in systems:
+        s.close()
+    plain.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

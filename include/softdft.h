@@ -155,6 +155,13 @@ int sdft_num_species(sdft_handle h, double* num_species);
 int sdft_solve_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num,
                      int32_t* iters, double* errs, int32_t* status);
 
+/* Device statistics of the calling thread's most recent sdft_solve /
+ * sdft_solve_batch: CUDA-event time of its kernel launches on the launch
+ * stream (ms), number of kernel launches, and per request the device time
+ * from its first to its last iteration (%globaltimer, ms; n entries).
+ * No reference counterpart: measurement support for the batched solve. */
+int sdft_last_batch_stats(double* device_ms, int32_t* launches, double* latency_ms, int32_t n);
+
 #ifdef __cplusplus
 }
 #endif

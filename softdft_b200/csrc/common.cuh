@@ -1,0 +1,168 @@
+// common.cuh -- device-side request layout shared by every stage of the solve.
+//
+// One request (one inhomogeneous system) is owned by one CTA for the whole
+// solve.  Grid arrays use the reference's column-major layout with the grid
+// index K fastest (src/iDFT/setup/setup_steps/process_fields.jl:20-59):
+//   x      = [ mu_ex_K (NB x NP) | lng_K (MB x 2 x NP) | Psi (NP) | PsiC ]
+//   lambda = (NB x NP), Ext/trapez = (NB x NP), rho_beads = (NB x NP),
+//   rho_bonds = (MB x 2 x NP), rho_seg_u = (n_seg x S x NP).
+// Every mirrored-grid convolution of the reference is carried in DCT-II
+// coefficient space ("C-space"): P real coefficients per field, see fft.cuh.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sdft {
+
+constexpr int kThreads = 256;        // CTA size of the solve kernels
+constexpr int kMaxStates = 4;        // per-segment state families the device supports
+constexpr int kMaxBeads = 32;        // bead types
+constexpr int kMaxBonds = 64;        // bond types
+constexpr int kMaxAnderson = 16;     // Anderson depth m
+constexpr double kPi = 3.14159265358979323846;
+
+// status codes written by the kernels (mirror sdft_status)
+enum : int {
+  ST_OK = 0,
+  ST_MAX_ITERS = 1,
+  ST_NORM = 6,
+  ST_NONFINITE = 7,
+  ST_RUNNING = 100,
+};
+
+struct DSpecies {
+  int n_seg;          // segments N_u
+  int S;              // state slots per segment
+  int fixed;          // grid index of the grafted segment 0, -1 if free
+  int pad0;
+  const int* states;  // [n_seg * S] bead type per (segment, slot), -1 padding
+  const int* nst;     // [n_seg] states per segment
+  const double* md;   // [n_seg] max path distance from segment g to segment 0 (fixed species)
+  double fixed_density;
+  double mu_species;  // bulk chemical potential (set to 0 for grafted species each evaluation)
+  double normative;   // prod_g (sum_states e^-dmuH)^(1/N)  (child_propagators.jl:41-50)
+  double norm_free;   // normative^(N-1): chain normalisation of a free species (handle_fixed.jl:105-108)
+  double lambda_fixed;
+  double* gC;         // [(g * S + i) * S + j] * P + K : parent g state i, child g+1 state j
+  double* gP;         // [(g * S + i) * S + j] * P + K : child g state i, parent g-1 state j
+  double* rho_seg;    // [(g * S + i) * P + K]
+};
+
+struct DReq {
+  // sizes
+  int NP, M, L;       // grid points P, FFT length M = P/2, log2(M)
+  int NB, MB, NS;
+  int funcs;          // SDFT_FUNC_* bits
+  int n_tau;          // unused (reserved)
+  double dz, lB, total_charge;
+  long long n;        // Anderson unknowns
+  // per-bead / per-bond constants
+  const double* sig;  // [NB]
+  const double* z;    // [NB]
+  const double* dmu;  // [NB]
+  const int* bonds;   // [MB * 2]
+  const DSpecies* sp; // [NS]
+  // fixed fields
+  const double* Ext;      // [NB * P]
+  const double* trapez;   // [NB * P]
+  const double* Csurf;    // [P] DCT-II of the mirrored surface charge
+  // C-space weights, k = 0..P-1 (index k of the reference's 2P-point FFT grid)
+  const double* Wbond;    // [MB * P] filtered bond kernel: w_b(k) * exp(-(k/kc)^4)
+  const double* Wfmt;     // [NB * 3 * P] delta shell, step, vector (odd) weights at R = sigma/2
+  const double* Wmsa;     // [NB * P]
+  const double* Wcoul;    // [P]
+  // FFT tables
+  const double2* tw;      // [M/2] e^{-2 pi i k / M}
+  const double2* twP;     // [M+1] e^{-2 pi i k / P}
+  const double2* twD;     // [M+1] e^{-i pi k / (2P)}
+  // state
+  double* x;              // [n] unknowns
+  double* g;              // [n] G(x) of the last evaluation
+  double* lambda;         // [NB * P]
+  double* rho_beads;      // [NB * P]
+  double* rho_bonds;      // [MB * 2 * P]
+  double* Cb;             // [NB * P]      DCT-II of rho_beads * trapez
+  double* Cbond;          // [MB * 2 * P]  DCT-II of rho_bonds * trapez(end bead)
+  double* Cmu;            // [NB * P]      accumulated mu_ex coefficients
+  double* Clng;           // [MB * 2 * P]  accumulated ln g coefficients
+  double* wa;             // [max(NB, 6) * P] scratch (weighted densities, derivatives)
+  double* wb;             // [MB * 2 * P]  scratch (bond weighted densities)
+  double* wc;             // [max(NB, 6 + MB) * P] scratch (derivative fields)
+  // Anderson
+  double* hx;             // [m * n] history of x
+  double* hg;             // [m * n] history of G(x) - x
+  double* lsq_u;          // [n] LSQR work vector
+  // results
+  int* status;            // [1]
+  int* iters;             // [1]
+  double* err;            // [1]
+  double* scal;           // [8] scalars: 0 PsiC shift, 1.. reserved
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 scl2(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// ---------------------------------------------------------------------------
+// CTA reductions (warp shuffles + one shared slot per warp)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// returns the CTA-wide sum to every thread; red must hold >= 32 doubles
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int i = 0; i < nw; i++) t += red[i];
+  return t;
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = red[0];
+  const int nw = blockDim.x >> 5;
+  for (int i = 1; i < nw; i++) t = fmax(t, red[i]);
+  return t;
+}
+
+// k sums at once (k <= 16): vals[k] in/out
+template <int KMAX>
+__device__ __forceinline__ void block_sum_vec(double* vals, int k, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  for (int q = 0; q < k; q++) vals[q] = warp_sum(vals[q]);
+  __syncthreads();
+  if (lane == 0)
+    for (int q = 0; q < k; q++) red[q * 32 + w] = vals[q];
+  __syncthreads();
+  for (int q = 0; q < k; q++) {
+    double t = 0.0;
+    for (int i = 0; i < nw; i++) t += red[q * 32 + i];
+    vals[q] = t;
+  }
+}
+
+}  // namespace sdft

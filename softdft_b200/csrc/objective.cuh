@@ -1,0 +1,826 @@
+// objective.cuh -- one evaluation of the fixed-point map G(x) by one CTA.
+//
+// Restates objective_dft (src/iDFT/evaluation/objective/objective_dft.jl:17-30):
+//   lambda       get_onebody_potential!      eval_spatial_density.jl:138-149
+//   chains       compute_child_propagators   freely_jointed/child_propagators.jl:1-162
+//                compute_parent_propagators  freely_jointed/parent_propagators.jl:1-142
+//                handle_fixed                freely_jointed/handle_fixed.jl:1-120
+//                accumulate_densities!       freely_jointed/accumulate_densities.jl:95-184
+//   beads        update_spatial_structures!  functions/update_spatial_structures.jl:1-34
+//   rho_hat      calc_rho_beads/bonds_hat!   fourier_transforms/calc_rho_hat.jl:17-97
+//   functionals  TPT1mfmt / mfmt            functionals/excluded_volume/{TPT1mfmt,mfmt}.jl
+//                TPT1msa / msa              functionals/electrostaticcorrelations/{TPT1msa,msa}.jl
+//   mu, lng      eval_mu_functionals         functions/eval_mu_functional.jl:1-52
+//   Psi, PsiC    solve_coulomb               coulomb/models/coulomb.jl:84-125, coulomb/neutrality_shift.jl
+// All convolutions run in DCT-II coefficient space (fft.cuh).  Linear chains
+// (parent of segment g is g-1) with an optional grafted segment 0.
+#pragma once
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace sdft {
+
+struct Shared {
+  double2* z;   // M complex
+  double* red;  // 512 doubles
+};
+
+__device__ __forceinline__ const double* xs_mu(const DReq& r, const double* x) { return x; }
+__device__ __forceinline__ const double* xs_lng(const DReq& r, const double* x) { return x + (size_t)r.NP * r.NB; }
+__device__ __forceinline__ const double* xs_psi(const DReq& r, const double* x) {
+  return x + (size_t)r.NP * (r.NB + 2 * r.MB);
+}
+__device__ __forceinline__ size_t off_psic(const DReq& r) { return (size_t)r.NP * (r.NB + 2 * r.MB + 1); }
+
+__device__ __forceinline__ int bond_of(const DReq& r, int a, int b) {
+  // bond table: sorted (min, max) pairs
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  for (int u = 0; u < r.MB; u++)
+    if (r.bonds[2 * u] == lo && r.bonds[2 * u + 1] == hi) return u;
+  return -1;
+}
+
+__device__ __forceinline__ double dist2_grid(int K, int c, double dz) {
+  double d = (double)(K - c) * dz;
+  return d * d;
+}
+
+// ---------------------------------------------------------------------------
+// lambda_K = mu_ex_K + (Psi + PsiC) z + Ext + dmuH
+// ---------------------------------------------------------------------------
+__device__ void stage_lambda(const DReq& r) {
+  const int P = r.NP;
+  const double* mu = xs_mu(r, r.x);
+  const double* psi = xs_psi(r, r.x);
+  const double psic = r.x[off_psic(r)];
+  for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) {
+    int j = idx / P, K = idx - j * P;
+    double p = psi[K] + psic;
+    r.lambda[idx] = mu[idx] + p * r.z[j] + r.Ext[idx] + r.dmu[j];
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// chain propagators
+// ---------------------------------------------------------------------------
+__device__ void chain_child(const DReq& r, const DSpecies& s, Shared sh) {
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  const double* lng = xs_lng(r, r.x);
+  const double inv_norm = 1.0 / s.normative;
+  for (int p = N - 2; p >= 0; p--) {
+    const int c = p + 1;
+    for (int ii = 0; ii < s.nst[p]; ii++) {
+      const int si = s.states[p * S + ii];
+      for (int jj = 0; jj < s.nst[c]; jj++) {
+        const int sj = s.states[c * S + jj];
+        const int bond = bond_of(r, si, sj);
+        const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+        double* out = s.gC + ((size_t)(p * S + ii) * S + jj) * P;
+        const double* lam_j = r.lambda + (size_t)sj * P;
+        const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
+        const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
+        const double* tr_j = r.trapez + (size_t)sj * P;
+        const double* gcc = (c < N - 1) ? s.gC + ((size_t)(c * S + jj) * S) * P : nullptr;
+        auto fchild = [&](int K) {
+          double f = exp(-lam_j[K] + lng_pj[K] / 2.0);
+          if (gcc) {
+            double t = 0.0;
+            for (int q = 0; q < S; q++) t += gcc[(size_t)q * P + K];
+            f *= t;
+          }
+          return f;
+        };
+        if (p == 0 && s.fixed >= 0) {
+          // parent grafted, child free: local sum within sigma_ij (child_propagators.jl:91-116)
+          const int Kp = s.fixed;
+          const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
+          const double Dij2 = Dij * Dij;
+          const double renorm = 2.0 * Dij;
+          const double el = exp(lng_pi[Kp] / 2.0);
+          double acc = 0.0;
+          for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+            double d2 = dist2_grid(K1, Kp, r.dz);
+            if (d2 <= Dij2) {
+              double t = fabs(fchild(K1)) * el * r.dz * tr_j[K1] / renorm;
+              if (fabs(d2 - Dij2) <= 1e-6) t /= 2.0;
+              acc += t / s.normative;
+            }
+          }
+          acc = block_sum(acc, sh.red);
+          for (int K = threadIdx.x; K < P; K += blockDim.x) out[K] = (K == Kp) ? acc : 0.0;
+        } else {
+          const double* wb = r.Wbond + (size_t)bond * P;
+          dct2_convolve(
+              sh.z, r, [&](int K) { return fchild(K) * tr_j[K]; }, [&](int q) { return wb[q]; },
+              [&](int K, double y) { out[K] = fabs(y) * exp(lng_pi[K] / 2.0) * inv_norm; });
+        }
+      }
+    }
+    if (s.fixed >= 0) {  // max-distance mask (child_propagators.jl:147-157)
+      const double md2 = s.md[p] * s.md[p];
+      __syncthreads();
+      for (int K = threadIdx.x; K < P; K += blockDim.x)
+        if (dist2_grid(K, s.fixed, r.dz) > md2)
+          for (int q = 0; q < S * S; q++) s.gC[((size_t)p * S * S + q) * P + K] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ void chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  const double* lng = xs_lng(r, r.x);
+  const double inv_norm = 1.0 / s.normative;
+  // root: base case gP[K, 1, idx_i, root] = 1 (only the graft point when fixed)
+  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    for (int ii = 0; ii < S; ii++)
+      for (int jj = 0; jj < S; jj++) {
+        double v = 0.0;
+        if (jj == 0 && ii < s.nst[0]) v = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
+        s.gP[((size_t)ii * S + jj) * P + K] = v;
+      }
+  }
+  __syncthreads();
+  for (int c = 1; c < N; c++) {
+    const int p = c - 1;
+    // base case then the parent loop overwrites slot jj < nst[p]
+    for (int K = threadIdx.x; K < P; K += blockDim.x)
+      for (int ii = 0; ii < S; ii++)
+        for (int jj = 0; jj < S; jj++)
+          s.gP[((size_t)(c * S + ii) * S + jj) * P + K] = (jj == 0 && ii < s.nst[c]) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int ii = 0; ii < s.nst[c]; ii++) {
+      const int si = s.states[c * S + ii];
+      for (int jj = 0; jj < s.nst[p]; jj++) {
+        const int sj = s.states[p * S + jj];
+        const int bond = bond_of(r, si, sj);
+        const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+        double* out = s.gP + ((size_t)(c * S + ii) * S + jj) * P;
+        const double* lam_j = r.lambda + (size_t)sj * P;
+        const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
+        const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
+        const double* tr_j = r.trapez + (size_t)sj * P;
+        const double* gpp = s.gP + ((size_t)(p * S + jj) * S) * P;
+        auto fparent = [&](int K) {
+          double t = 0.0;
+          for (int q = 0; q < S; q++) t += gpp[(size_t)q * P + K];
+          return exp(-lam_j[K] + lng_pj[K] / 2.0) * t;
+        };
+        if (p == 0 && s.fixed >= 0) {
+          // parent grafted (parent_propagators.jl:72-94)
+          const int Kp = s.fixed;
+          const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
+          const double Dij2 = Dij * Dij;
+          const double renorm = 2.0 * Dij;
+          const double f = fparent(Kp);
+          for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+            double d2 = dist2_grid(K1, Kp, r.dz);
+            if (d2 <= Dij2) {
+              double v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm / s.normative;
+              if (fabs(d2 - Dij2) <= 1e-6) v /= 2.0;
+              out[K1] = v;
+            }
+          }
+          __syncthreads();
+        } else {
+          const double* wb = r.Wbond + (size_t)bond * P;
+          dct2_convolve(
+              sh.z, r, [&](int K) { return fparent(K) * tr_j[K]; }, [&](int q) { return wb[q]; },
+              [&](int K, double y) { out[K] = fabs(y) * exp(lng_pi[K] / 2.0) * inv_norm; });
+        }
+      }
+    }
+    if (s.fixed >= 0) {
+      const double md2 = s.md[c] * s.md[c];
+      __syncthreads();
+      for (int K = threadIdx.x; K < P; K += blockDim.x)
+        if (dist2_grid(K, s.fixed, r.dz) > md2)
+          for (int q = 0; q < S * S; q++) s.gP[((size_t)c * S * S + q) * P + K] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+// handle_fixed (handle_fixed.jl:1-120): chain normalisation; false on lambda <= 0
+__device__ bool chain_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_out) {
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  double lam, norm;
+  if (s.fixed >= 0) {
+    norm = s.fixed_density;
+    s.mu_species = 0.0;
+    const int parent = 1;  // first free segment
+    double acc = 0.0;
+    for (int K = threadIdx.x; K < P; K += blockDim.x) {
+      for (int ii = 0; ii < s.nst[parent]; ii++) {
+        const int si = s.states[parent * S + ii];
+        double sp = 0.0;
+        for (int q = 0; q < S; q++) sp += s.gP[((size_t)(parent * S + ii) * S + q) * P + K];
+        double contr = exp(-r.lambda[(size_t)si * P + K]) * sp;
+        double temp;
+        if (parent < N - 1) {
+          temp = 0.0;
+          for (int jj = 0; jj < s.nst[parent + 1]; jj++) temp += s.gC[((size_t)(parent * S + ii) * S + jj) * P + K];
+        } else {
+          temp = (ii == 0) ? 1.0 : 0.0;  // leaf base case read as gC[K, :, idx_i, 1, parent]
+        }
+        acc += contr * temp * r.trapez[(size_t)si * P + K] * r.dz;
+      }
+    }
+    lam = block_sum(acc, sh.red);
+  } else {
+    lam = 1.0;
+    norm = s.norm_free;
+  }
+  if (!isfinite(lam) || lam <= 0.0) return false;
+  norm *= 1.0 / lam;
+  s.lambda_fixed = lam / s.norm_free;
+  *norm_out = norm;
+  return true;
+}
+
+// accumulate_densities! for one species: rho_seg and both bond ends
+__device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm) {
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  const double mu = s.mu_species;
+  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    for (int g = 0; g < N; g++) {
+      for (int ii = 0; ii < s.nst[g]; ii++) {
+        const int si = s.states[g * S + ii];
+        double sp;
+        if (N > 1) {
+          sp = 0.0;
+          for (int q = 0; q < S; q++) sp += s.gP[((size_t)(g * S + ii) * S + q) * P + K];
+        } else {
+          sp = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
+        }
+        const double contr = norm * exp(mu - r.lambda[(size_t)si * P + K]) * sp;
+        double temp;
+        if (g < N - 1) {
+          temp = 0.0;
+          for (int jj = 0; jj < s.nst[g + 1]; jj++) {
+            const int sj = s.states[(g + 1) * S + jj];
+            const int bond = bond_of(r, si, sj);
+            const double t2 = s.gC[((size_t)(g * S + ii) * S + jj) * P + K];
+            r.rho_bonds[(size_t)(bond * 2 + 0) * P + K] += contr * t2;
+            temp += t2;
+          }
+        } else {
+          temp = 1.0;
+        }
+        s.rho_seg[(size_t)(g * S + ii) * P + K] += contr * temp;
+      }
+    }
+    for (int c = 1; c < N; c++) {
+      for (int ii = 0; ii < s.nst[c]; ii++) {
+        const int si = s.states[c * S + ii];
+        double contr = norm * exp(mu - r.lambda[(size_t)si * P + K]);
+        if (c < N - 1) {
+          double t = 0.0;
+          for (int q = 0; q < S; q++) t += s.gC[((size_t)(c * S + ii) * S + q) * P + K];
+          contr *= t;
+        }
+        for (int jj = 0; jj < s.nst[c - 1]; jj++) {
+          const int sj = s.states[(c - 1) * S + jj];
+          const int bond = bond_of(r, si, sj);
+          r.rho_bonds[(size_t)(bond * 2 + 1) * P + K] += contr * s.gP[((size_t)(c * S + ii) * S + jj) * P + K];
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// eval_spatial_density! + update_spatial_structures!; false on a normalisation error
+__device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
+  const int P = r.NP;
+  for (int u = 0; u < r.NS; u++) {
+    const DSpecies& s = r.sp[u];
+    for (size_t q = threadIdx.x; q < (size_t)s.n_seg * s.S * P; q += blockDim.x) s.rho_seg[q] = 0.0;
+  }
+  for (size_t q = threadIdx.x; q < (size_t)r.MB * 2 * P; q += blockDim.x) r.rho_bonds[q] = 0.0;
+  __syncthreads();
+  for (int u = 0; u < r.NS; u++) {
+    DSpecies s = r.sp[u];
+    if (s.n_seg > 1) {
+      chain_child(r, s, sh);
+      chain_parent(r, s, sh);
+    }
+    double norm;
+    bool ok = chain_norm(r, s, sh, &norm);
+    if (!ok) {
+      *bad_species = u;
+      return false;
+    }
+    if (threadIdx.x == 0) {
+      DSpecies* w = const_cast<DSpecies*>(&r.sp[u]);
+      w->mu_species = s.mu_species;
+      w->lambda_fixed = s.lambda_fixed;
+    }
+    chain_accumulate(r, s, norm);
+  }
+  // update_spatial_structures!
+  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    for (int j = 0; j < r.NB; j++) r.rho_beads[(size_t)j * P + K] = 0.0;
+    for (int u = 0; u < r.NS; u++) {
+      const DSpecies& s = r.sp[u];
+      for (int g = 0; g < s.n_seg; g++)
+        for (int ii = 0; ii < s.nst[g]; ii++) {
+          const int st = s.states[g * s.S + ii];
+          const double v = s.rho_seg[(size_t)(g * s.S + ii) * P + K];
+          if (g == 0 && s.fixed >= 0) {
+            if (K == s.fixed) r.rho_beads[(size_t)st * P + K] += v / r.dz / r.trapez[(size_t)st * P + K];
+          } else {
+            r.rho_beads[(size_t)st * P + K] += v;
+          }
+        }
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// rho_hat (DCT-II of rho * trapez)
+// ---------------------------------------------------------------------------
+__device__ void stage_rho_hat(const DReq& r, Shared sh) {
+  const int P = r.NP;
+  for (int j = 0; j < r.NB; j++) {
+    const double* rho = r.rho_beads + (size_t)j * P;
+    const double* tr = r.trapez + (size_t)j * P;
+    double* C = r.Cb + (size_t)j * P;
+    dct2_forward(
+        sh.z, r, [&](int K) { return rho[K] * tr[K]; }, [&](int q, double c) { C[q] = c; });
+  }
+  for (int u = 0; u < r.MB; u++)
+    for (int e = 0; e < 2; e++) {
+      const int bead = r.bonds[2 * u + e];
+      const double* rho = r.rho_bonds + (size_t)(u * 2 + e) * P;
+      const double* tr = r.trapez + (size_t)bead * P;
+      double* C = r.Cbond + (size_t)(u * 2 + e) * P;
+      dct2_forward(
+          sh.z, r, [&](int K) { return rho[K] * tr[K]; }, [&](int q, double c) { C[q] = c; });
+    }
+}
+
+// ---------------------------------------------------------------------------
+// White-Bear FMT (+TPT1): point-wise derivative of iLST mfmt.jl:210-244 and
+// TPT1mfmt.jl:311-374 on the true grid
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mfmt_deriv_pt(double n0, double n1, double n2, double n3, double nV1, double nV2,
+                                              double* d) {
+  const double om = 1.0 - n3;
+  const double l1 = log(om);
+  const double i1 = 1.0 / om;
+  const double i3 = 1.0 / n3;
+  const double i36 = 1.0 / (36.0 * kPi);
+  const double dot12 = nV1 * nV2, dot22 = nV2 * nV2;
+  d[0] = -l1;
+  d[1] = n2 * i1;
+  d[2] = n1 * i1 + (n2 * n2 - dot22) * 3.0 * i36 * i3 * (l1 * i3 + i1 * i1);
+  d[3] = n0 * i1 + (n1 * n2 - dot12) * (i1 * i1) -
+         (l1 * (i3 * i3 * i3) * 2.0 * i36 + (i3 * i3) * i1 * i36 + (1.0 - 3.0 * n3) * (i3 * i3) * i36 * (i1 * i1 * i1)) *
+             (n2 * n2 * n2 - 3.0 * n2 * dot22);
+  d[4] = -nV2 * i1;
+  d[5] = -nV1 * i1 - (l1 * i3 + i1 * i1) * n2 * nV2 * i3 * 6.0 * i36;
+}
+
+__device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
+  const int P = r.NP, NB = r.NB, MB = r.MB;
+  double* n0 = r.wa;
+  double* n1 = r.wa + (size_t)1 * P;
+  double* n2 = r.wa + (size_t)2 * P;
+  double* n3 = r.wa + (size_t)3 * P;
+  double* nV1 = r.wa + (size_t)4 * P;
+  double* nV2 = r.wa + (size_t)5 * P;
+  for (int q = threadIdx.x; q < 4 * P; q += blockDim.x) r.wa[q] = 0.0;
+  __syncthreads();
+  // scalar weighted densities, |.| per bead type as in TPT1mfmt.jl:79-89
+  for (int j = 0; j < NB; j++) {
+    const double s = r.sig[j];
+    const double* C = r.Cb + (size_t)j * P;
+    const double* W1 = r.Wfmt + ((size_t)j * 3 + 0) * P;
+    const double* W2 = r.Wfmt + ((size_t)j * 3 + 1) * P;
+    dct2_inverse(
+        sh.z, r, [&](int q) { return C[q] * W1[q]; },
+        [&](int K, double y) {
+          double a = fabs(y);
+          n0[K] += a / (kPi * (s * s));
+          n1[K] += a / (2 * kPi * s);
+          n2[K] += a;
+        });
+    dct2_inverse(
+        sh.z, r, [&](int q) { return C[q] * W2[q]; }, [&](int K, double y) { n3[K] += fabs(y); });
+  }
+  // vector weighted densities: odd output of the odd weight; the bead sum is linear
+  for (int v = 0; v < 2; v++) {
+    double* out = v == 0 ? nV1 : nV2;
+    dct2_inverse(
+        sh.z, r,
+        [&](int q) {
+          if (q == 0) return 0.0;
+          const int k = P - q;
+          double t = 0.0;
+          for (int j = 0; j < NB; j++) {
+            double c = r.Cb[(size_t)j * P + k] * r.Wfmt[((size_t)j * 3 + 2) * P + k];
+            t += v == 0 ? c / (2 * kPi * r.sig[j]) : c;
+          }
+          return t;
+        },
+        [&](int K, double y) { out[K] = (K & 1) ? y : -y; });
+  }
+  // bond weighted densities (TPT1mfmt.jl:106-133)
+  if (tpt1) {
+    for (int u = 0; u < MB; u++)
+      for (int e = 0; e < 2; e++) {
+        const int i = r.bonds[2 * u + e];
+        const double* C = r.Cbond + (size_t)(u * 2 + e) * P;
+        const double* W1 = r.Wfmt + ((size_t)i * 3 + 0) * P;
+        const double si2 = r.sig[i] * r.sig[i];
+        double* out = r.wb + (size_t)(u * 2 + e) * P;
+        dct2_inverse(
+            sh.z, r, [&](int q) { return C[q] * W1[q] / si2 / kPi; }, [&](int K, double y) { out[K] = fabs(y); });
+      }
+  }
+  // point-wise derivative; fields D0..D5 and ln y_HS per bond
+  double* D = r.wc;
+  double* lny = r.wc + (size_t)6 * P;
+  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    double a0 = n0[K], a1 = n1[K], a2 = n2[K], a3 = n3[K], v1 = nV1[K], v2 = nV2[K];
+    if (a3 > 0.95) {
+      const double fac = 0.95 / a3;
+      a0 *= fac; a1 *= fac; a2 *= fac; a3 *= fac; v1 *= fac; v2 *= fac;
+    }
+    double d[6];
+    if (a3 > 1e-10) {
+      mfmt_deriv_pt(a0, a1, a2, a3, v1, v2, d);
+      if (tpt1) {
+        double Xi = 1.0 - (v2 * v2) / (a2 * a2);
+        if (Xi < 0.0) Xi = 0.0;
+        const double i1 = 1.0 / (1.0 - a3);
+        const double term2 = a2 * Xi / 4.0 * (i1 * i1);
+        const double term3 = (a2 * a2) * Xi / 72.0 * (i1 * i1 * i1);
+        for (int u = 0; u < MB; u++) {
+          const int bi = r.bonds[2 * u], bj = r.bonds[2 * u + 1];
+          const double sij = (r.sig[bi] + r.sig[bj]) / 2;
+          const double tau = r.sig[bi] * r.sig[bj] / sij;
+          const double y = i1 + term2 * tau + term3 * (tau * tau);
+          const double dl2 = (tau / 4.0 * (i1 * i1) + a2 * (tau * tau) * (i1 * i1 * i1) / 36.0) / y;
+          const double dl3 =
+              ((i1 * i1) + a2 * Xi / 2.0 * (i1 * i1 * i1) * tau + (a2 * a2) * Xi / 24.0 * ((i1 * i1) * (i1 * i1)) * (tau * tau)) / y;
+          const double rb = r.wb[(size_t)(u * 2) * P + K] + r.wb[(size_t)(u * 2 + 1) * P + K];
+          d[2] -= 0.5 * rb * dl2;
+          d[3] -= 0.5 * rb * dl3;
+          const double dlv = -v2 * (tau / (2.0 * a2) * (i1 * i1) + (tau * tau) / 36.0 * (i1 * i1 * i1)) / y;
+          d[5] -= 0.5 * rb * dlv;
+          lny[(size_t)u * P + K] = log(y);
+        }
+      }
+    } else {
+      for (int q = 0; q < 6; q++) d[q] = 0.0;
+      if (tpt1)
+        for (int u = 0; u < MB; u++) lny[(size_t)u * P + K] = 0.0;
+    }
+    for (int q = 0; q < 6; q++) D[(size_t)q * P + K] = d[q];
+  }
+  __syncthreads();
+  // forward transforms: even D0..D3, odd D4, D5 (DST-II through (-1)^K and reversal)
+  double* CD = r.wa;  // 6 coefficient arrays (weighted densities are dead now)
+  for (int q = 0; q < 6; q++) {
+    const double* src = D + (size_t)q * P;
+    double* dst = CD + (size_t)q * P;
+    if (q < 4) {
+      dct2_forward(
+          sh.z, r, [&](int K) { return src[K]; }, [&](int k, double c) { dst[k] = c; });
+    } else {
+      if (threadIdx.x == 0) dst[0] = 0.0;
+      dct2_forward(
+          sh.z, r, [&](int K) { return (K & 1) ? -src[K] : src[K]; },
+          [&](int k, double c) {
+            if (k > 0) dst[P - k] = c;
+          });
+    }
+  }
+  // mu_ex coefficients (accumulate_mu_ex!, TPT1mfmt.jl:244-283)
+  for (int idx = threadIdx.x; idx < NB * P; idx += blockDim.x) {
+    const int j = idx / P, k = idx - j * P;
+    const double s = r.sig[j];
+    const double W1 = r.Wfmt[((size_t)j * 3 + 0) * P + k];
+    const double W2 = r.Wfmt[((size_t)j * 3 + 1) * P + k];
+    const double W3 = r.Wfmt[((size_t)j * 3 + 2) * P + k];
+    const double c1 = CD[k] / (kPi * (s * s)) + CD[(size_t)P + k] / (2 * kPi * s) + CD[(size_t)2 * P + k];
+    const double c2 = CD[(size_t)3 * P + k];
+    const double c3 = CD[(size_t)4 * P + k] / (2 * kPi * s) + CD[(size_t)5 * P + k];
+    r.Cmu[idx] += c1 * W1 + c2 * W2 - c3 * W3;
+  }
+  __syncthreads();
+  // ln g coefficients (accumulate_lng!, TPT1mfmt.jl:286-313)
+  if (tpt1) {
+    for (int u = 0; u < MB; u++) {
+      const double* src = lny + (size_t)u * P;
+      const int ia = r.bonds[2 * u], ib = r.bonds[2 * u + 1];
+      const double* Wa = r.Wfmt + ((size_t)ia * 3) * P;
+      const double* Wb = r.Wfmt + ((size_t)ib * 3) * P;
+      const double sa = kPi * (r.sig[ia] * r.sig[ia]), sb = kPi * (r.sig[ib] * r.sig[ib]);
+      double* L0 = r.Clng + (size_t)(u * 2) * P;
+      double* L1 = r.Clng + (size_t)(u * 2 + 1) * P;
+      dct2_forward(
+          sh.z, r, [&](int K) { return src[K]; },
+          [&](int k, double c) {
+            L0[k] += c * (Wa[k] / sa);
+            L1[k] += c * (Wb[k] / sb);
+          });
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MSA (+TPT1): Gamma by the damped fixed point of iLST msa.jl:181-230
+// ---------------------------------------------------------------------------
+struct MsaGamma {
+  double G, eta, H;
+};
+
+__device__ __forceinline__ MsaGamma gamma_msa_pt(const double* rho, const double* sig, const double* Z, int nb,
+                                                 double lB) {
+  const double tol = 1e-10;
+  double s = 0.0;
+  for (int j = 0; j < nb; j++) s += rho[j] * Z[j] * Z[j];
+  const double kappa = sqrt(4.0 * kPi * lB * s);
+  MsaGamma out;
+  if (kappa < tol) {
+    out.G = kappa / 2.0;
+    out.eta = 0.0;
+    out.H = 2.0 / kPi;
+    return out;
+  }
+  double sr = 0.0, srs = 0.0, s3 = 0.0;
+  for (int j = 0; j < nb; j++) {
+    sr += rho[j] * sig[j];
+    srs += rho[j];
+    s3 += rho[j] * sig[j] * sig[j] * sig[j];
+  }
+  const double sig_eff = sr / srs;
+  const double xx = sig_eff * sqrt(4.0 * kPi * lB * s);
+  double G = (sqrt(1.0 + 2.0 * xx) - 1.0) / (2.0 * sig_eff);
+  const double term2 = 2.0 / kPi * (1.0 - kPi / 6.0 * s3);
+  double eta = 0.0, H = 0.0;
+  for (int it = 1;; it++) {
+    double hs = 0.0, es = 0.0;
+    for (int j = 0; j < nb; j++) {
+      hs += rho[j] * sig[j] * sig[j] * sig[j] / (1.0 + G * sig[j]);
+      es += rho[j] * Z[j] * sig[j] / (1.0 + G * sig[j]);
+    }
+    H = hs + term2;
+    eta = es / H;
+    double gs = 0.0;
+    for (int j = 0; j < nb; j++) {
+      const double a = Z[j] - eta * sig[j] * sig[j];
+      gs += rho[j] * a * a / (1.0 + G * sig[j]) / (1.0 + G * sig[j]);
+    }
+    const double G1 = sqrt(kPi * lB * gs);
+    const double Gn = 0.9 * G + 0.1 * G1;
+    if (fabs(G1 - G) < tol || it >= 1000) {
+      G = Gn;
+      break;
+    }
+    G = Gn;
+  }
+  out.G = G;
+  out.eta = eta;
+  out.H = H;
+  return out;
+}
+
+__device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
+  const int P = r.NP, NB = r.NB, MB = r.MB;
+  for (int j = 0; j < NB; j++) {
+    const double* C = r.Cb + (size_t)j * P;
+    const double* W = r.Wmsa + (size_t)j * P;
+    double* out = r.wa + (size_t)j * P;
+    dct2_inverse(
+        sh.z, r, [&](int q) { return C[q] * W[q]; }, [&](int K, double y) { out[K] = fabs(y); });
+  }
+  if (tpt1)
+    for (int u = 0; u < MB; u++)
+      for (int e = 0; e < 2; e++) {
+        const int i = r.bonds[2 * u + e];
+        const double* C = r.Cbond + (size_t)(u * 2 + e) * P;
+        const double* W = r.Wmsa + (size_t)i * P;
+        double* out = r.wb + (size_t)(u * 2 + e) * P;
+        dct2_inverse(
+            sh.z, r, [&](int q) { return C[q] * W[q]; }, [&](int K, double y) { out[K] = fabs(y); });
+      }
+  // point-wise derivative (TPT1msa.jl:129-156 -> iLST TPT1msa.jl:200-282)
+  const double* sig = r.sig;
+  const double* Z = r.z;
+  const double lB = r.lB;
+  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    double rho[kMaxBeads], dphi[kMaxBeads];
+    for (int j = 0; j < NB; j++) rho[j] = r.wa[(size_t)j * P + K];
+    const MsaGamma gm = gamma_msa_pt(rho, sig, Z, NB, lB);
+    const double G = gm.G, eta = gm.eta, H = gm.H;
+    double us = 0.0;
+    for (int j = 0; j < NB; j++)
+      us += rho[j] * sig[j] * sig[j] * ((Z[j] - eta * sig[j] * sig[j]) / (1.0 + G * sig[j]) + Z[j]);
+    us = -kPi / 6 * us;
+    for (int j = 0; j < NB; j++)
+      dphi[j] = -lB * (G * (Z[j] * Z[j]) / (1.0 + G * sig[j]) +
+                       eta * sig[j] * ((2.0 * Z[j] - eta * (sig[j] * sig[j])) / (1.0 + G * sig[j]) + eta * (sig[j] * sig[j]) / 3.0) +
+                       Z[j] * us);
+    if (tpt1) {
+      double* lngo = r.wc + (size_t)NB * P;
+      if (G == 0.0) {
+        for (int u = 0; u < MB; u++) {
+          const int i = r.bonds[2 * u], j = r.bonds[2 * u + 1];
+          lngo[(size_t)u * P + K] = -lB / ((sig[i] + sig[j]) / 2.0) * Z[i] * Z[j];
+        }
+      } else {
+        for (int u = 0; u < MB; u++) {
+          const int i = r.bonds[2 * u], j = r.bonds[2 * u + 1];
+          const double sij = (sig[i] + sig[j]) / 2.0;
+          const double Xi = (Z[i] - eta * (sig[i] * sig[i])) / (1.0 + G * sig[i]);
+          const double Xj = (Z[j] - eta * (sig[j] * sig[j])) / (1.0 + G * sig[j]);
+          lngo[(size_t)u * P + K] = -lB / sij * Xi * Xj;
+        }
+        double dfG = 0.0, dfe = 0.0, deG = 0.0, dHG = 0.0;
+        for (int w = 0; w < NB; w++) {
+          const double a = Z[w] - eta * sig[w] * sig[w];
+          const double og = 1.0 + G * sig[w];
+          dfG += rho[w] * sig[w] * a * a / og / og / og;
+          dfe += rho[w] * sig[w] * sig[w] * a / og / og;
+          deG += rho[w] * Z[w] * sig[w] * sig[w] / og / og;
+          dHG += rho[w] * sig[w] * sig[w] * sig[w] * sig[w] / og / og;
+        }
+        dfG = -2.0 * kPi * lB * dfG;
+        dfe = -2.0 * kPi * lB * dfe;
+        deG = -1.0 / H * deG;
+        const double deH = -eta / H;
+        dHG = -dHG;
+        const double detaG = deG + deH * dHG;
+        const double denom = 1.0 / (2.0 * G - dfe * detaG - dfG);
+        for (int w = 0; w < NB; w++) {
+          const double inv = 1.0 / (1.0 + G * sig[w]);
+          const double Xw = (Z[w] - eta * (sig[w] * sig[w])) * inv;
+          const double dfr = kPi * lB * (Xw * Xw);
+          const double der = sig[w] / H * Z[w] * inv;
+          const double dHr = (sig[w] * sig[w] * sig[w]) * (inv - 1.0 / 3.0);
+          const double dGr = (dfr + dfe * (der + dfe * deH * dHr)) * denom;
+          const double detar = detaG * dGr;
+          for (int u = 0; u < MB; u++) {
+            const int i = r.bonds[2 * u], j = r.bonds[2 * u + 1];
+            const double sij = (sig[i] + sig[j]) / 2.0;
+            const double ii = 1.0 / (1.0 + G * sig[i]);
+            const double Xi = (Z[i] - eta * (sig[i] * sig[i])) * ii;
+            const double dXi = -((sig[i] * sig[i]) * ii * detar + sig[i] * Xi * ii * dGr);
+            const double ij = 1.0 / (1.0 + G * sig[j]);
+            const double Xj = (Z[j] - eta * (sig[j] * sig[j])) * ij;
+            const double dXj = -((sig[j] * sig[j]) * ij * detar + sig[j] * Xj * ij * dGr);
+            const double rb = r.wb[(size_t)(u * 2) * P + K] + r.wb[(size_t)(u * 2 + 1) * P + K];
+            dphi[w] += rb / 2.0 * lB / sij * (dXi * Xj + Xi * dXj);
+          }
+        }
+      }
+    }
+    for (int j = 0; j < NB; j++) r.wc[(size_t)j * P + K] = dphi[j];
+  }
+  __syncthreads();
+  for (int j = 0; j < NB; j++) {
+    const double* src = r.wc + (size_t)j * P;
+    const double* W = r.Wmsa + (size_t)j * P;
+    double* Cm = r.Cmu + (size_t)j * P;
+    dct2_forward(
+        sh.z, r, [&](int K) { return src[K]; }, [&](int k, double c) { Cm[k] += c * W[k]; });
+  }
+  if (tpt1)
+    for (int u = 0; u < MB; u++) {
+      const double* src = r.wc + (size_t)(NB + u) * P;
+      const double* Wa = r.Wmsa + (size_t)r.bonds[2 * u] * P;
+      const double* Wb = r.Wmsa + (size_t)r.bonds[2 * u + 1] * P;
+      double* L0 = r.Clng + (size_t)(u * 2) * P;
+      double* L1 = r.Clng + (size_t)(u * 2 + 1) * P;
+      dct2_forward(
+          sh.z, r, [&](int K) { return src[K]; },
+          [&](int k, double c) {
+            L0[k] += c * Wa[k];
+            L1[k] += c * Wb[k];
+          });
+    }
+}
+
+// ---------------------------------------------------------------------------
+// neutrality shift (neutrality_shift.jl:1-99) -> PsiC increment
+// ---------------------------------------------------------------------------
+__device__ double stage_neutrality(const DReq& r, Shared sh) {
+  const int P = r.NP, NS = r.NS;
+  // per species: N_u and sum_seg N z (partial sums per thread, one vector reduction)
+  double part[2 * 16];
+  for (int u = 0; u < 2 * NS; u++) part[u] = 0.0;
+  for (int u = 0; u < NS; u++) {
+    const DSpecies& s = r.sp[u];
+    for (int g = 0; g < s.n_seg; g++)
+      for (int ii = 0; ii < s.nst[g]; ii++) {
+        const int st = s.states[g * s.S + ii];
+        const double* rs = s.rho_seg + (size_t)(g * s.S + ii) * P;
+        double nn = 0.0;
+        if (g == 0 && s.fixed >= 0) {
+          if (threadIdx.x == 0) nn = rs[s.fixed];
+        } else {
+          for (int K = threadIdx.x; K < P; K += blockDim.x) nn += rs[K] * r.trapez[(size_t)st * P + K] * r.dz;
+        }
+        part[2 * u] += nn;
+        part[2 * u + 1] += nn * r.z[st];
+      }
+  }
+  block_sum_vec<32>(part, 2 * NS, sh.red);
+  double psi1 = 0.0;
+  if (threadIdx.x == 0) {
+    double num[16], chg[16];
+    double Qtot = r.total_charge;
+    for (int u = 0; u < NS; u++) {
+      const DSpecies& s = r.sp[u];
+      num[u] = part[2 * u] / (double)s.n_seg;
+      chg[u] = num[u] <= 0.0 ? 0.0 : part[2 * u + 1] / num[u];
+      bool fam = false;
+      for (int g = 0; g < s.n_seg; g++) fam |= s.nst[g] > 1;
+      if (fam || s.fixed >= 0) {
+        Qtot += num[u] * chg[u];
+        chg[u] = 0.0;
+      }
+    }
+    double acc = 0.0;
+    for (int u = 0; u < NS; u++) acc += num[u] * chg[u];
+    double err = fabs(Qtot + acc);
+    double Cstar = exp(-psi1);
+    int iter = 1;
+    while (err > 1e-10) {
+      double fx = Qtot, fx1 = 0.0;
+      for (int i = 0; i < NS; i++) {
+        const double t = pow(Cstar, chg[i]) * num[i] * chg[i];
+        fx += t;
+        fx1 -= t * chg[i];
+      }
+      err = fabs(fx);
+      if (fabs(fx1) < 1e-10) break;
+      const double del = fmax(1.0, fabs(fx / fx1));
+      psi1 -= fx / (fx1 * del);
+      Cstar = exp(-psi1);
+      iter++;
+      if (iter > 1000) break;
+    }
+    sh.red[0] = psi1;
+  }
+  __syncthreads();
+  psi1 = sh.red[0];
+  __syncthreads();
+  return psi1;
+}
+
+// ---------------------------------------------------------------------------
+// full G(x): writes r.g; returns false on a normalisation error
+// ---------------------------------------------------------------------------
+__device__ bool objective(const DReq& r, Shared sh) {
+  const int P = r.NP;
+  stage_lambda(r);
+  int bad = -1;
+  if (!stage_densities(r, sh, &bad)) return false;
+  stage_rho_hat(r, sh);
+  for (size_t q = threadIdx.x; q < (size_t)r.NB * P; q += blockDim.x) r.Cmu[q] = 0.0;
+  for (size_t q = threadIdx.x; q < (size_t)r.MB * 2 * P; q += blockDim.x) r.Clng[q] = 0.0;
+  __syncthreads();
+  if (r.funcs & 0x1) stage_fmt(r, sh, false);
+  if (r.funcs & 0x2) stage_fmt(r, sh, true);
+  if (r.funcs & 0x4) stage_msa(r, sh, false);
+  if (r.funcs & 0x8) stage_msa(r, sh, true);
+  double* g = r.g;
+  for (int j = 0; j < r.NB; j++) {
+    const double* C = r.Cmu + (size_t)j * P;
+    double* out = g + (size_t)j * P;
+    dct2_inverse(
+        sh.z, r, [&](int q) { return C[q]; }, [&](int K, double y) { out[K] = y; });
+  }
+  double* gl = g + (size_t)P * r.NB;
+  for (int q = 0; q < 2 * r.MB; q++) {
+    const double* C = r.Clng + (size_t)q * P;
+    double* out = gl + (size_t)q * P;
+    dct2_inverse(
+        sh.z, r, [&](int k) { return C[k]; }, [&](int K, double y) { out[K] = y; });
+  }
+  // Poisson (solve_poisson_eq): (surf + sum_j z_j rho_hat_j) * w_coul
+  double* gpsi = g + (size_t)P * (r.NB + 2 * r.MB);
+  dct2_inverse(
+      sh.z, r,
+      [&](int k) {
+        double f = r.Csurf[k];
+        for (int j = 0; j < r.NB; j++) f += r.Cb[(size_t)j * P + k] * r.z[j];
+        return f * r.Wcoul[k];
+      },
+      [&](int K, double y) { gpsi[K] = y; });
+  const double shift = stage_neutrality(r, sh);
+  if (threadIdx.x == 0) g[off_psic(r)] = r.x[off_psic(r)] + shift;
+  __syncthreads();
+  return true;
+}
+
+}  // namespace sdft

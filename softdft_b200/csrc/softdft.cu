@@ -1,0 +1,800 @@
+// softdft.cu -- kernels and the C ABI of include/softdft.h.
+//
+// One CTA owns one request for a whole solve (k_solve): every stage of
+// objective_dft and the Anderson update run back to back in that CTA, with the
+// FFT workspace in shared memory and the request's fields in HBM/L2.  A batch
+// is one launch with one CTA per request; requests of different sizes share the
+// launch.  The host side builds the grid fields and k-space weights of
+// setup_iDFT (src/iDFT/setup/setup_iDFT.jl:9-30) from the plain-C descriptor.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/softdft.h"
+#include "anderson.cuh"
+#include "common.cuh"
+#include "objective.cuh"
+#include "omega.cuh"
+
+using namespace sdft;
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+constexpr int kRedDoubles = 1024;
+
+__device__ __forceinline__ Shared make_shared(double* smem) {
+  Shared sh;
+  sh.red = smem;
+  sh.z = reinterpret_cast<double2*>(smem + kRedDoubles);
+  return sh;
+}
+
+struct SolveSlot {       // per-request solver state kept across launches
+  int iter;
+  int status;
+  int use_picard;
+  int pad;
+  double err;
+  unsigned long long t0, t1;  // %globaltimer (ns) at the first and the last iteration
+  double lam[kMaxAnderson];
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_objective(const DReq* reqs) {
+  extern __shared__ double smem[];
+  const DReq& r = reqs[blockIdx.x];
+  Shared sh = make_shared(smem);
+  bool ok = objective(r, sh);
+  if (threadIdx.x == 0) *r.status = ok ? ST_OK : ST_NORM;
+}
+
+extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_solve(const DReq* reqs, SolveSlot* slots, SolveCfg cfg,
+                                                                    int max_chunk) {
+  extern __shared__ double smem[];
+  const DReq& r = reqs[blockIdx.x];
+  SolveSlot* sl = &slots[blockIdx.x];
+  Shared sh = make_shared(smem);
+  if (sl->status != ST_RUNNING) return;
+  if (threadIdx.x == 0 && sl->iter == 0) sl->t0 = global_ns();
+  AndersonState st;
+  st.use_picard = sl->use_picard;
+  for (int c = 0; c < kMaxAnderson; c++) st.lam[c] = sl->lam[c];
+  int iter = sl->iter;
+  int status = ST_RUNNING;
+  double err = sl->err;
+  for (int step = 0; step < max_chunk && iter < cfg.max_iters; step++) {
+    iter++;
+    if (!objective(r, sh)) {
+      status = ST_NORM;
+      break;
+    }
+    int s = anderson_step(r, cfg, iter, st, sh.red, &err);
+    if (s != ST_RUNNING) {
+      status = s;
+      break;
+    }
+  }
+  if (status == ST_RUNNING && iter >= cfg.max_iters) status = ST_MAX_ITERS;
+  if (threadIdx.x == 0) {
+    sl->iter = iter;
+    sl->status = status;
+    sl->use_picard = st.use_picard;
+    sl->err = err;
+    sl->t1 = global_ns();
+    for (int c = 0; c < kMaxAnderson; c++) sl->lam[c] = st.lam[c];
+    *r.status = status;
+    *r.iters = iter;
+    *r.err = err;
+  }
+}
+
+extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_omega(const DReq* reqs, double* out) {
+  extern __shared__ double smem[];
+  const DReq& r = reqs[blockIdx.x];
+  Shared sh = make_shared(smem);
+  grand_potential(r, sh, out);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static thread_local double g_batch_ms = 0.0;
+static thread_local int g_batch_launches = 0;
+static thread_local std::vector<double> g_batch_latency;
+
+static int set_err(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                 \
+  do {                                                                                 \
+    cudaError_t e_ = (expr);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return set_err(SDFT_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct SpeciesHost {
+  int n_seg, S, fixed;
+  std::vector<int> states, nst;
+  std::vector<double> md;
+  double fixed_density, mu_species, normative, norm_free;
+};
+
+struct sdft_request {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int precision = SDFT_PREC_FP64;
+  int NP = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
+  long long n = 0;
+  std::vector<SpeciesHost> sp;
+  char* dmem = nullptr;
+  size_t bytes = 0;
+  DReq h{};            // host copy of the device descriptor
+  DReq* dreq = nullptr;
+  SolveSlot* dslot = nullptr;
+  double* dout = nullptr;  // omega + num species
+  int anderm_alloc = 0;
+  size_t hist_off = 0;
+};
+
+extern "C" int32_t sdft_abi_version(void) { return SDFT_ABI_VERSION; }
+extern "C" const char* sdft_last_error(void) { return g_err.c_str(); }
+
+extern "C" int sdft_device_count(int32_t* count) {
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    *count = 0;
+    return set_err(SDFT_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  }
+  *count = c;
+  return SDFT_OK;
+}
+
+extern "C" void sdft_numerics_default(sdft_numerics* o) {
+  o->max_iters = 100000;
+  o->anderm = 5;
+  o->damping = 0.5;
+  o->mixing_max = 1.0;
+  o->switch_tole = 1e-3;
+  o->tole = 1e-6;
+}
+
+namespace {
+
+double kvec(int k, int N, double DR) {
+  if (k <= N / 2) return 2.0 * kPi * (double)k / ((double)N * DR);
+  return -2.0 * kPi * (double)(N - k) / ((double)N * DR);
+}
+double w_delta(int k, int N, double DR, double b) {  // delta_func.jl
+  if (k == 0) return 4.0 * kPi * (b * b);
+  double kv = kvec(k, N, DR), d = std::sqrt(kv * kv);
+  return 4.0 * kPi * b * std::sin(b * d) / d;
+}
+double w_step(int k, int N, double DR, double b) {  // step_func.jl
+  if (k == 0) return (4.0 / 3.0) * kPi * (b * b * b);
+  double kv = kvec(k, N, DR), d = std::sqrt(kv * kv);
+  return 4.0 * kPi * (std::sin(b * d) - b * d * std::cos(b * d)) / (d * d * d);
+}
+double w_vec(int k, int N, double DR, double b) {  // vectored_delta_func.jl
+  if (k == 0) return 0.0;
+  double kv = kvec(k, N, DR), d = std::sqrt(kv * kv);
+  return -4.0 * kPi * (std::sin(b * d) - b * d * std::cos(b * d)) / (d * d * d) * kv;
+}
+double w_coul(int k, int N, double DR, double BJ) {  // coul_func_fft.jl
+  if (k == 0) return 0.0;
+  double kv = kvec(k, N, DR);
+  return 2.0 * kPi * BJ / ((1.0 - std::cos(kv * DR)) / (DR * DR));
+}
+double filter_k(int k, int N, double dz) {  // apply_filter.jl
+  double kc = 0.5 * (kPi / dz);
+  int nn = k > N / 2 ? k - N : k;
+  double kd = 2.0 * kPi * (double)nn / ((double)N * dz);
+  double t = std::sqrt(kd * kd) / kc;
+  double t2 = t * t;
+  return std::exp(-(t2 * t2));
+}
+double2 cis(long double a) { return make_double2((double)cosl(a), (double)sinl(a)); }
+int jround(double x) { return (int)std::nearbyint(x); }
+
+struct Layout {
+  size_t off = 0;
+  template <class T>
+  size_t take(size_t count) {
+    size_t o = (off + 255) & ~(size_t)255;
+    off = o + count * sizeof(T);
+    return o;
+  }
+};
+
+int bond_lookup(const std::vector<int>& bonds, int a, int b) {
+  int lo = std::min(a, b), hi = std::max(a, b);
+  for (size_t u = 0; u < bonds.size() / 2; u++)
+    if (bonds[2 * u] == lo && bonds[2 * u + 1] == hi) return (int)u;
+  return -1;
+}
+
+}  // namespace
+
+extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
+  if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
+  if (precision != SDFT_PREC_FP64)
+    return set_err(SDFT_ERR_UNSUPPORTED, "only the FP64 precision is available in this build");
+  const int P = d->np;
+  if (P < 16 || (P & (P - 1)) != 0)
+    return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP = 2^k >= 16 (got " + std::to_string(P) + ")");
+  if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
+  if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
+  if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
+  if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
+  if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(SDFT_ERR_CUDA, "no CUDA device");
+  auto* q = new sdft_request();
+  cudaGetDevice(&q->device);
+  q->precision = precision;
+  q->NP = P;
+  q->M = P / 2;
+  q->L = 0;
+  while ((1 << q->L) < q->M) q->L++;
+  q->NB = d->nb;
+  q->MB = d->mb;
+  q->NS = d->n_species;
+  const int NB = q->NB, MB = q->MB, NS = q->NS, M = q->M;
+  const int NPS = 2 * P;
+  q->n = (long long)P * (NB + 2 * MB + 1) + 1;
+  std::vector<int> bonds(d->bond_types, d->bond_types + 2 * MB);
+  // species
+  size_t gC_elems = 0, rho_elems = 0;
+  for (int u = 0; u < NS; u++) {
+    const sdft_species_desc& s = d->species[u];
+    SpeciesHost h;
+    h.n_seg = s.n_seg;
+    h.S = s.max_states;
+    if (h.n_seg < 1 || h.S < 1 || h.S > kMaxStates) {
+      delete q;
+      return set_err(SDFT_ERR_UNSUPPORTED, "segments >= 1 and 1 <= states <= 4 per segment are required");
+    }
+    for (int g = 0; g < h.n_seg; g++) {
+      if (s.parent[g] != g - 1) {
+        delete q;
+        return set_err(SDFT_ERR_UNSUPPORTED, "the device solve supports linear chains (parent of segment g is g-1)");
+      }
+      if (s.n_states[g] < 1 || s.n_states[g] > h.S) {
+        delete q;
+        return set_err(SDFT_ERR_ARG, "n_states out of range");
+      }
+    }
+    h.nst.assign(s.n_states, s.n_states + h.n_seg);
+    h.states.assign(s.states, s.states + (size_t)h.n_seg * h.S);
+    h.fixed = -1;
+    if (s.fixed_coord) {
+      for (int g = 0; g < h.n_seg; g++) {
+        if (s.fixed_coord[g] >= 0 && g != 0) {
+          delete q;
+          return set_err(SDFT_ERR_UNSUPPORTED, "only segment 0 can be fixed in a 1D slit");
+        }
+      }
+      h.fixed = s.fixed_coord[0];
+    }
+    if (h.fixed >= 0) {
+      if (h.fixed >= P || h.n_seg < 2 || !s.max_distance) {
+        delete q;
+        return set_err(SDFT_ERR_ARG, "fixed segment needs a grid point, a free segment and max_distance");
+      }
+      if (h.n_seg == 2 && h.nst[1] > 1) {
+        delete q;
+        return set_err(SDFT_ERR_UNSUPPORTED, "grafted dimer with a multi-state free segment");
+      }
+      h.md.resize(h.n_seg);
+      for (int g = 0; g < h.n_seg; g++) h.md[g] = s.max_distance[(size_t)g * h.n_seg + 0];
+    } else {
+      h.md.assign(h.n_seg, 0.0);
+    }
+    for (int g = 0; g < h.n_seg; g++)
+      for (int i = 0; i < h.nst[g]; i++) {
+        int st = h.states[(size_t)g * h.S + i];
+        if (st < 0 || st >= NB) {
+          delete q;
+          return set_err(SDFT_ERR_ARG, "state bead type out of range");
+        }
+        if (g > 0)
+          for (int j = 0; j < h.nst[g - 1]; j++)
+            if (bond_lookup(bonds, st, h.states[(size_t)(g - 1) * h.S + j]) < 0) {
+              delete q;
+              return set_err(SDFT_ERR_ARG, "bond missing from bond_types");
+            }
+      }
+    h.fixed_density = s.fixed_density;
+    h.mu_species = s.mu_species;
+    // normative (child_propagators.jl:41-50): levels are visited leaves first
+    double nv = 1.0;
+    for (int g = h.n_seg - 1; g >= 0; g--) {
+      double t = 0.0;
+      for (int i = 0; i < h.nst[g]; i++) t += std::exp(-d->delta_muH[h.states[(size_t)g * h.S + i]]);
+      nv *= std::pow(t, 1.0 / (double)h.n_seg);
+    }
+    h.normative = nv;
+    h.norm_free = std::pow(nv, (double)(h.n_seg - 1));
+    if (h.n_seg > 1) gC_elems += (size_t)h.n_seg * h.S * h.S * P;
+    rho_elems += (size_t)h.n_seg * h.S * P;
+    q->sp.push_back(h);
+  }
+  // ---- layout
+  const int m_alloc = kMaxAnderson;
+  q->anderm_alloc = m_alloc;
+  const int nwa = std::max(NB, 6), nwc = std::max(NB + MB, 6 + MB);
+  Layout lay;
+  size_t o_sig = lay.take<double>(NB), o_z = lay.take<double>(NB), o_dmu = lay.take<double>(NB);
+  size_t o_bonds = lay.take<int>(2 * MB + 2);
+  size_t o_sp = lay.take<DSpecies>(NS);
+  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS);
+  for (int u = 0; u < NS; u++) {
+    const SpeciesHost& h = q->sp[u];
+    o_states[u] = lay.take<int>(h.states.size());
+    o_nst[u] = lay.take<int>(h.nst.size());
+    o_md[u] = lay.take<double>(h.md.size());
+    size_t gsz = h.n_seg > 1 ? (size_t)h.n_seg * h.S * h.S * P : 0;
+    o_gC[u] = lay.take<double>(gsz);
+    o_gP[u] = lay.take<double>(gsz);
+    o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
+  }
+  size_t o_Ext = lay.take<double>((size_t)NB * P), o_tr = lay.take<double>((size_t)NB * P);
+  size_t o_Csurf = lay.take<double>(P);
+  size_t o_Wbond = lay.take<double>((size_t)MB * P + 1), o_Wfmt = lay.take<double>((size_t)NB * 3 * P);
+  size_t o_Wmsa = lay.take<double>((size_t)NB * P), o_Wcoul = lay.take<double>(P);
+  size_t o_tw = lay.take<double2>(M / 2 + 1), o_twP = lay.take<double2>(M + 1), o_twD = lay.take<double2>(M + 1);
+  size_t o_x = lay.take<double>(q->n), o_g = lay.take<double>(q->n);
+  size_t o_lam = lay.take<double>((size_t)NB * P), o_rb = lay.take<double>((size_t)NB * P);
+  size_t o_rbo = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_Cb = lay.take<double>((size_t)NB * P), o_Cbond = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_Cmu = lay.take<double>((size_t)NB * P), o_Clng = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_wa = lay.take<double>((size_t)nwa * P), o_wb = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_wc = lay.take<double>((size_t)nwc * P);
+  size_t o_hx = lay.take<double>((size_t)m_alloc * q->n), o_hg = lay.take<double>((size_t)m_alloc * q->n);
+  size_t o_u = lay.take<double>(q->n);
+  size_t o_status = lay.take<int>(4), o_iters = lay.take<int>(4), o_err = lay.take<double>(4);
+  size_t o_scal = lay.take<double>(8);
+  size_t o_dreq = lay.take<DReq>(1), o_slot = lay.take<SolveSlot>(1), o_out = lay.take<double>(1 + NS);
+  q->bytes = lay.off;
+  cudaError_t e = cudaMalloc(&q->dmem, q->bytes);
+  if (e != cudaSuccess) {
+    delete q;
+    return set_err(SDFT_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  e = cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaFree(q->dmem);
+    delete q;
+    return set_err(SDFT_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  cudaMemsetAsync(q->dmem, 0, q->bytes, q->stream);
+  char* base = q->dmem;
+  auto P_ = [&](size_t o) { return (void*)(base + o); };
+  // ---- host tables
+  std::vector<double> Ext((size_t)NB * P, 0.0), tr((size_t)NB * P, 1.0);
+  if (d->hard_walls) {  // hard_walls.jl:6-46
+    for (int K = 0; K < P; K++) {
+      int idx = K + 1;
+      for (int j = 0; j < NB; j++) {
+        double dd = d->diameter[j];
+        int lo = jround((0.0 + dd / 2.0) / d->bin_width) + 1;
+        int hi = jround((d->length - dd / 2.0) / d->bin_width) + 1;
+        size_t qq = (size_t)j * P + K;
+        if (idx < lo) {
+          Ext[qq] += 1.0e20;
+          tr[qq] = 1.0;
+        } else if (idx == lo) {
+          tr[qq] = 0.5;
+        }
+        if (idx > hi) {
+          Ext[qq] += 1.0e20;
+          tr[qq] = 1.0;
+        } else if (idx == hi) {
+          tr[qq] = 0.5;
+        }
+      }
+    }
+  }
+  std::vector<double> surf(P, 0.0), Csurf(P, 0.0);
+  if (d->charged_walls) {  // charged_walls.jl:7-57
+    double pos[2] = {0.0, d->length};
+    for (int w = 0; w < 2; w++) {
+      int gp = jround(pos[w] / d->bin_width) + 1;
+      if (gp >= 1 && gp <= P) surf[gp - 1] += d->wall_charge[w] * (1.0 / d->bin_width);
+    }
+    for (int k = 0; k < P; k++) {
+      long double acc = 0.0L;
+      for (int K = 0; K < P; K++)
+        if (surf[K] != 0.0) acc += (long double)surf[K] * cosl(3.14159265358979323846264338327950288L * k * (2 * K + 1) / (2.0L * P));
+      Csurf[k] = (double)acc;
+    }
+  }
+  std::vector<double> Wbond((size_t)MB * P + 1, 0.0), Wfmt((size_t)NB * 3 * P), Wmsa((size_t)NB * P), Wcoul(P);
+  for (int u = 0; u < MB; u++) {
+    double sij = (d->diameter[bonds[2 * u]] + d->diameter[bonds[2 * u + 1]]) / 2.0;
+    for (int k = 0; k < P; k++)
+      Wbond[(size_t)u * P + k] = filter_k(k, NPS, d->bin_width) * (w_delta(k, NPS, d->bin_width, sij) / (4.0 * kPi * (sij * sij)));
+  }
+  for (int j = 0; j < NB; j++) {
+    double b = d->diameter[j] / 2.0;
+    for (int k = 0; k < P; k++) {
+      Wfmt[((size_t)j * 3 + 0) * P + k] = w_delta(k, NPS, d->bin_width, b);
+      Wfmt[((size_t)j * 3 + 1) * P + k] = w_step(k, NPS, d->bin_width, b);
+      Wfmt[((size_t)j * 3 + 2) * P + k] = w_vec(k, NPS, d->bin_width, b);
+      Wmsa[(size_t)j * P + k] = w_delta(k, NPS, d->bin_width, b) / (4.0 * kPi * (b * b));
+    }
+  }
+  for (int k = 0; k < P; k++) Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
+  const long double PI_L = 3.14159265358979323846264338327950288L;
+  std::vector<double2> tw(M / 2 + 1), twP(M + 1), twD(M + 1);
+  for (int k = 0; k <= M / 2; k++) tw[k] = cis(-2.0L * PI_L * k / M);
+  for (int k = 0; k <= M; k++) twP[k] = cis(-2.0L * PI_L * k / P);
+  for (int k = 0; k <= M; k++) twD[k] = cis(-PI_L * k / (2.0L * P));
+  std::vector<double> x0(q->n, 0.0);
+  for (int j = 0; j < NB; j++)
+    for (int K = 0; K < P; K++) x0[(size_t)j * P + K] = d->mu_ex_bulk[j];
+  for (int u = 0; u < MB; u++)
+    for (int e2 = 0; e2 < 2; e2++)
+      for (int K = 0; K < P; K++) x0[(size_t)P * NB + (size_t)(u * 2 + e2) * P + K] = d->lng_bulk[u];
+  // ---- device descriptor
+  std::vector<DSpecies> dsp(NS);
+  for (int u = 0; u < NS; u++) {
+    const SpeciesHost& h = q->sp[u];
+    DSpecies& s = dsp[u];
+    s.n_seg = h.n_seg;
+    s.S = h.S;
+    s.fixed = h.fixed;
+    s.states = (const int*)P_(o_states[u]);
+    s.nst = (const int*)P_(o_nst[u]);
+    s.md = (const double*)P_(o_md[u]);
+    s.fixed_density = h.fixed_density;
+    s.mu_species = h.mu_species;
+    s.normative = h.normative;
+    s.norm_free = h.norm_free;
+    s.lambda_fixed = 1.0;
+    s.gC = h.n_seg > 1 ? (double*)P_(o_gC[u]) : nullptr;
+    s.gP = h.n_seg > 1 ? (double*)P_(o_gP[u]) : nullptr;
+    s.rho_seg = (double*)P_(o_rho[u]);
+  }
+  DReq& r = q->h;
+  r.NP = P;
+  r.M = M;
+  r.L = q->L;
+  r.NB = NB;
+  r.MB = MB;
+  r.NS = NS;
+  r.funcs = (int)d->functionals;
+  r.dz = d->bin_width;
+  r.lB = d->bjerrum_length;
+  r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
+  r.n = q->n;
+  r.sig = (const double*)P_(o_sig);
+  r.z = (const double*)P_(o_z);
+  r.dmu = (const double*)P_(o_dmu);
+  r.bonds = (const int*)P_(o_bonds);
+  r.sp = (const DSpecies*)P_(o_sp);
+  r.Ext = (const double*)P_(o_Ext);
+  r.trapez = (const double*)P_(o_tr);
+  r.Csurf = (const double*)P_(o_Csurf);
+  r.Wbond = (const double*)P_(o_Wbond);
+  r.Wfmt = (const double*)P_(o_Wfmt);
+  r.Wmsa = (const double*)P_(o_Wmsa);
+  r.Wcoul = (const double*)P_(o_Wcoul);
+  r.tw = (const double2*)P_(o_tw);
+  r.twP = (const double2*)P_(o_twP);
+  r.twD = (const double2*)P_(o_twD);
+  r.x = (double*)P_(o_x);
+  r.g = (double*)P_(o_g);
+  r.lambda = (double*)P_(o_lam);
+  r.rho_beads = (double*)P_(o_rb);
+  r.rho_bonds = (double*)P_(o_rbo);
+  r.Cb = (double*)P_(o_Cb);
+  r.Cbond = (double*)P_(o_Cbond);
+  r.Cmu = (double*)P_(o_Cmu);
+  r.Clng = (double*)P_(o_Clng);
+  r.wa = (double*)P_(o_wa);
+  r.wb = (double*)P_(o_wb);
+  r.wc = (double*)P_(o_wc);
+  r.hx = (double*)P_(o_hx);
+  r.hg = (double*)P_(o_hg);
+  r.lsq_u = (double*)P_(o_u);
+  r.status = (int*)P_(o_status);
+  r.iters = (int*)P_(o_iters);
+  r.err = (double*)P_(o_err);
+  r.scal = (double*)P_(o_scal);
+  q->dreq = (DReq*)P_(o_dreq);
+  q->dslot = (SolveSlot*)P_(o_slot);
+  q->dout = (double*)P_(o_out);
+  auto up = [&](size_t o, const void* src, size_t nbytes) {
+    return cudaMemcpyAsync(base + o, src, nbytes, cudaMemcpyHostToDevice, q->stream);
+  };
+  cudaError_t ce = cudaSuccess;
+  auto chk = [&](cudaError_t x) {
+    if (ce == cudaSuccess) ce = x;
+  };
+  chk(up(o_sig, d->diameter, sizeof(double) * NB));
+  chk(up(o_z, d->valence, sizeof(double) * NB));
+  chk(up(o_dmu, d->delta_muH, sizeof(double) * NB));
+  if (MB) chk(up(o_bonds, bonds.data(), sizeof(int) * 2 * MB));
+  for (int u = 0; u < NS; u++) {
+    const SpeciesHost& h = q->sp[u];
+    chk(up(o_states[u], h.states.data(), sizeof(int) * h.states.size()));
+    chk(up(o_nst[u], h.nst.data(), sizeof(int) * h.nst.size()));
+    chk(up(o_md[u], h.md.data(), sizeof(double) * h.md.size()));
+  }
+  chk(up(o_sp, dsp.data(), sizeof(DSpecies) * NS));
+  chk(up(o_Ext, Ext.data(), sizeof(double) * Ext.size()));
+  chk(up(o_tr, tr.data(), sizeof(double) * tr.size()));
+  chk(up(o_Csurf, Csurf.data(), sizeof(double) * P));
+  chk(up(o_Wbond, Wbond.data(), sizeof(double) * Wbond.size()));
+  chk(up(o_Wfmt, Wfmt.data(), sizeof(double) * Wfmt.size()));
+  chk(up(o_Wmsa, Wmsa.data(), sizeof(double) * Wmsa.size()));
+  chk(up(o_Wcoul, Wcoul.data(), sizeof(double) * P));
+  chk(up(o_tw, tw.data(), sizeof(double2) * tw.size()));
+  chk(up(o_twP, twP.data(), sizeof(double2) * twP.size()));
+  chk(up(o_twD, twD.data(), sizeof(double2) * twD.size()));
+  chk(up(o_x, x0.data(), sizeof(double) * q->n));
+  chk(up(o_dreq, &r, sizeof(DReq)));
+  chk(cudaStreamSynchronize(q->stream));
+  if (ce != cudaSuccess) {
+    cudaStreamDestroy(q->stream);
+    cudaFree(q->dmem);
+    delete q;
+    return set_err(SDFT_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce));
+  }
+  *out = q;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_request_destroy(sdft_handle h) {
+  if (!h) return SDFT_OK;
+  cudaStreamSynchronize(h->stream);
+  cudaFree(h->dmem);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* device_bytes) {
+  if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  if (n_unknowns) *n_unknowns = h->n;
+  if (device_bytes) *device_bytes = (int64_t)h->bytes;
+  return SDFT_OK;
+}
+
+static size_t smem_bytes(int M) { return sizeof(double) * kRedDoubles + sizeof(double2) * (size_t)M; }
+
+static int prepare_kernel(const void* fn, size_t smem) {
+  if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_set_state(sdft_handle h, const double* mu_ex_K, const double* lng_K, const double* Psi,
+                              const double* PsiC) {
+  if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  const size_t P = h->NP;
+  double* x = h->h.x;
+  if (mu_ex_K) CUDA_TRY(cudaMemcpyAsync(x, mu_ex_K, sizeof(double) * P * h->NB, cudaMemcpyHostToDevice, h->stream));
+  if (lng_K && h->MB)
+    CUDA_TRY(cudaMemcpyAsync(x + P * h->NB, lng_K, sizeof(double) * P * 2 * h->MB, cudaMemcpyHostToDevice, h->stream));
+  if (Psi) CUDA_TRY(cudaMemcpyAsync(x + P * (h->NB + 2 * h->MB), Psi, sizeof(double) * P, cudaMemcpyHostToDevice, h->stream));
+  if (PsiC)
+    CUDA_TRY(cudaMemcpyAsync(x + P * (h->NB + 2 * h->MB + 1), PsiC, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return SDFT_OK;
+}
+
+static int copy_vec_out(sdft_handle h, const double* dv, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
+  const size_t P = h->NP;
+  if (mu_ex_K) CUDA_TRY(cudaMemcpyAsync(mu_ex_K, dv, sizeof(double) * P * h->NB, cudaMemcpyDeviceToHost, h->stream));
+  if (lng_K && h->MB)
+    CUDA_TRY(cudaMemcpyAsync(lng_K, dv + P * h->NB, sizeof(double) * P * 2 * h->MB, cudaMemcpyDeviceToHost, h->stream));
+  if (Psi) CUDA_TRY(cudaMemcpyAsync(Psi, dv + P * (h->NB + 2 * h->MB), sizeof(double) * P, cudaMemcpyDeviceToHost, h->stream));
+  if (PsiC)
+    CUDA_TRY(cudaMemcpyAsync(PsiC, dv + P * (h->NB + 2 * h->MB + 1), sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_get_state(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
+  if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  return copy_vec_out(h, h->h.x, mu_ex_K, lng_K, Psi, PsiC);
+}
+
+extern "C" int sdft_objective(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
+  if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  size_t sm = smem_bytes(h->M);
+  int rc = prepare_kernel((const void*)sdft_k_objective, sm);
+  if (rc) return rc;
+  sdft_k_objective<<<1, kThreads, sm, h->stream>>>(h->dreq);
+  CUDA_TRY(cudaGetLastError());
+  int st = 0;
+  CUDA_TRY(cudaMemcpyAsync(&st, h->h.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (st == ST_NORM) return set_err(SDFT_ERR_NORM, "Normalization error: lambda <= 0 or not finite");
+  return copy_vec_out(h, h->h.g, mu_ex_K, lng_K, Psi, PsiC);
+}
+
+static int validate_numerics(const sdft_numerics* num) {
+  if (!num) return set_err(SDFT_ERR_ARG, "null numerics");
+  if (num->anderm < 2 || num->anderm > kMaxAnderson) return set_err(SDFT_ERR_UNSUPPORTED, "anderm must be in [2, 16]");
+  if (num->max_iters < 1) return set_err(SDFT_ERR_ARG, "max_iters must be >= 1");
+  return SDFT_OK;
+}
+
+// chunked persistent solve of a batch of requests that share one stream
+static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32_t* iters, double* errs, int32_t* status) {
+  int rc = validate_numerics(num);
+  if (rc) return rc;
+  cudaStream_t stream = hs[0]->stream;
+  int maxM = 0;
+  for (int i = 0; i < n; i++) maxM = std::max(maxM, hs[i]->M);
+  size_t sm = smem_bytes(maxM);
+  rc = prepare_kernel((const void*)sdft_k_solve, sm);
+  if (rc) return rc;
+  DReq* dreqs = nullptr;
+  SolveSlot* dslots = nullptr;
+  CUDA_TRY(cudaMallocAsync(&dreqs, sizeof(DReq) * n, stream));
+  CUDA_TRY(cudaMallocAsync(&dslots, sizeof(SolveSlot) * n, stream));
+  std::vector<DReq> hreq(n);
+  std::vector<SolveSlot> slots(n);
+  for (int i = 0; i < n; i++) {
+    hreq[i] = hs[i]->h;
+    SolveSlot s{};
+    s.iter = 0;
+    s.status = ST_RUNNING;
+    s.use_picard = 1;
+    s.err = 1.0;
+    slots[i] = s;
+  }
+  // requests on other streams must be idle before the batch stream uses them
+  for (int i = 0; i < n; i++)
+    if (hs[i]->stream != stream) CUDA_TRY(cudaStreamSynchronize(hs[i]->stream));
+  CUDA_TRY(cudaMemcpyAsync(dreqs, hreq.data(), sizeof(DReq) * n, cudaMemcpyHostToDevice, stream));
+  CUDA_TRY(cudaMemcpyAsync(dslots, slots.data(), sizeof(SolveSlot) * n, cudaMemcpyHostToDevice, stream));
+  SolveCfg cfg;
+  cfg.max_iters = num->max_iters;
+  cfg.anderm = num->anderm;
+  cfg.damping = num->damping;
+  cfg.mixing_max = num->mixing_max;
+  cfg.switch_tole = num->switch_tole;
+  cfg.tole = num->tole;
+  // bounded launches: each runs at most `chunk` iterations per request, the
+  // host re-launches until every request has converged, failed or hit max_iters
+  const int chunk = 1024;
+  cudaEvent_t ev0, ev1;
+  CUDA_TRY(cudaEventCreate(&ev0));
+  CUDA_TRY(cudaEventCreate(&ev1));
+  double dev_ms = 0.0;
+  int launches = 0;
+  for (;;) {
+    CUDA_TRY(cudaEventRecord(ev0, stream));
+    sdft_k_solve<<<n, kThreads, sm, stream>>>(dreqs, dslots, cfg, chunk);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(ev1, stream));
+    launches++;
+    CUDA_TRY(cudaMemcpyAsync(slots.data(), dslots, sizeof(SolveSlot) * n, cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+    dev_ms += ms;
+    bool running = false;
+    for (int i = 0; i < n; i++) running |= slots[i].status == ST_RUNNING;
+    if (!running) break;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  g_batch_ms = dev_ms;
+  g_batch_launches = launches;
+  g_batch_latency.assign(n, 0.0);
+  for (int i = 0; i < n; i++) g_batch_latency[i] = (double)(slots[i].t1 - slots[i].t0) * 1e-6;
+  cudaFreeAsync(dreqs, stream);
+  cudaFreeAsync(dslots, stream);
+  CUDA_TRY(cudaStreamSynchronize(stream));
+  int worst = SDFT_OK;
+  for (int i = 0; i < n; i++) {
+    if (iters) iters[i] = slots[i].iter;
+    if (errs) errs[i] = slots[i].err;
+    int r = slots[i].status == ST_OK ? SDFT_OK
+            : slots[i].status == ST_MAX_ITERS ? SDFT_MAX_ITERS
+            : slots[i].status == ST_NORM ? SDFT_ERR_NORM
+                                         : SDFT_ERR_NONFINITE;
+    if (status) status[i] = r;
+    if (r > worst) worst = r;
+  }
+  return worst;
+}
+
+extern "C" int sdft_solve(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err) {
+  if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  int32_t it = 0, st = 0;
+  double e = 0.0;
+  int rc = run_batch(&h, 1, num, &it, &e, &st);
+  if (iters) *iters = it;
+  if (err) *err = e;
+  if (rc == SDFT_ERR_CUDA) return rc;
+  if (st == SDFT_ERR_NORM) return set_err(SDFT_ERR_NORM, "Normalization error: lambda <= 0 or not finite");
+  if (st == SDFT_ERR_NONFINITE) return set_err(SDFT_ERR_NONFINITE, "non-finite fixed-point residual");
+  return st;
+}
+
+extern "C" int sdft_solve_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32_t* iters, double* errs,
+                                int32_t* status) {
+  if (!hs || n < 1) return set_err(SDFT_ERR_ARG, "empty batch");
+  for (int i = 0; i < n; i++)
+    if (!hs[i]) return set_err(SDFT_ERR_ARG, "null handle in batch");
+  return run_batch(hs, n, num, iters, errs, status);
+}
+
+extern "C" int sdft_last_batch_stats(double* device_ms, int32_t* launches, double* latency_ms, int32_t n) {
+  if (device_ms) *device_ms = g_batch_ms;
+  if (launches) *launches = g_batch_launches;
+  if (latency_ms)
+    for (int i = 0; i < n && i < (int)g_batch_latency.size(); i++) latency_ms[i] = g_batch_latency[i];
+  return SDFT_OK;
+}
+
+extern "C" int sdft_get_densities(sdft_handle h, double* const* rho_segments, double* rho_beads_K, double* rho_bonds_K) {
+  if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  const size_t P = h->NP;
+  if (rho_segments) {
+    std::vector<DSpecies> dsp(h->NS);
+    CUDA_TRY(cudaMemcpyAsync(dsp.data(), h->h.sp, sizeof(DSpecies) * h->NS, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int u = 0; u < h->NS; u++)
+      if (rho_segments[u])
+        CUDA_TRY(cudaMemcpyAsync(rho_segments[u], dsp[u].rho_seg, sizeof(double) * P * h->sp[u].S * h->sp[u].n_seg,
+                                 cudaMemcpyDeviceToHost, h->stream));
+  }
+  if (rho_beads_K) CUDA_TRY(cudaMemcpyAsync(rho_beads_K, h->h.rho_beads, sizeof(double) * P * h->NB, cudaMemcpyDeviceToHost, h->stream));
+  if (rho_bonds_K && h->MB)
+    CUDA_TRY(cudaMemcpyAsync(rho_bonds_K, h->h.rho_bonds, sizeof(double) * P * 2 * h->MB, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return SDFT_OK;
+}
+
+static int run_omega(sdft_handle h, std::vector<double>& out) {
+  size_t sm = smem_bytes(h->M);
+  int rc = prepare_kernel((const void*)sdft_k_omega, sm);
+  if (rc) return rc;
+  sdft_k_omega<<<1, kThreads, sm, h->stream>>>(h->dreq, h->dout);
+  CUDA_TRY(cudaGetLastError());
+  out.assign(1 + h->NS, 0.0);
+  CUDA_TRY(cudaMemcpyAsync(out.data(), h->dout, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_grand_potential(sdft_handle h, double* omega) {
+  if (!h || !omega) return set_err(SDFT_ERR_ARG, "null argument");
+  std::vector<double> out;
+  int rc = run_omega(h, out);
+  if (rc) return rc;
+  *omega = out[0];
+  return SDFT_OK;
+}
+
+extern "C" int sdft_num_species(sdft_handle h, double* num_species) {
+  if (!h || !num_species) return set_err(SDFT_ERR_ARG, "null argument");
+  std::vector<double> out;
+  int rc = run_omega(h, out);
+  if (rc) return rc;
+  for (int u = 0; u < h->NS; u++) num_species[u] = out[1 + u];
+  return SDFT_OK;
+}

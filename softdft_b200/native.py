@@ -1,0 +1,170 @@
+"""ctypes binding of libsoftdft.so, the device solve behind include/softdft.h.
+
+The library is built in-tree (``__graft_entry__.build()``); importing this
+module never falls back to anything else: a missing library or a missing GPU
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .host.descriptor import Descriptor, Numerics
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsoftdft.so")
+_LIB = None
+
+SDFT_OK = 0
+SDFT_MAX_ITERS = 1
+STATUS_NAMES = {0: "OK", 1: "MAX_ITERS", 2: "ERR_ARG", 3: "ERR_UNSUPPORTED", 4: "ERR_CUDA", 5: "ERR_OOM",
+                6: "ERR_NORM", 7: "ERR_NONFINITE", 8: "ERR_TIMEOUT"}
+EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_numerics_default",
+           "sdft_request_create", "sdft_request_destroy", "sdft_request_sizes", "sdft_set_state",
+           "sdft_get_state", "sdft_objective", "sdft_solve", "sdft_get_densities", "sdft_grand_potential",
+           "sdft_num_species", "sdft_solve_batch", "sdft_last_batch_stats"]
+
+
+class SdftError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build the CUDA extension first (__graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.sdft_abi_version.restype = C.c_int32
+        L.sdft_last_error.restype = C.c_char_p
+        L.sdft_device_count.argtypes = [C.POINTER(C.c_int32)]
+        L.sdft_numerics_default.argtypes = [vp]
+        L.sdft_numerics_default.restype = None
+        L.sdft_request_create.argtypes = [vp, C.c_int32, C.POINTER(vp)]
+        L.sdft_request_destroy.argtypes = [vp]
+        L.sdft_request_sizes.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.sdft_set_state.argtypes = [vp, vp, vp, vp, vp]
+        L.sdft_get_state.argtypes = [vp, vp, vp, vp, vp]
+        L.sdft_objective.argtypes = [vp, vp, vp, vp, vp]
+        L.sdft_solve.argtypes = [vp, vp, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        L.sdft_get_densities.argtypes = [vp, vp, vp, vp]
+        L.sdft_grand_potential.argtypes = [vp, C.POINTER(C.c_double)]
+        L.sdft_num_species.argtypes = [vp, vp]
+        L.sdft_solve_batch.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
+        L.sdft_last_batch_stats.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int32), vp, C.c_int32]
+        _LIB = L
+    return _LIB
+
+
+def _check(rc: int) -> int:
+    if rc not in (SDFT_OK, SDFT_MAX_ITERS):
+        raise SdftError(rc, lib().sdft_last_error().decode())
+    return rc
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def device_count() -> int:
+    c = C.c_int32()
+    lib().sdft_device_count(C.byref(c))
+    return int(c.value)
+
+
+class DeviceSystem:
+    """One request on the GPU (the C-ABI handle)."""
+
+    def __init__(self, d: Descriptor, precision: int = 0):
+        self.d = d
+        self.h = C.c_void_p()
+        _check(lib().sdft_request_create(C.byref(d.desc), precision, C.byref(self.h)))
+        n = C.c_int64()
+        b = C.c_int64()
+        lib().sdft_request_sizes(self.h, C.byref(n), C.byref(b))
+        self.n = int(n.value)
+        self.device_bytes = int(b.value)
+
+    def close(self):
+        if self.h:
+            lib().sdft_request_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _split(self, x):
+        d = self.d
+        P, NB, MB = d.np_, d.nb, d.mb
+        return (x[: P * NB], x[P * NB: P * (NB + 2 * MB)], x[P * (NB + 2 * MB): P * (NB + 2 * MB + 1)], x[-1:])
+
+    def get_x(self) -> np.ndarray:
+        x = np.zeros(self.n)
+        mu, lng, psi, psic = self._split(x)
+        _check(lib().sdft_get_state(self.h, _p(mu), _p(lng) if lng.size else None, _p(psi), _p(psic)))
+        return x
+
+    def set_x(self, x: np.ndarray) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        mu, lng, psi, psic = (np.ascontiguousarray(a) for a in self._split(x))
+        _check(lib().sdft_set_state(self.h, _p(mu), _p(lng) if lng.size else None, _p(psi), _p(psic)))
+
+    def objective(self) -> np.ndarray:
+        g = np.zeros(self.n)
+        mu, lng, psi, psic = self._split(g)
+        _check(lib().sdft_objective(self.h, _p(mu), _p(lng) if lng.size else None, _p(psi), _p(psic)))
+        return g
+
+    def solve(self, num: Numerics):
+        it = C.c_int32()
+        err = C.c_double()
+        rc = _check(lib().sdft_solve(self.h, C.byref(num), C.byref(it), C.byref(err)))
+        return int(it.value), float(err.value), rc
+
+    def densities(self):
+        d = self.d
+        segs = [np.zeros(d.np_ * d.max_states[u] * d.n_seg[u]) for u in range(d.n_species)]
+        arr = (C.c_void_p * d.n_species)(*[s.ctypes.data for s in segs])
+        beads = np.zeros(d.np_ * d.nb)
+        bonds = np.zeros(max(d.np_ * 2 * d.mb, 1))
+        _check(lib().sdft_get_densities(self.h, arr, _p(beads), _p(bonds)))
+        return segs, beads, bonds[: d.np_ * 2 * d.mb]
+
+    def grand_potential(self) -> float:
+        om = C.c_double()
+        _check(lib().sdft_grand_potential(self.h, C.byref(om)))
+        return float(om.value)
+
+    def num_species(self) -> np.ndarray:
+        out = np.zeros(self.d.n_species)
+        _check(lib().sdft_num_species(self.h, _p(out)))
+        return out
+
+
+def solve_batch(systems, num: Numerics):
+    n = len(systems)
+    hs = (C.c_void_p * n)(*[s.h.value for s in systems])
+    iters = np.zeros(n, dtype=np.int32)
+    errs = np.zeros(n)
+    status = np.zeros(n, dtype=np.int32)
+    rc = lib().sdft_solve_batch(hs, n, C.byref(num), _p(iters), _p(errs), _p(status))
+    if rc not in (0, 1, 6, 7):
+        raise SdftError(rc, lib().sdft_last_error().decode())
+    return iters, errs, status
+
+
+def last_batch_stats(n: int = 0):
+    """(device_ms, launches, per-request latency ms) of the last solve on this thread."""
+    ms = C.c_double()
+    launches = C.c_int32()
+    lat = np.zeros(max(n, 1))
+    lib().sdft_last_batch_stats(C.byref(ms), C.byref(launches), _p(lat), n)
+    return float(ms.value), int(launches.value), lat[:n]

@@ -159,7 +159,8 @@ def batch_uneven(n: int = 512, seed: int = 3, np_lo: int = 2048, np_hi: int = 16
 
 
 def grafted_brush(np_: int, dz: float, n_chain: int, sigma_g: float, pKa: float, pH: float, salt_M: float,
-                  eta: float = 0.3, anderm: int = 5, damping: float = 0.1, tole: float = 1e-8) -> dict:
+                  eta: float = 0.3, anderm: int = 5, damping: float = 0.1, tole: float = 1e-8,
+                  mixing_max: float = 0.05, switch_tole: float = 10.0) -> dict:
     """Weak-polyacid brushes grafted by segment 1 on both walls."""
     H = slit_length(np_, dz)
     rho_salt = molar_to_density(salt_M)
@@ -184,6 +185,7 @@ def grafted_brush(np_: int, dz: float, n_chain: int, sigma_g: float, pKa: float,
             {"species": ["Y", "Z"], "coeffs": [1, 1], "pK": 14.0},
         ],
         "monomers": _monomers(),
-        "numerical": {"anderm": anderm, "damping": damping, "tole": tole},
+        "numerical": {"anderm": anderm, "damping": damping, "tole": tole, "mixing_max": mixing_max,
+                      "switch_tole": switch_tole},
         "model": ["ideal", "TPT1mfmt", "TPT1msa"],
     }

@@ -1,0 +1,137 @@
+"""Device solve vs the CPU oracle, through the C ABI (libsoftdft.so).
+
+Tolerances (FP64 plain form):
+* one G(x) evaluation: 1e-11 relative to max|G| (the device convolves in DCT
+  space, the oracle with complex FFTs of the mirrored grid, as the reference);
+* densities of the evaluation: 1e-12;
+* converged states at tole 1e-10: 1e-7 relative on densities, 1e-8 on Omega.
+  Trajectories cannot be compared step by step: the first Anderson steps
+  solve near-collinear least-squares problems and the Picard phase amplifies
+  1e-16 differences, so iteration counts are reported, not matched.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleSystem
+from softdft_b200 import native
+from softdft_b200.host.descriptor import numerics_from_dict
+from tests.helpers import descriptor, rel, small_slit
+from softdft_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "acid_salt": small_slit(),
+    "charged_walls": small_slit(wall_charge=-0.05),
+    "mfmt_msa": small_slit(models=["ideal", "mfmt", "msa"]),
+    "no_walls": small_slit(walls=False),
+    "low_pH": small_slit(pH=3.0, salt=0.01),
+    "brush": workloads.grafted_brush(256, 0.05, 10, 0.05, 4.5, 7.0, 0.01),
+    "diblock_small": None,
+}
+
+
+def _diblock_small():
+    ds = workloads.diblock_slit(512)
+    ds["species"][0]["sequence"] = "A" * 6 + "C" * 6
+    return ds
+
+
+CASES["diblock_small"] = _diblock_small()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_objective_matches_oracle(name):
+    dft = descriptor(CASES[name])
+    o = OracleSystem(dft.descriptor)
+    g = native.DeviceSystem(dft.descriptor)
+    assert rel(g.get_x(), o.get_x()) == 0.0
+    go, gg = o.objective(), g.objective()
+    assert rel(gg, go) < 1e-11
+    so, bo, bno = o.densities()
+    sg, bg, bng = g.densities()
+    assert rel(bg, bo) < 1e-12
+    if bno.size:
+        assert rel(bng, bno) < 1e-12
+    for a, b in zip(sg, so):
+        assert rel(a, b) < 1e-12
+
+
+def test_objective_at_perturbed_state():
+    dft = descriptor(CASES["acid_salt"])
+    o = OracleSystem(dft.descriptor)
+    g = native.DeviceSystem(dft.descriptor)
+    rng = np.random.default_rng(7)
+    x = o.get_x() + 1e-2 * rng.standard_normal(o.n)
+    o.set_x(x)
+    g.set_x(x)
+    assert rel(g.objective(), o.objective()) < 1e-11
+
+
+def test_picard_trajectory_matches():
+    ds = copy.deepcopy(CASES["acid_salt"])
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    g = native.DeviceSystem(dft.descriptor)
+    num = numerics_from_dict(dict(ds["numerical"], max_iters=30, switch_tole=1e-30))
+    _, eo, _, _ = o.solve(num)
+    _, eg, _ = g.solve(num)
+    assert rel(g.get_x(), o.get_x()) < 1e-12
+    assert abs(eg - eo) / eo < 1e-10
+
+
+@pytest.mark.parametrize("name", ["acid_salt", "brush"])
+def test_converged_state_matches(name):
+    ds = copy.deepcopy(CASES[name])
+    ds["numerical"]["tole"] = 1e-10
+    ds["numerical"]["max_iters"] = 5000
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    g = native.DeviceSystem(dft.descriptor)
+    num = numerics_from_dict(ds["numerical"])
+    it_o, err_o, rc_o, _ = o.solve(num)
+    it_g, err_g, rc_g = g.solve(num)
+    assert rc_o == 0 and rc_g == 0, (it_o, err_o, it_g, err_g)
+    assert err_g < 1e-10
+    _, bo, _ = o.densities()
+    _, bg, _ = g.densities()
+    assert rel(bg, bo) < 1e-7
+    om_o, om_g = o.grand_potential(), g.grand_potential()
+    assert abs(om_g - om_o) / abs(om_o) < 1e-8
+    assert rel(g.num_species(), o.num_species()) < 1e-7
+
+
+def test_batch_equals_single():
+    ds = copy.deepcopy(CASES["acid_salt"])
+    num = numerics_from_dict(dict(ds["numerical"], max_iters=60))
+    systems = []
+    for pH in (5.0, 7.0, 9.0):
+        d2 = copy.deepcopy(ds)
+        d2["species"][4]["pSpecies"] = pH
+        systems.append(descriptor(d2))
+    singles = []
+    for dft in systems:
+        s = native.DeviceSystem(dft.descriptor)
+        s.solve(num)
+        singles.append(s.get_x())
+    batch = [native.DeviceSystem(dft.descriptor) for dft in systems]
+    iters, errs, status = native.solve_batch(batch, num)
+    for b, x in zip(batch, singles):
+        assert rel(b.get_x(), x) == 0.0
+
+
+def test_max_iters_status_and_nonfinite():
+    ds = copy.deepcopy(CASES["acid_salt"])
+    dft = descriptor(ds)
+    g = native.DeviceSystem(dft.descriptor)
+    num = numerics_from_dict(dict(ds["numerical"], max_iters=3))
+    it, err, rc = g.solve(num)
+    assert it == 3 and rc == native.SDFT_MAX_ITERS
+    x = g.get_x()
+    x[5] = np.nan
+    g.set_x(x)
+    with pytest.raises(native.SdftError) as e:
+        g.solve(num)
+    assert e.value.code == 7

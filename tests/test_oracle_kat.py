@@ -1,0 +1,106 @@
+"""Known-answer tests that pin the CPU oracle (the reference ships no golden
+vectors and cannot run here, so these physics identities are the anchor):
+
+* bulk fixed point: in a wall-free box the mirrored grid is an infinite
+  homogeneous fluid, so G(x0) at the bulk state x0 (process_guess.jl:5-54) must
+  return x0 (FMT/TPT1 weights, propagators and the bulk iLST formulas agree);
+* ideal-chain limit: without excess functionals every segment density equals
+  the bulk segment density;
+* ideal dissociation: the B-state fraction is 1/(1 + 10^(pKa - pH));
+* the k-space weights carry the analytic integrals at k = 0 (n3 of a uniform
+  density is rho*pi*sigma^3/6).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleSystem
+from tests.helpers import descriptor, rel, small_slit
+
+
+def test_bulk_fixed_point_fmt():
+    ds = small_slit(models=["ideal", "TPT1mfmt"], walls=False)
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    x0 = o.get_x()
+    g = o.objective()
+    mu0, lng0, psi0, psic0 = dft.split(x0)
+    mu, lng, psi, psic = dft.split(g)
+    assert rel(mu, mu0) < 1e-9
+    assert rel(lng, lng0) < 1e-9
+    assert np.max(np.abs(psi)) < 1e-9
+    assert abs(psic[0]) < 1e-8
+
+
+def test_bulk_fixed_point_fmt_msa():
+    ds = small_slit(models=["ideal", "TPT1mfmt", "TPT1msa"], walls=False)
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    x0 = o.get_x()
+    g = o.objective()
+    mu0, lng0, _, _ = dft.split(x0)
+    mu, lng, psi, _ = dft.split(g)
+    assert rel(mu, mu0) < 1e-8
+    assert rel(lng, lng0) < 1e-8
+    assert np.max(np.abs(psi)) < 1e-9
+
+
+def test_ideal_chain_limit():
+    ds = small_slit(models=["ideal"], walls=False, n_chain=8)
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    o.objective()
+    segs, beads, _ = o.densities()
+    bulk = dft.bulk_system.bulk
+    d = dft.descriptor
+    for u in range(d.n_species):
+        s = segs[u].reshape((d.n_seg[u], d.max_states[u], d.np_))
+        ref = bulk.rho_segments[u]  # (S, N)
+        for g in range(d.n_seg[u]):
+            for i in range(d.max_states[u]):
+                assert np.allclose(s[g, i], ref[i, g], rtol=1e-12, atol=1e-300)
+    assert rel(beads.reshape(d.nb, d.np_)[:, d.np_ // 2], bulk.rho_beads) < 1e-12
+
+
+@pytest.mark.parametrize("pH", [3.0, 4.5, 7.0])
+def test_ideal_dissociation_fraction(pH):
+    ds = small_slit(models=["ideal"], walls=False, pH=pH, n_chain=5)
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    o.objective()
+    segs, _, _ = o.densities()
+    d = dft.descriptor
+    s = segs[0].reshape((d.n_seg[0], d.max_states[0], d.np_))
+    alpha = s[:, 1, :].sum() / s.sum()
+    assert abs(alpha - 1.0 / (1.0 + 10 ** (4.5 - pH))) < 1e-12
+
+
+def test_packing_fraction_weight_at_k0():
+    ds = small_slit(models=["ideal", "TPT1mfmt"], walls=False)
+    dft = descriptor(ds)
+    bulk = dft.bulk_system.bulk
+    sig = np.asarray(dft.bulk_system.molsys.diameters)
+    eta = float(np.sum(bulk.rho_beads * math.pi * sig ** 3 / 6))
+    # the oracle's FMT n3 weight at k=0 is 4/3 pi (sigma/2)^3; a uniform field
+    # reproduces the bulk packing fraction through the excess chemical potential
+    o = OracleSystem(dft.descriptor)
+    g = o.objective()
+    mu, _, _, _ = dft.split(g)
+    assert 0.25 < eta < 0.45
+    assert rel(mu[dft.NP // 2], bulk.mu_ex) < 1e-9
+
+
+def test_walls_zero_density_inside():
+    ds = small_slit()
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    o.objective()
+    _, beads, _ = o.densities()
+    d = dft.descriptor
+    b = beads.reshape(d.nb, d.np_)
+    ext, tr = o.fields()
+    ext = ext.reshape(d.nb, d.np_)
+    assert np.all(b[ext > 1e19] == 0.0)
+    # contact points carry trapezoid weight 1/2
+    assert np.count_nonzero(tr.reshape(d.nb, d.np_)[0] == 0.5) == 2
