@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=0, help="requests per GPU (0: two per SM)")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling case: only batched solves capped at --max-iters, one short line out")
+    ap.add_argument("--max-iters", type=int, default=0)
     return ap.parse_args()
 
 
@@ -200,6 +203,28 @@ def run_reference(args, ws, rank):
     print(json.dumps(out), flush=True)
 
 
+def run_profile_case(args):
+    """A short, bounded launch sequence of the solve kernel for ncu captures."""
+    import numpy as np
+
+    from softdft_b200 import native
+    from softdft_b200.api import setup_request
+    from softdft_b200.host.descriptor import numerics_from_dict
+    name, ds = workload()
+    nd = dict(ds["numerical"])
+    if args.max_iters > 0:
+        nd["max_iters"] = args.max_iters
+    dft = setup_request(copy.deepcopy(ds))
+    num = numerics_from_dict(nd)
+    B = args.batch if args.batch > 0 else 148
+    systems = [native.DeviceSystem(dft.descriptor) for _ in range(B)]
+    for _ in range(args.warmup + args.steps):
+        iters, errs, status = native.solve_batch(systems, num)
+    ms, nl, _ = native.last_batch_stats(B)
+    print(json.dumps({"profile_case": name, "batch": B, "iters": int(np.max(iters)), "device_ms": ms,
+                      "launches": nl}), flush=True)
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
 
@@ -313,7 +338,9 @@ def main():
     args = parse()
     ws, rank, local = dist_init()
     try:
-        if args.impl == "reference":
+        if args.profile:
+            run_profile_case(args)
+        elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:
             run_ours(args, ws, rank, local)
