@@ -162,6 +162,30 @@ int sdft_solve_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num,
  * No reference counterpart: measurement support for the batched solve. */
 int sdft_last_batch_stats(double* device_ms, int32_t* launches, double* latency_ms, int32_t n);
 
+/* Bytes of the static device array behind sdft_objective_noalloc (16 MiB). */
+#define SDFT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+
+/* One G(x) evaluation that allocates no device memory.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc, because their device
+ * memory belongs to another allocator (a framework's caching pool, or a budget
+ * reserved once at start-up) or because they cannot afford the implicit device
+ * synchronisation a cudaMalloc may cause while other work is in flight.
+ *  - x_dev, g_dev: the caller's device arrays of n = NP*(NB+2*MB+1)+1 doubles in
+ *    the layout of sdft_objective (x read, G(x) written).
+ *  - Every other array (grid fields, weights, propagators, densities, spectra)
+ *    lives in one static device array of SDFT_NOALLOC_SCRATCH_BYTES that each GPU
+ *    loading the library holds until the process exits.  A system whose working
+ *    set exceeds it is rejected with SDFT_ERR_ARG and a message giving both sizes
+ *    (the plain slit, NP = 1024 with a 20-segment chain, needs about 3 MB).
+ *  - The first call on a device looks up the array's device address; make that
+ *    first call before any stream capture.
+ *  - All calls share the array and it keeps the last call's contents; each call
+ *    clears the part it uses.  Calls that overlap on the GPU (other streams or
+ *    host threads) race on it.
+ *  - stream: a cudaStream_t, NULL for the default stream; the call waits for its
+ *    own work on that stream before returning. */
+int sdft_objective_noalloc(const sdft_system_desc* desc, const double* x_dev, double* g_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

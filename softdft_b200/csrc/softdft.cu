@@ -798,3 +798,310 @@ extern "C" int sdft_num_species(sdft_handle h, double* num_species) {
   for (int u = 0; u < h->NS; u++) num_species[u] = out[1 + u];
   return SDFT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// G(x) without device allocation (sdft_objective_noalloc)
+//
+// Some callers cannot call cudaMalloc: their device memory belongs to another
+// allocator (a framework's caching pool, or a budget reserved once at start-up)
+// that must stay the only owner, or they cannot afford the implicit device
+// synchronisation a cudaMalloc may cause while other work is in flight.  This
+// entry point evaluates G(x) with every intermediate array in one static device
+// array of SDFT_NOALLOC_SCRATCH_BYTES; the caller passes x and G(x) as its own
+// device arrays.  The array exists on every GPU that loads the library, until
+// the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+static __device__ __align__(256) unsigned char sdft_noalloc_scratch[SDFT_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+constexpr int kNoAllocMaxDevices = 64;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// device address of the scratch array on the current device, looked up once per device
+int noalloc_scratch_address(void** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return set_err(SDFT_ERR_CUDA, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, sdft_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_err(SDFT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return SDFT_OK;
+}
+}  // namespace
+
+extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x_dev, double* g_dev, void* stream_ptr) {
+  if (!d || !x_dev || !g_dev) return set_err(SDFT_ERR_ARG, "null argument");
+  if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
+  const int P = d->np;
+  if (P < 16 || (P & (P - 1)) != 0) return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP = 2^k >= 16");
+  if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
+  if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
+  if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
+  if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
+  if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_ptr);
+  void* base_v = nullptr;
+  int rc = noalloc_scratch_address(&base_v);
+  if (rc) return rc;
+  char* base = static_cast<char*>(base_v);
+  const int NB = d->nb, MB = d->mb, NS = d->n_species, M = P / 2;
+  int L = 0;
+  while ((1 << L) < M) L++;
+  const int NPS = 2 * P;
+  std::vector<int> bonds(d->bond_types, d->bond_types + 2 * MB);
+  std::vector<SpeciesHost> sp;
+  for (int u = 0; u < NS; u++) {
+    const sdft_species_desc& s = d->species[u];
+    SpeciesHost h;
+    h.n_seg = s.n_seg;
+    h.S = s.max_states;
+    if (h.n_seg < 1 || h.S < 1 || h.S > kMaxStates)
+      return set_err(SDFT_ERR_UNSUPPORTED, "segments >= 1 and 1 <= states <= 4 per segment are required");
+    for (int g = 0; g < h.n_seg; g++) {
+      if (s.parent[g] != g - 1) return set_err(SDFT_ERR_UNSUPPORTED, "linear chains only");
+      if (s.n_states[g] < 1 || s.n_states[g] > h.S) return set_err(SDFT_ERR_ARG, "n_states out of range");
+    }
+    h.nst.assign(s.n_states, s.n_states + h.n_seg);
+    h.states.assign(s.states, s.states + (size_t)h.n_seg * h.S);
+    h.fixed = -1;
+    if (s.fixed_coord) {
+      for (int g = 1; g < h.n_seg; g++)
+        if (s.fixed_coord[g] >= 0) return set_err(SDFT_ERR_UNSUPPORTED, "only segment 0 can be fixed in a 1D slit");
+      h.fixed = s.fixed_coord[0];
+    }
+    if (h.fixed >= 0) {
+      if (h.fixed >= P || h.n_seg < 2 || !s.max_distance)
+        return set_err(SDFT_ERR_ARG, "fixed segment needs a grid point, a free segment and max_distance");
+      if (h.n_seg == 2 && h.nst[1] > 1) return set_err(SDFT_ERR_UNSUPPORTED, "grafted dimer with a multi-state free segment");
+      h.md.resize(h.n_seg);
+      for (int g = 0; g < h.n_seg; g++) h.md[g] = s.max_distance[(size_t)g * h.n_seg];
+    } else {
+      h.md.assign(h.n_seg, 0.0);
+    }
+    for (int g = 0; g < h.n_seg; g++)
+      for (int i = 0; i < h.nst[g]; i++) {
+        int st = h.states[(size_t)g * h.S + i];
+        if (st < 0 || st >= NB) return set_err(SDFT_ERR_ARG, "state bead type out of range");
+        if (g > 0)
+          for (int j = 0; j < h.nst[g - 1]; j++)
+            if (bond_lookup(bonds, st, h.states[(size_t)(g - 1) * h.S + j]) < 0)
+              return set_err(SDFT_ERR_ARG, "bond missing from bond_types");
+      }
+    h.fixed_density = s.fixed_density;
+    h.mu_species = s.mu_species;
+    double nv = 1.0;
+    for (int g = h.n_seg - 1; g >= 0; g--) {
+      double t = 0.0;
+      for (int i = 0; i < h.nst[g]; i++) t += std::exp(-d->delta_muH[h.states[(size_t)g * h.S + i]]);
+      nv *= std::pow(t, 1.0 / (double)h.n_seg);
+    }
+    h.normative = nv;
+    h.norm_free = std::pow(nv, (double)(h.n_seg - 1));
+    sp.push_back(h);
+  }
+  // layout inside the scratch array (no Anderson history: G(x) only)
+  const int nwa = std::max(NB, 6), nwc = std::max(NB + MB, 6 + MB);
+  Layout lay;
+  size_t o_sig = lay.take<double>(NB), o_z = lay.take<double>(NB), o_dmu = lay.take<double>(NB);
+  size_t o_bonds = lay.take<int>(2 * MB + 2);
+  size_t o_sp = lay.take<DSpecies>(NS);
+  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS);
+  for (int u = 0; u < NS; u++) {
+    const SpeciesHost& h = sp[u];
+    o_states[u] = lay.take<int>(h.states.size());
+    o_nst[u] = lay.take<int>(h.nst.size());
+    o_md[u] = lay.take<double>(h.md.size());
+    size_t gsz = h.n_seg > 1 ? (size_t)h.n_seg * h.S * h.S * P : 0;
+    o_gC[u] = lay.take<double>(gsz);
+    o_gP[u] = lay.take<double>(gsz);
+    o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
+  }
+  size_t o_Ext = lay.take<double>((size_t)NB * P), o_tr = lay.take<double>((size_t)NB * P);
+  size_t o_Csurf = lay.take<double>(P);
+  size_t o_Wbond = lay.take<double>((size_t)MB * P + 1), o_Wfmt = lay.take<double>((size_t)NB * 3 * P);
+  size_t o_Wmsa = lay.take<double>((size_t)NB * P), o_Wcoul = lay.take<double>(P);
+  size_t o_tw = lay.take<double2>(M / 2 + 1), o_twP = lay.take<double2>(M + 1), o_twD = lay.take<double2>(M + 1);
+  size_t o_lam = lay.take<double>((size_t)NB * P), o_rb = lay.take<double>((size_t)NB * P);
+  size_t o_rbo = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_Cb = lay.take<double>((size_t)NB * P), o_Cbond = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_Cmu = lay.take<double>((size_t)NB * P), o_Clng = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_wa = lay.take<double>((size_t)nwa * P), o_wb = lay.take<double>((size_t)MB * 2 * P + 1);
+  size_t o_wc = lay.take<double>((size_t)nwc * P);
+  size_t o_status = lay.take<int>(4), o_iters = lay.take<int>(4), o_err = lay.take<double>(4);
+  size_t o_scal = lay.take<double>(8);
+  size_t o_dreq = lay.take<DReq>(1);
+  if (lay.off > (size_t)SDFT_NOALLOC_SCRATCH_BYTES)
+    return set_err(SDFT_ERR_ARG, "system needs " + std::to_string(lay.off) + " bytes of scratch; sdft_objective_noalloc holds " +
+                                     std::to_string((size_t)SDFT_NOALLOC_SCRATCH_BYTES));
+  // host tables (the same formulas as sdft_request_create)
+  std::vector<double> Ext((size_t)NB * P, 0.0), tr((size_t)NB * P, 1.0);
+  if (d->hard_walls) {
+    for (int K = 0; K < P; K++) {
+      int idx = K + 1;
+      for (int j = 0; j < NB; j++) {
+        double dd = d->diameter[j];
+        int lo = jround((0.0 + dd / 2.0) / d->bin_width) + 1;
+        int hi = jround((d->length - dd / 2.0) / d->bin_width) + 1;
+        size_t qq = (size_t)j * P + K;
+        if (idx < lo) {
+          Ext[qq] += 1.0e20;
+          tr[qq] = 1.0;
+        } else if (idx == lo) {
+          tr[qq] = 0.5;
+        }
+        if (idx > hi) {
+          Ext[qq] += 1.0e20;
+          tr[qq] = 1.0;
+        } else if (idx == hi) {
+          tr[qq] = 0.5;
+        }
+      }
+    }
+  }
+  std::vector<double> surf(P, 0.0), Csurf(P, 0.0);
+  if (d->charged_walls) {
+    double pos[2] = {0.0, d->length};
+    for (int w = 0; w < 2; w++) {
+      int gp = jround(pos[w] / d->bin_width) + 1;
+      if (gp >= 1 && gp <= P) surf[gp - 1] += d->wall_charge[w] * (1.0 / d->bin_width);
+    }
+    for (int k = 0; k < P; k++) {
+      long double acc = 0.0L;
+      for (int K = 0; K < P; K++)
+        if (surf[K] != 0.0) acc += (long double)surf[K] * cosl(3.14159265358979323846264338327950288L * k * (2 * K + 1) / (2.0L * P));
+      Csurf[k] = (double)acc;
+    }
+  }
+  std::vector<double> Wbond((size_t)MB * P + 1, 0.0), Wfmt((size_t)NB * 3 * P), Wmsa((size_t)NB * P), Wcoul(P);
+  for (int u = 0; u < MB; u++) {
+    double sij = (d->diameter[bonds[2 * u]] + d->diameter[bonds[2 * u + 1]]) / 2.0;
+    for (int k = 0; k < P; k++)
+      Wbond[(size_t)u * P + k] = filter_k(k, NPS, d->bin_width) * (w_delta(k, NPS, d->bin_width, sij) / (4.0 * kPi * (sij * sij)));
+  }
+  for (int j = 0; j < NB; j++) {
+    double b = d->diameter[j] / 2.0;
+    for (int k = 0; k < P; k++) {
+      Wfmt[((size_t)j * 3 + 0) * P + k] = w_delta(k, NPS, d->bin_width, b);
+      Wfmt[((size_t)j * 3 + 1) * P + k] = w_step(k, NPS, d->bin_width, b);
+      Wfmt[((size_t)j * 3 + 2) * P + k] = w_vec(k, NPS, d->bin_width, b);
+      Wmsa[(size_t)j * P + k] = w_delta(k, NPS, d->bin_width, b) / (4.0 * kPi * (b * b));
+    }
+  }
+  for (int k = 0; k < P; k++) Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
+  const long double PI_L = 3.14159265358979323846264338327950288L;
+  std::vector<double2> tw(M / 2 + 1), twP(M + 1), twD(M + 1);
+  for (int k = 0; k <= M / 2; k++) tw[k] = cis(-2.0L * PI_L * k / M);
+  for (int k = 0; k <= M; k++) twP[k] = cis(-2.0L * PI_L * k / P);
+  for (int k = 0; k <= M; k++) twD[k] = cis(-PI_L * k / (2.0L * P));
+  auto at = [&](size_t o) { return (void*)(base + o); };
+  std::vector<DSpecies> dsp(NS);
+  for (int u = 0; u < NS; u++) {
+    const SpeciesHost& h = sp[u];
+    DSpecies& s = dsp[u];
+    s.n_seg = h.n_seg;
+    s.S = h.S;
+    s.fixed = h.fixed;
+    s.states = (const int*)at(o_states[u]);
+    s.nst = (const int*)at(o_nst[u]);
+    s.md = (const double*)at(o_md[u]);
+    s.fixed_density = h.fixed_density;
+    s.mu_species = h.mu_species;
+    s.normative = h.normative;
+    s.norm_free = h.norm_free;
+    s.lambda_fixed = 1.0;
+    s.gC = h.n_seg > 1 ? (double*)at(o_gC[u]) : nullptr;
+    s.gP = h.n_seg > 1 ? (double*)at(o_gP[u]) : nullptr;
+    s.rho_seg = (double*)at(o_rho[u]);
+  }
+  DReq r{};
+  r.NP = P;
+  r.M = M;
+  r.L = L;
+  r.NB = NB;
+  r.MB = MB;
+  r.NS = NS;
+  r.funcs = (int)d->functionals;
+  r.dz = d->bin_width;
+  r.lB = d->bjerrum_length;
+  r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
+  r.n = (long long)P * (NB + 2 * MB + 1) + 1;
+  r.sig = (const double*)at(o_sig);
+  r.z = (const double*)at(o_z);
+  r.dmu = (const double*)at(o_dmu);
+  r.bonds = (const int*)at(o_bonds);
+  r.sp = (const DSpecies*)at(o_sp);
+  r.Ext = (const double*)at(o_Ext);
+  r.trapez = (const double*)at(o_tr);
+  r.Csurf = (const double*)at(o_Csurf);
+  r.Wbond = (const double*)at(o_Wbond);
+  r.Wfmt = (const double*)at(o_Wfmt);
+  r.Wmsa = (const double*)at(o_Wmsa);
+  r.Wcoul = (const double*)at(o_Wcoul);
+  r.tw = (const double2*)at(o_tw);
+  r.twP = (const double2*)at(o_twP);
+  r.twD = (const double2*)at(o_twD);
+  r.x = const_cast<double*>(x_dev);  // read only in G(x)
+  r.g = g_dev;
+  r.lambda = (double*)at(o_lam);
+  r.rho_beads = (double*)at(o_rb);
+  r.rho_bonds = (double*)at(o_rbo);
+  r.Cb = (double*)at(o_Cb);
+  r.Cbond = (double*)at(o_Cbond);
+  r.Cmu = (double*)at(o_Cmu);
+  r.Clng = (double*)at(o_Clng);
+  r.wa = (double*)at(o_wa);
+  r.wb = (double*)at(o_wb);
+  r.wc = (double*)at(o_wc);
+  r.hx = nullptr;
+  r.hg = nullptr;
+  r.lsq_u = nullptr;
+  r.status = (int*)at(o_status);
+  r.iters = (int*)at(o_iters);
+  r.err = (double*)at(o_err);
+  r.scal = (double*)at(o_scal);
+  // the array keeps the previous call's contents: clear the region this call uses
+  CUDA_TRY(cudaMemsetAsync(base, 0, lay.off, stream));
+  auto up = [&](size_t o, const void* src, size_t nbytes) {
+    return cudaMemcpyAsync(base + o, src, nbytes, cudaMemcpyHostToDevice, stream);
+  };
+  CUDA_TRY(up(o_sig, d->diameter, sizeof(double) * NB));
+  CUDA_TRY(up(o_z, d->valence, sizeof(double) * NB));
+  CUDA_TRY(up(o_dmu, d->delta_muH, sizeof(double) * NB));
+  if (MB) CUDA_TRY(up(o_bonds, bonds.data(), sizeof(int) * 2 * MB));
+  for (int u = 0; u < NS; u++) {
+    CUDA_TRY(up(o_states[u], sp[u].states.data(), sizeof(int) * sp[u].states.size()));
+    CUDA_TRY(up(o_nst[u], sp[u].nst.data(), sizeof(int) * sp[u].nst.size()));
+    CUDA_TRY(up(o_md[u], sp[u].md.data(), sizeof(double) * sp[u].md.size()));
+  }
+  CUDA_TRY(up(o_sp, dsp.data(), sizeof(DSpecies) * NS));
+  CUDA_TRY(up(o_Ext, Ext.data(), sizeof(double) * Ext.size()));
+  CUDA_TRY(up(o_tr, tr.data(), sizeof(double) * tr.size()));
+  CUDA_TRY(up(o_Csurf, Csurf.data(), sizeof(double) * P));
+  CUDA_TRY(up(o_Wbond, Wbond.data(), sizeof(double) * Wbond.size()));
+  CUDA_TRY(up(o_Wfmt, Wfmt.data(), sizeof(double) * Wfmt.size()));
+  CUDA_TRY(up(o_Wmsa, Wmsa.data(), sizeof(double) * Wmsa.size()));
+  CUDA_TRY(up(o_Wcoul, Wcoul.data(), sizeof(double) * P));
+  CUDA_TRY(up(o_tw, tw.data(), sizeof(double2) * tw.size()));
+  CUDA_TRY(up(o_twP, twP.data(), sizeof(double2) * twP.size()));
+  CUDA_TRY(up(o_twD, twD.data(), sizeof(double2) * twD.size()));
+  CUDA_TRY(up(o_dreq, &r, sizeof(DReq)));
+  size_t sm = smem_bytes(M);
+  rc = prepare_kernel((const void*)sdft_k_objective, sm);
+  if (rc) return rc;
+  sdft_k_objective<<<1, kThreads, sm, stream>>>((const DReq*)at(o_dreq));
+  CUDA_TRY(cudaGetLastError());
+  int st = 0;
+  CUDA_TRY(cudaMemcpyAsync(&st, r.status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CUDA_TRY(cudaStreamSynchronize(stream));
+  if (st == ST_NORM) return set_err(SDFT_ERR_NORM, "Normalization error: lambda <= 0 or not finite");
+  return SDFT_OK;
+}

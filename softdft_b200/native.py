@@ -168,3 +168,13 @@ def last_batch_stats(n: int = 0):
     lat = np.zeros(max(n, 1))
     lib().sdft_last_batch_stats(C.byref(ms), C.byref(launches), _p(lat), n)
     return float(ms.value), int(launches.value), lat[:n]
+
+
+def objective_noalloc(d: Descriptor, x_dev_ptr: int, g_dev_ptr: int, stream_ptr: int = 0) -> None:
+    """G(x) through sdft_objective_noalloc: no device allocation by the library;
+    x and G(x) are the caller's device arrays (n doubles each, raw pointers)."""
+    L = lib()
+    f = L.sdft_objective_noalloc
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    _check(f(C.byref(d.desc), C.c_void_p(x_dev_ptr), C.c_void_p(g_dev_ptr), C.c_void_p(stream_ptr or None)))
