@@ -171,6 +171,10 @@ typedef struct species_t {
   double* rho_seg;      /* [(seg*S + idx)*NP + K] */
   double* gC;           /* (K, j, c, i, seg) */
   double* gP;           /* (K, j, i, seg) */
+  int linear;           /* parent of segment g is g-1 */
+  int* eC;              /* [seg] power-of-two exponent carried by the stored gC of seg */
+  int* eP;              /* [seg] the same for gP */
+  int scaled;           /* some exponent of this evaluation is non-zero */
 } species_t;
 
 struct oracle_sys {
@@ -329,7 +333,7 @@ static void eval_external_field(oracle_sys* o) {
 static void species_free(species_t* s) {
   free(s->parent); free(s->n_states); free(s->states); free(s->n_children); free(s->children);
   free(s->level_start); free(s->level_seg); free(s->fixed); free(s->max_distance);
-  free(s->rho_seg); free(s->gC); free(s->gP);
+  free(s->rho_seg); free(s->gC); free(s->gP); free(s->eC); free(s->eP);
 }
 
 void oracle_destroy(oracle_sys* o) {
@@ -476,6 +480,10 @@ int oracle_create(const sdft_system_desc* d, oracle_sys** out) {
         if (s->fixed[g] >= 0) { oracle_destroy(o); return fail(SDFT_ERR_UNSUPPORTED, "only segment 0 can be fixed"); }
       if (n < 2) { oracle_destroy(o); return fail(SDFT_ERR_UNSUPPORTED, "a fixed species needs a free segment"); }
     }
+    s->linear = 1;
+    for (int g = 1; g < n; g++) s->linear &= s->parent[g] == g - 1;
+    s->eC = calloc((size_t)n, sizeof(int));
+    s->eP = calloc((size_t)n, sizeof(int));
     s->rho_seg = calloc((size_t)NP * S * n, sizeof(double));
     s->gC = calloc((size_t)NP * S * C * S * n, sizeof(double));
     s->gP = calloc((size_t)NP * S * S * n, sizeof(double));
@@ -609,11 +617,30 @@ static void convolve_bond(oracle_sys* o, int bond) {
   fft_exec(&o->plan, o->f_hat, 1);
 }
 
+/* Per-segment renormalisation (linear chains).  The reference scales chain
+   propagators only by `normative`; products over ~100+ segments underflow
+   (e^-700) and the density prefactor e^{mu_species} overflows.  When the largest
+   propagator entry of a segment leaves [2^-400, 2^400] the segment's entries are
+   divided by the power of two 2^e that brings the maximum into [0.5, 1) (an
+   exact scaling) and e is carried; otherwise e = 0 and the arithmetic is the
+   reference's.  Returns e. */
+static int renormalise(double* a, size_t count) {
+  double mx = 0.0;
+  for (size_t q = 0; q < count; q++) mx = fmax(mx, fabs(a[q]));
+  if (!(mx > 0.0) || !isfinite(mx)) return 0;
+  if (mx >= 0x1p-400 && mx <= 0x1p400) return 0;
+  int e;
+  frexp(mx, &e);
+  for (size_t q = 0; q < count; q++) a[q] = ldexp(a[q], -e);
+  return e;
+}
+
 static void compute_child_propagators(oracle_sys* o, species_t* s) {
   int NP = o->NP, S = s->S;
   const double* lng = o->x + (size_t)NP * o->NB;
   double normative = normative_of(o, s);
   memset(s->gC, 0, sizeof(double) * (size_t)NP * S * s->C * S * s->n_seg);
+  memset(s->eC, 0, sizeof(int) * (size_t)s->n_seg);
   for (int l = s->n_levels - 1; l >= 0; l--) {
     for (int q = s->level_start[l]; q < s->level_start[l + 1]; q++) {
       int parent = s->level_seg[q];
@@ -691,6 +718,11 @@ static void compute_child_propagators(oracle_sys* o, species_t* s) {
           }
         }
       }
+      if (s->linear && s->n_children[parent] > 0) {
+        int e = renormalise(s->gC + gC_idx(o, s, 0, 0, 0, 0, parent), (size_t)NP * S * s->C * S);
+        s->eC[parent] = e + s->eC[parent + 1];
+        if (e) s->scaled = 1;
+      }
     }
   }
 }
@@ -700,6 +732,7 @@ static int compute_parent_propagators(oracle_sys* o, species_t* s) {
   const double* lng = o->x + (size_t)NP * o->NB;
   double normative = normative_of(o, s);
   memset(s->gP, 0, sizeof(double) * (size_t)NP * S * S * s->n_seg);
+  memset(s->eP, 0, sizeof(int) * (size_t)s->n_seg);
   for (int l = 0; l < s->n_levels; l++) {
     for (int q = s->level_start[l]; q < s->level_start[l + 1]; q++) {
       int child = s->level_seg[q];
@@ -756,12 +789,19 @@ static int compute_parent_propagators(oracle_sys* o, species_t* s) {
             for (int i = 0; i < S; i++)
               for (int j = 0; j < S; j++) s->gP[gP_idx(o, s, K1, j, i, child)] = 0.0;
       }
+      if (s->linear && child > 0) {
+        int e = renormalise(s->gP + gP_idx(o, s, 0, 0, 0, child), (size_t)NP * S * S);
+        s->eP[child] = e + s->eP[child - 1];
+        if (e) s->scaled = 1;
+      }
     }
   }
   return SDFT_OK;
 }
 
-/* handle_fixed.jl:1-120 -> norm; sets the species' mu to 0 when grafted */
+/* handle_fixed.jl:1-120 -> norm; sets the species' mu to 0 when grafted.  With
+   renormalised propagators lambda is computed from the scaled segment-1 entries;
+   the carried exponent enters accumulate_densities through log_prefactor. */
 static int handle_fixed(oracle_sys* o, species_t* s, double* norm_out) {
   int NP = o->NP, S = s->S;
   double normative = normative_of(o, s);
@@ -814,17 +854,32 @@ static int handle_fixed(oracle_sys* o, species_t* s, double* norm_out) {
   return SDFT_OK;
 }
 
+/* ln of the density prefactor of segment g when propagators were renormalised:
+   norm e^{mu} 2^{eP_g + eC_g} (free chains: norm = normative^(N-1); grafted:
+   norm = density / lambda with lambda carrying 2^{eP_1 + eC_1}) */
+static double log_prefactor(const species_t* s, double norm, double normative, int g) {
+  int sg = s->eP[g] + (g < s->n_seg - 1 ? s->eC[g] : 0);
+  if (s->any_fixed) {
+    int s1 = s->eP[1] + (1 < s->n_seg - 1 ? s->eC[1] : 0);
+    return log(norm) + s->mu_species + (double)(sg - s1) * 0.6931471805599453;
+  }
+  return s->mu_species + (double)(s->n_seg - 1) * log(normative) + (double)sg * 0.6931471805599453;
+}
+
 /* accumulate_densities! (accumulate_densities.jl:95-184) */
 static void accumulate_densities(oracle_sys* o, species_t* s, double norm) {
   int NP = o->NP, S = s->S;
   double mu = s->mu_species;
+  double normative = normative_of(o, s);
   for (int parent = 0; parent < s->n_seg; parent++) {
     for (int idx_i = 0; idx_i < s->n_states[parent]; idx_i++) {
       int state_i = s->states[parent * S + idx_i];
+      double lp = s->scaled ? log_prefactor(s, norm, normative, parent) : 0.0;
       for (int K = 0; K < NP; K++) {
         double sp = 0.0;
         for (int jj = 0; jj < S; jj++) sp += s->gP[gP_idx(o, s, K, jj, idx_i, parent)];
-        double contr = norm * exp(mu - o->lambda[IDX_MU(o, K, state_i)]) * sp;
+        double contr = s->scaled ? exp(lp - o->lambda[IDX_MU(o, K, state_i)]) * sp
+                                 : norm * exp(mu - o->lambda[IDX_MU(o, K, state_i)]) * sp;
         double temp;
         if (s->n_children[parent] == 0) {
           temp = sum_gC_states(o, s, K, 0, idx_i, parent);
@@ -854,8 +909,10 @@ static void accumulate_densities(oracle_sys* o, species_t* s, double norm) {
     if (parent < 0) continue;
     for (int idx_i = 0; idx_i < s->n_states[child]; idx_i++) {
       int state_i = s->states[child * S + idx_i];
+      double lp = s->scaled ? log_prefactor(s, norm, normative, child) : 0.0;
       for (int K = 0; K < NP; K++) {
-        double contr = norm * exp(mu - o->lambda[IDX_MU(o, K, state_i)]);
+        double contr = s->scaled ? exp(lp - o->lambda[IDX_MU(o, K, state_i)])
+                                 : norm * exp(mu - o->lambda[IDX_MU(o, K, state_i)]);
         for (int gc = 0; gc < s->n_children[child]; gc++) contr *= sum_gC_states(o, s, K, gc, idx_i, child);
         for (int idx_j = 0; idx_j < s->n_states[parent]; idx_j++) {
           int state_j = s->states[parent * S + idx_j];
@@ -883,12 +940,15 @@ static int eval_spatial_density(oracle_sys* o) {
   }
   for (int u = 0; u < o->NS; u++) {
     species_t* s = &o->sp[u];
+    s->scaled = 0;
     compute_child_propagators(o, s);
     int rc = compute_parent_propagators(o, s);
     if (rc) return rc;
     double norm;
     rc = handle_fixed(o, s, &norm);
     if (rc) return rc;
+    /* the reference's prefactor norm e^{mu - lambda} overflows beyond e^709 */
+    if (fabs(s->mu_species) + (double)(s->n_seg - 1) * fabs(log(normative_of(o, s))) > 600.0) s->scaled = 1;
     accumulate_densities(o, s, norm);
   }
   return SDFT_OK;

@@ -20,6 +20,7 @@ constexpr int kMaxStates = 4;        // per-segment state families the device su
 constexpr int kMaxBeads = 32;        // bead types
 constexpr int kMaxBonds = 64;        // bond types
 constexpr int kMaxAnderson = 16;     // Anderson depth m
+constexpr int kMaxTB = 4;            // transforms in flight per CTA
 constexpr double kPi = 3.14159265358979323846;
 
 // status codes written by the kernels (mirror sdft_status)
@@ -47,6 +48,7 @@ struct DSpecies {
   double* gC;         // [(g * S + i) * S + j] * P + K : parent g state i, child g+1 state j
   double* gP;         // [(g * S + i) * S + j] * P + K : child g state i, parent g-1 state j
   double* rho_seg;    // [(g * S + i) * P + K]
+  int* expo;          // [2 * n_seg]: power-of-two exponent carried by gC of g, then by gP of g
 };
 
 struct DReq {
@@ -54,7 +56,7 @@ struct DReq {
   int NP, M, L;       // grid points P, FFT length M = P/2, log2(M)
   int NB, MB, NS;
   int funcs;          // SDFT_FUNC_* bits
-  int n_tau;          // unused (reserved)
+  int TB;             // transform buffers in shared memory for this launch (1..kMaxTB)
   double dz, lB, total_charge;
   long long n;        // Anderson unknowns
   // per-bead / per-bond constants
@@ -89,6 +91,7 @@ struct DReq {
   double* wa;             // [max(NB, 6) * P] scratch (weighted densities, derivatives)
   double* wb;             // [MB * 2 * P]  scratch (bond weighted densities)
   double* wc;             // [max(NB, 6 + MB) * P] scratch (derivative fields)
+  double* wd;             // [2 * NB * P] scratch (per-bead FMT weighted densities)
   // Anderson
   double* hx;             // [m * n] history of x
   double* hg;             // [m * n] history of G(x) - x

@@ -1,5 +1,6 @@
 // fft.cuh -- CTA-wide DCT-II / inverse-DCT-II of P real points through one
-// complex FFT of M = P/2 points held in shared memory.
+// complex FFT of M = P/2 points held in shared memory, several transforms at
+// a time.
 //
 // The reference convolves every field on a mirrored, doubled grid of 2P
 // points with complex FFTs (src/iDFT/coordinate_system/Cartesian/process_fourier.jl:15-49,
@@ -13,21 +14,51 @@
 // Makhoul's reordering and a real FFT of P points, i.e. a complex FFT of P/2
 // points (J. Makhoul, IEEE TASSP 28(1), 1980).
 //
-// Shared buffer: z[M] double2.  Forward: the load scatters into bit-reversed
-// order, a radix-2 decimation-in-time FFT leaves z in natural order.  Inverse:
-// a decimation-in-frequency IFFT takes natural order and leaves bit-reversed
-// order, undone by the gather of the store.  No permutation pass is needed.
+// Shared memory holds TB transform buffers of M complex values each, padded by
+// one slot every 8 (index i lives at i + i/8) so that the strided accesses of
+// the butterfly passes fall on different banks.  Forward: the load scatters into
+// bit-reversed order and radix-8/4/2 decimation-in-time passes (three radix-2
+// stages per pass, in registers) leave natural order.  Inverse: radix-8/4/2
+// decimation-in-frequency passes take natural order and leave bit-reversed
+// order, undone by the gather of the store.  The DCT twiddle step only couples
+// Z[k] and Z[M-k], so a convolution is: load, FFT, one in-place pair pass that
+// also applies the weight, IFFT, store.
 //
-// Every butterfly of the pair step (k, M-k) only touches Z[k] and Z[M-k], so a
-// whole convolution is: load, FFT, one in-place pair pass, IFFT, store.
+// Batched entry points run nT <= TB independent transforms in the same passes
+// (transform t uses buffer t); the functors take the transform index.
 #pragma once
 
 #include "common.cuh"
 
 namespace sdft {
 
+__device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
+
 __device__ __forceinline__ int brev_bits(int m, int L) {
   return L == 0 ? 0 : (int)(__brev((unsigned)m) >> (32 - L));
+}
+
+struct FftCtx {
+  double2* z;        // TB buffers of `stride` slots
+  int stride;        // M + M/8
+  int P, M, L, H;    // H = M/2
+  const double2* __restrict__ tw;   // [M/2] e^{-2 pi i k / M}
+  const double2* __restrict__ twP;  // [M+1] e^{-2 pi i k / P}
+  const double2* __restrict__ twD;  // [M+1] e^{-i pi k / 2P}
+};
+
+__device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
+  FftCtx c;
+  c.z = z;
+  c.M = r.M;
+  c.L = r.L;
+  c.P = r.NP;
+  c.H = r.M >> 1;
+  c.stride = r.M + (r.M >> 3);
+  c.tw = r.tw;
+  c.twP = r.twP;
+  c.twD = r.twD;
+  return c;
 }
 
 // position of real sample K in the packed complex buffer: (bit-reversed index, component)
@@ -37,66 +68,172 @@ __device__ __forceinline__ void dct_slot(int K, int P, int L, int* pos, int* com
   *comp = q & 1;
 }
 
-// z <- (bit-reversed) packed reorder of x, x[K] = f(K)
 template <class F>
-__device__ __forceinline__ void dct_load(double2* z, int P, int L, F f) {
-  double* zd = reinterpret_cast<double*>(z);
-  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+__device__ __forceinline__ void load_b(const FftCtx& c, int nT, F f) {
+  const int lp = c.L + 1;  // log2 P
+  for (int it = threadIdx.x; it < (nT << lp); it += blockDim.x) {
+    const int t = it >> lp, K = it & (c.P - 1);
     int pos, comp;
-    dct_slot(K, P, L, &pos, &comp);
-    zd[2 * pos + comp] = f(K);
+    dct_slot(K, c.P, c.L, &pos, &comp);
+    reinterpret_cast<double*>(c.z + (size_t)t * c.stride + fpad(pos))[comp] = f(t, K);
   }
 }
 
-// radix-2 DIT on bit-reversed input -> natural output (forward, e^{-i})
-__device__ __forceinline__ void fft_dit(double2* z, int M, int L, const double2* __restrict__ tw) {
-  const int half_n = M >> 1;
-  for (int s = 0; s < L; s++) {
-    __syncthreads();
+template <class S>
+__device__ __forceinline__ void store_b(const FftCtx& c, int nT, double scale, S st) {
+  const int lp = c.L + 1;
+  for (int it = threadIdx.x; it < (nT << lp); it += blockDim.x) {
+    const int t = it >> lp, K = it & (c.P - 1);
+    int pos, comp;
+    dct_slot(K, c.P, c.L, &pos, &comp);
+    st(t, K, reinterpret_cast<const double*>(c.z + (size_t)t * c.stride + fpad(pos))[comp] * scale);
+  }
+}
+
+__device__ __forceinline__ void bfly(double2& a, double2& b, double2 w) {  // DIT: (a + wb, a - wb)
+  const double2 wb = cmul(b, w);
+  b = sub2(a, wb);
+  a = add2(a, wb);
+}
+__device__ __forceinline__ void bfly_dif(double2& a, double2& b, double2 w) {  // DIF: (a + b, (a - b) w)
+  const double2 d = sub2(a, b);
+  a = add2(a, b);
+  b = cmul(d, w);
+}
+
+// forward FFT of nT buffers: bit-reversed input -> natural output
+__device__ __forceinline__ void fft_fwd_b(const FftCtx& c, int nT) {
+  const int M = c.M, L = c.L;
+  for (int s = 0; s < L;) {
+    const int rr = min(3, L - s);
     const int h = 1 << s;
-    for (int b = threadIdx.x; b < half_n; b += blockDim.x) {
-      int pos = b & (h - 1);
-      int i = ((b >> s) << (s + 1)) + pos;
-      int j = i + h;
-      double2 w = __ldg(&tw[pos << (L - 1 - s)]);
-      double2 a = z[i];
-      double2 c = cmul(z[j], w);
-      z[i] = add2(a, c);
-      z[j] = sub2(a, c);
+    __syncthreads();
+    if (rr == 3) {
+      const int per = M >> 3, lper = L - 3;
+      for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
+        const int t = it >> lper, u = it & (per - 1);
+        double2* zb = c.z + (size_t)t * c.stride;
+        const int p = u & (h - 1);
+        const int base = ((u >> s) << (s + 3)) + p;
+        double2 x[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) x[j] = zb[fpad(base + j * h)];
+        const double2 w1 = __ldg(&c.tw[p << (L - 1 - s)]);
+#pragma unroll
+        for (int m = 0; m < 4; m++) bfly(x[2 * m], x[2 * m + 1], w1);
+        const double2 w2a = __ldg(&c.tw[p << (L - 2 - s)]);
+        const double2 w2b = __ldg(&c.tw[(p + h) << (L - 2 - s)]);
+        bfly(x[0], x[2], w2a);
+        bfly(x[1], x[3], w2b);
+        bfly(x[4], x[6], w2a);
+        bfly(x[5], x[7], w2b);
+#pragma unroll
+        for (int j = 0; j < 4; j++) bfly(x[j], x[j + 4], __ldg(&c.tw[(p + j * h) << (L - 3 - s)]));
+#pragma unroll
+        for (int j = 0; j < 8; j++) zb[fpad(base + j * h)] = x[j];
+      }
+    } else if (rr == 2) {
+      const int per = M >> 2, lper = L - 2;
+      for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
+        const int t = it >> lper, u = it & (per - 1);
+        double2* zb = c.z + (size_t)t * c.stride;
+        const int p = u & (h - 1);
+        const int base = ((u >> s) << (s + 2)) + p;
+        double2 x[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) x[j] = zb[fpad(base + j * h)];
+        const double2 w1 = __ldg(&c.tw[p << (L - 1 - s)]);
+        bfly(x[0], x[1], w1);
+        bfly(x[2], x[3], w1);
+        bfly(x[0], x[2], __ldg(&c.tw[p << (L - 2 - s)]));
+        bfly(x[1], x[3], __ldg(&c.tw[(p + h) << (L - 2 - s)]));
+#pragma unroll
+        for (int j = 0; j < 4; j++) zb[fpad(base + j * h)] = x[j];
+      }
+    } else {
+      const int per = M >> 1, lper = L - 1;
+      for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
+        const int t = it >> lper, u = it & (per - 1);
+        double2* zb = c.z + (size_t)t * c.stride;
+        const int p = u & (h - 1);
+        const int base = ((u >> s) << (s + 1)) + p;
+        double2 a = zb[fpad(base)], b = zb[fpad(base + h)];
+        bfly(a, b, __ldg(&c.tw[p << (L - 1 - s)]));
+        zb[fpad(base)] = a;
+        zb[fpad(base + h)] = b;
+      }
     }
+    s += rr;
   }
   __syncthreads();
 }
 
-// radix-2 DIF inverse on natural input -> bit-reversed output (e^{+i}, unscaled)
-__device__ __forceinline__ void ifft_dif(double2* z, int M, int L, const double2* __restrict__ tw) {
-  const int half_n = M >> 1;
-  for (int s = L - 1; s >= 0; s--) {
+// inverse FFT of nT buffers (unscaled): natural input -> bit-reversed output
+__device__ __forceinline__ void fft_inv_b(const FftCtx& c, int nT) {
+  const int M = c.M, L = c.L;
+  for (int top = L; top > 0;) {
+    const int rr = min(3, top);
+    const int s0 = top - rr;
+    const int h = 1 << s0;
     __syncthreads();
-    const int h = 1 << s;
-    for (int b = threadIdx.x; b < half_n; b += blockDim.x) {
-      int pos = b & (h - 1);
-      int i = ((b >> s) << (s + 1)) + pos;
-      int j = i + h;
-      double2 w = conj2(__ldg(&tw[pos << (L - 1 - s)]));
-      double2 a = z[i];
-      double2 c = z[j];
-      z[i] = add2(a, c);
-      z[j] = cmul(sub2(a, c), w);
+    if (rr == 3) {
+      const int per = M >> 3, lper = L - 3;
+      for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
+        const int t = it >> lper, u = it & (per - 1);
+        double2* zb = c.z + (size_t)t * c.stride;
+        const int p = u & (h - 1);
+        const int base = ((u >> s0) << (s0 + 3)) + p;
+        double2 x[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) x[j] = zb[fpad(base + j * h)];
+#pragma unroll
+        for (int j = 0; j < 4; j++) bfly_dif(x[j], x[j + 4], conj2(__ldg(&c.tw[(p + j * h) << (L - 3 - s0)])));
+        const double2 w2a = conj2(__ldg(&c.tw[p << (L - 2 - s0)]));
+        const double2 w2b = conj2(__ldg(&c.tw[(p + h) << (L - 2 - s0)]));
+        bfly_dif(x[0], x[2], w2a);
+        bfly_dif(x[1], x[3], w2b);
+        bfly_dif(x[4], x[6], w2a);
+        bfly_dif(x[5], x[7], w2b);
+        const double2 w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
+#pragma unroll
+        for (int m = 0; m < 4; m++) bfly_dif(x[2 * m], x[2 * m + 1], w1);
+#pragma unroll
+        for (int j = 0; j < 8; j++) zb[fpad(base + j * h)] = x[j];
+      }
+    } else if (rr == 2) {
+      const int per = M >> 2, lper = L - 2;
+      for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
+        const int t = it >> lper, u = it & (per - 1);
+        double2* zb = c.z + (size_t)t * c.stride;
+        const int p = u & (h - 1);
+        const int base = ((u >> s0) << (s0 + 2)) + p;
+        double2 x[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) x[j] = zb[fpad(base + j * h)];
+        bfly_dif(x[0], x[2], conj2(__ldg(&c.tw[p << (L - 2 - s0)])));
+        bfly_dif(x[1], x[3], conj2(__ldg(&c.tw[(p + h) << (L - 2 - s0)])));
+        const double2 w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
+        bfly_dif(x[0], x[1], w1);
+        bfly_dif(x[2], x[3], w1);
+#pragma unroll
+        for (int j = 0; j < 4; j++) zb[fpad(base + j * h)] = x[j];
+      }
+    } else {
+      const int per = M >> 1, lper = L - 1;
+      for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
+        const int t = it >> lper, u = it & (per - 1);
+        double2* zb = c.z + (size_t)t * c.stride;
+        const int p = u & (h - 1);
+        const int base = ((u >> s0) << (s0 + 1)) + p;
+        double2 a = zb[fpad(base)], b = zb[fpad(base + h)];
+        bfly_dif(a, b, conj2(__ldg(&c.tw[p << (L - 1 - s0)])));
+        zb[fpad(base)] = a;
+        zb[fpad(base + h)] = b;
+      }
     }
+    top = s0;
   }
   __syncthreads();
-}
-
-// y[K] = scale * iDCT2 sample K; g(K, y)
-template <class G>
-__device__ __forceinline__ void dct_store(const double2* z, int P, int L, double scale, G g) {
-  const double* zd = reinterpret_cast<const double*>(z);
-  for (int K = threadIdx.x; K < P; K += blockDim.x) {
-    int pos, comp;
-    dct_slot(K, P, L, &pos, &comp);
-    g(K, zd[2 * pos + comp] * scale);
-  }
 }
 
 // ---- pair step ------------------------------------------------------------
@@ -158,101 +295,116 @@ __device__ __forceinline__ double2 mid_inverse(double eh, double ePh, double2 dh
   return conj2(V);
 }
 
+// pair items: it -> (t, k) with k in [0, H); k = 0 also handles k = H
+#define SDFT_PAIR_LOOP(c, nT)                                           \
+  const int lH_ = (c).L - 1;                                            \
+  for (int it = threadIdx.x; it < ((nT) << lH_); it += blockDim.x) {   \
+    const int t = it >> lH_, k = it & ((c).H - 1);                      \
+    double2* zb = (c).z + (size_t)t * (c).stride;
+
 // ---- whole transforms ------------------------------------------------------
 
-// C[q] for q in [0, P): forward DCT-II of f; emit(q, C[q]) for every q (C[P] is not emitted).
+// C[q] for q in [0, P): forward DCT-II of f(t, .); emit(t, q, C[q])
 template <class F, class E>
-__device__ __forceinline__ void dct2_forward(double2* z, const DReq& r, F f, E emit) {
-  const int P = r.NP, M = r.M, L = r.L;
+__device__ __forceinline__ void dct2_forward_b(const FftCtx& c, int nT, F f, E emit) {
+  const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
-  dct_load(z, P, L, f);
-  fft_dit(z, M, L, r.tw);
-  const int H = M >> 1;
-  for (int k = threadIdx.x; k <= H; k += blockDim.x) {
-    if (k == 0) {
-      double c0, cM;
-      zero_forward(z[0], __ldg(&r.twD[M]), &c0, &cM);
-      emit(0, c0);
-      emit(M, cM);
-    } else if (k == H) {
-      double ch, cPh;
-      mid_forward(z[H], __ldg(&r.twD[H]), &ch, &cPh);
-      emit(H, ch);
-      emit(P - H, cPh);
-    } else {
-      Quad q = pair_forward(z[k], z[M - k], __ldg(&r.twP[k]), __ldg(&r.twD[k]), __ldg(&r.twD[M - k]));
-      emit(k, q.c0);
-      emit(P - k, q.c1);
-      emit(M - k, q.c2);
-      emit(M + k, q.c3);
-    }
+  load_b(c, nT, f);
+  fft_fwd_b(c, nT);
+  SDFT_PAIR_LOOP(c, nT)
+  if (k == 0) {
+    double c0, cM;
+    zero_forward(zb[0], __ldg(&c.twD[M]), &c0, &cM);
+    emit(t, 0, c0);
+    emit(t, M, cM);
+    double ch, cPh;
+    mid_forward(zb[fpad(H)], __ldg(&c.twD[H]), &ch, &cPh);
+    emit(t, H, ch);
+    emit(t, P - H, cPh);
+  } else {
+    Quad q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], __ldg(&c.twP[k]), __ldg(&c.twD[k]), __ldg(&c.twD[M - k]));
+    emit(t, k, q.c0);
+    emit(t, P - k, q.c1);
+    emit(t, M - k, q.c2);
+    emit(t, M + k, q.c3);
   }
-  __syncthreads();
+}
+__syncthreads();
 }
 
-// y = iDCT2(E), E[q] = get(q) for q in [0, P); store(K, y[K])
+// y = iDCT2(E_t), E_t[q] = get(t, q); store(t, K, y[K])
 template <class G, class S>
-__device__ __forceinline__ void dct2_inverse(double2* z, const DReq& r, G get, S store) {
-  const int P = r.NP, M = r.M, L = r.L;
-  const int H = M >> 1;
+__device__ __forceinline__ void dct2_inverse_b(const FftCtx& c, int nT, G get, S store) {
+  const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
-  for (int k = threadIdx.x; k <= H; k += blockDim.x) {
-    if (k == 0) {
-      z[0] = zero_inverse(get(0), get(M), __ldg(&r.twD[M]));
-    } else if (k == H) {
-      z[H] = mid_inverse(get(H), get(P - H), __ldg(&r.twD[H]));
-    } else {
-      Quad e;
-      e.c0 = get(k);
-      e.c1 = get(P - k);
-      e.c2 = get(M - k);
-      e.c3 = get(M + k);
-      double2 a, b;
-      pair_inverse(e, __ldg(&r.twP[k]), __ldg(&r.twD[k]), __ldg(&r.twD[M - k]), &a, &b);
-      z[k] = a;
-      z[M - k] = b;
-    }
+  SDFT_PAIR_LOOP(c, nT)
+  if (k == 0) {
+    zb[0] = zero_inverse(get(t, 0), get(t, M), __ldg(&c.twD[M]));
+    zb[fpad(H)] = mid_inverse(get(t, H), get(t, P - H), __ldg(&c.twD[H]));
+  } else {
+    Quad e;
+    e.c0 = get(t, k);
+    e.c1 = get(t, P - k);
+    e.c2 = get(t, M - k);
+    e.c3 = get(t, M + k);
+    double2 a, b;
+    pair_inverse(e, __ldg(&c.twP[k]), __ldg(&c.twD[k]), __ldg(&c.twD[M - k]), &a, &b);
+    zb[fpad(k)] = a;
+    zb[fpad(M - k)] = b;
   }
-  ifft_dif(z, M, r.L, r.tw);
-  dct_store(z, P, L, 1.0 / (double)M, store);
-  __syncthreads();
+}
+fft_inv_b(c, nT);
+store_b(c, nT, 1.0 / (double)M, store);
+__syncthreads();
 }
 
-// y = iDCT2(W .* DCT2(f)); W[q] = wgt(q); store(K, y[K])
+// y = iDCT2(W_t .* DCT2(f_t)); W_t[q] = wgt(t, q); store(t, K, y[K])
 template <class F, class W, class S>
-__device__ __forceinline__ void dct2_convolve(double2* z, const DReq& r, F f, W wgt, S store) {
-  const int P = r.NP, M = r.M, L = r.L;
-  const int H = M >> 1;
+__device__ __forceinline__ void dct2_convolve_b(const FftCtx& c, int nT, F f, W wgt, S store) {
+  const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
-  dct_load(z, P, L, f);
-  fft_dit(z, M, L, r.tw);
-  for (int k = threadIdx.x; k <= H; k += blockDim.x) {
-    if (k == 0) {
-      double2 dM = __ldg(&r.twD[M]);
-      double c0, cM;
-      zero_forward(z[0], dM, &c0, &cM);
-      z[0] = zero_inverse(c0 * wgt(0), cM * wgt(M), dM);
-    } else if (k == H) {
-      double2 dh = __ldg(&r.twD[H]);
-      double ch, cPh;
-      mid_forward(z[H], dh, &ch, &cPh);
-      z[H] = mid_inverse(ch * wgt(H), cPh * wgt(P - H), dh);
-    } else {
-      double2 wk = __ldg(&r.twP[k]), dk = __ldg(&r.twD[k]), dk2 = __ldg(&r.twD[M - k]);
-      Quad q = pair_forward(z[k], z[M - k], wk, dk, dk2);
-      q.c0 *= wgt(k);
-      q.c1 *= wgt(P - k);
-      q.c2 *= wgt(M - k);
-      q.c3 *= wgt(M + k);
-      double2 a, b;
-      pair_inverse(q, wk, dk, dk2, &a, &b);
-      z[k] = a;
-      z[M - k] = b;
-    }
+  load_b(c, nT, f);
+  fft_fwd_b(c, nT);
+  SDFT_PAIR_LOOP(c, nT)
+  if (k == 0) {
+    const double2 dM = __ldg(&c.twD[M]);
+    double c0, cM;
+    zero_forward(zb[0], dM, &c0, &cM);
+    const double2 dh = __ldg(&c.twD[H]);
+    double ch, cPh;
+    mid_forward(zb[fpad(H)], dh, &ch, &cPh);
+    zb[0] = zero_inverse(c0 * wgt(t, 0), cM * wgt(t, M), dM);
+    zb[fpad(H)] = mid_inverse(ch * wgt(t, H), cPh * wgt(t, P - H), dh);
+  } else {
+    const double2 wk = __ldg(&c.twP[k]), dk = __ldg(&c.twD[k]), dk2 = __ldg(&c.twD[M - k]);
+    Quad q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], wk, dk, dk2);
+    q.c0 *= wgt(t, k);
+    q.c1 *= wgt(t, P - k);
+    q.c2 *= wgt(t, M - k);
+    q.c3 *= wgt(t, M + k);
+    double2 a, b;
+    pair_inverse(q, wk, dk, dk2, &a, &b);
+    zb[fpad(k)] = a;
+    zb[fpad(M - k)] = b;
   }
-  ifft_dif(z, M, L, r.tw);
-  dct_store(z, P, L, 1.0 / (double)M, store);
-  __syncthreads();
+}
+fft_inv_b(c, nT);
+store_b(c, nT, 1.0 / (double)M, store);
+__syncthreads();
+}
+
+#undef SDFT_PAIR_LOOP
+
+// ---- single-transform wrappers -----------------------------------------
+template <class F, class E>
+__device__ __forceinline__ void dct2_forward(const FftCtx& c, F f, E emit) {
+  dct2_forward_b(
+      c, 1, [&](int, int K) { return f(K); }, [&](int, int q, double v) { emit(q, v); });
+}
+template <class G, class S>
+__device__ __forceinline__ void dct2_inverse(const FftCtx& c, G get, S store) {
+  dct2_inverse_b(
+      c, 1, [&](int, int q) { return get(q); }, [&](int, int K, double y) { store(K, y); });
 }
 
 }  // namespace sdft

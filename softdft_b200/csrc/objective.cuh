@@ -22,8 +22,8 @@
 namespace sdft {
 
 struct Shared {
-  double2* z;   // M complex
-  double* red;  // 512 doubles
+  double2* z;   // TB transform buffers (fft.cuh)
+  double* red;  // 1024 doubles
 };
 
 __device__ __forceinline__ const double* xs_mu(const DReq& r, const double* x) { return x; }
@@ -64,17 +64,44 @@ __device__ void stage_lambda(const DReq& r) {
 
 // ---------------------------------------------------------------------------
 // chain propagators
+//
+// Per-segment renormalisation: the reference scales propagators only by
+// `normative`, so products over ~100+ segments underflow and the density
+// prefactor e^{mu_species} overflows.  When the largest entry of a segment's
+// propagators leaves [2^-400, 2^400] the entries are divided by the power of two
+// 2^e that brings the maximum into [0.5, 1) -- an exact scaling -- and e is
+// carried (expo); otherwise e = 0 and the arithmetic is the reference's.
 // ---------------------------------------------------------------------------
-__device__ void chain_child(const DReq& r, const DSpecies& s, Shared sh) {
+__device__ int renormalise_block(double* a, int count_per_K, int P, double* red) {
+  double mx = 0.0;
+  for (int K = threadIdx.x; K < P; K += blockDim.x)
+    for (int q = 0; q < count_per_K; q++) mx = fmax(mx, fabs(a[(size_t)q * P + K]));
+  mx = block_max(mx, red);
+  if (!(mx > 0.0) || !isfinite(mx)) return 0;
+  if (mx >= 0x1p-400 && mx <= 0x1p400) return 0;
+  int e;
+  frexp(mx, &e);
+  for (int K = threadIdx.x; K < P; K += blockDim.x)
+    for (int q = 0; q < count_per_K; q++) a[(size_t)q * P + K] = ldexp(a[(size_t)q * P + K], -e);
+  __syncthreads();
+  return e;
+}
+
+__device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
   const int P = r.NP, S = s.S, N = s.n_seg;
+  bool scaled = false;
+  int e_child = 0;  // exponent carried by gC of segment p + 1 (the leaf carries none)
   const double* lng = xs_lng(r, r.x);
   const double inv_norm = 1.0 / s.normative;
+  const FftCtx fc = make_fft(sh.z, r);
   for (int p = N - 2; p >= 0; p--) {
     const int c = p + 1;
-    for (int ii = 0; ii < s.nst[p]; ii++) {
-      const int si = s.states[p * S + ii];
-      for (int jj = 0; jj < s.nst[c]; jj++) {
-        const int sj = s.states[c * S + jj];
+    const int nc = s.nst[c];
+    const int npair = s.nst[p] * nc;
+    if (p == 0 && s.fixed >= 0) {
+      for (int pi = 0; pi < npair; pi++) {
+        const int ii = pi / nc, jj = pi - ii * nc;
+        const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
         const int bond = bond_of(r, si, sj);
         const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
         double* out = s.gC + ((size_t)(p * S + ii) * S + jj) * P;
@@ -83,39 +110,66 @@ __device__ void chain_child(const DReq& r, const DSpecies& s, Shared sh) {
         const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
         const double* tr_j = r.trapez + (size_t)sj * P;
         const double* gcc = (c < N - 1) ? s.gC + ((size_t)(c * S + jj) * S) * P : nullptr;
-        auto fchild = [&](int K) {
-          double f = exp(-lam_j[K] + lng_pj[K] / 2.0);
-          if (gcc) {
-            double t = 0.0;
-            for (int q = 0; q < S; q++) t += gcc[(size_t)q * P + K];
-            f *= t;
-          }
-          return f;
-        };
-        if (p == 0 && s.fixed >= 0) {
-          // parent grafted, child free: local sum within sigma_ij (child_propagators.jl:91-116)
-          const int Kp = s.fixed;
-          const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
-          const double Dij2 = Dij * Dij;
-          const double renorm = 2.0 * Dij;
-          const double el = exp(lng_pi[Kp] / 2.0);
-          double acc = 0.0;
-          for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
-            double d2 = dist2_grid(K1, Kp, r.dz);
-            if (d2 <= Dij2) {
-              double t = fabs(fchild(K1)) * el * r.dz * tr_j[K1] / renorm;
-              if (fabs(d2 - Dij2) <= 1e-6) t /= 2.0;
-              acc += t / s.normative;
+        // parent grafted, child free: local sum within sigma_ij (child_propagators.jl:91-116)
+        const int Kp = s.fixed;
+        const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
+        const double Dij2 = Dij * Dij;
+        const double renorm = 2.0 * Dij;
+        const double el = exp(lng_pi[Kp] / 2.0);
+        double acc = 0.0;
+        for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+          double d2 = dist2_grid(K1, Kp, r.dz);
+          if (d2 <= Dij2) {
+            double f = exp(-lam_j[K1] + lng_pj[K1] / 2.0);
+            if (gcc) {
+              double t = 0.0;
+              for (int q = 0; q < S; q++) t += gcc[(size_t)q * P + K1];
+              f *= t;
             }
+            double t = fabs(f) * el * r.dz * tr_j[K1] / renorm;
+            if (fabs(d2 - Dij2) <= 1e-6) t /= 2.0;
+            acc += t / s.normative;
           }
-          acc = block_sum(acc, sh.red);
-          for (int K = threadIdx.x; K < P; K += blockDim.x) out[K] = (K == Kp) ? acc : 0.0;
-        } else {
-          const double* wb = r.Wbond + (size_t)bond * P;
-          dct2_convolve(
-              sh.z, r, [&](int K) { return fchild(K) * tr_j[K]; }, [&](int q) { return wb[q]; },
-              [&](int K, double y) { out[K] = fabs(y) * exp(lng_pi[K] / 2.0) * inv_norm; });
         }
+        acc = block_sum(acc, sh.red);
+        for (int K = threadIdx.x; K < P; K += blockDim.x) out[K] = (K == Kp) ? acc : 0.0;
+      }
+    } else {
+      for (int g0 = 0; g0 < npair; g0 += r.TB) {
+        const int nT = min(r.TB, npair - g0);
+        const double* lam_t[kMaxTB];
+        const double* lngj_t[kMaxTB];
+        const double* lngi_t[kMaxTB];
+        const double* tr_t[kMaxTB];
+        const double* gcc_t[kMaxTB];
+        const double* wb_t[kMaxTB];
+        double* out_t[kMaxTB];
+        for (int t = 0; t < nT; t++) {
+          const int pi = g0 + t, ii = pi / nc, jj = pi - ii * nc;
+          const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
+          const int bond = bond_of(r, si, sj);
+          const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+          out_t[t] = s.gC + ((size_t)(p * S + ii) * S + jj) * P;
+          lam_t[t] = r.lambda + (size_t)sj * P;
+          lngj_t[t] = lng + (size_t)(bond * 2 + pair_j) * P;
+          lngi_t[t] = lng + (size_t)(bond * 2 + pair_i) * P;
+          tr_t[t] = r.trapez + (size_t)sj * P;
+          gcc_t[t] = (c < N - 1) ? s.gC + ((size_t)(c * S + jj) * S) * P : nullptr;
+          wb_t[t] = r.Wbond + (size_t)bond * P;
+        }
+        dct2_convolve_b(
+            fc, nT,
+            [&](int t, int K) {
+              double f = exp(-lam_t[t][K] + lngj_t[t][K] / 2.0);
+              if (gcc_t[t]) {
+                double q2 = 0.0;
+                for (int q = 0; q < S; q++) q2 += gcc_t[t][(size_t)q * P + K];
+                f *= q2;
+              }
+              return f * tr_t[t][K];
+            },
+            [&](int t, int q) { return wb_t[t][q]; },
+            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * exp(lngi_t[t][K] / 2.0) * inv_norm; });
       }
     }
     if (s.fixed >= 0) {  // max-distance mask (child_propagators.jl:147-157)
@@ -126,11 +180,21 @@ __device__ void chain_child(const DReq& r, const DSpecies& s, Shared sh) {
           for (int q = 0; q < S * S; q++) s.gC[((size_t)p * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
+    const int e = renormalise_block(s.gC + (size_t)p * S * S * P, S * S, P, sh.red);
+    e_child += e;
+    scaled |= e != 0;
+    if (threadIdx.x == 0) s.expo[p] = e_child;
   }
+  if (threadIdx.x == 0) s.expo[N - 1] = 0;
+  __syncthreads();
+  return scaled;
 }
 
-__device__ void chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
+__device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
   const int P = r.NP, S = s.S, N = s.n_seg;
+  bool scaled = false;
+  int e_parent = 0;  // exponent carried by gP of segment c - 1 (the root carries none)
+  if (threadIdx.x == 0) s.expo[N] = 0;
   const double* lng = xs_lng(r, r.x);
   const double inv_norm = 1.0 / s.normative;
   // root: base case gP[K, 1, idx_i, root] = 1 (only the graft point when fixed)
@@ -143,6 +207,7 @@ __device__ void chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
       }
   }
   __syncthreads();
+  const FftCtx fc = make_fft(sh.z, r);
   for (int c = 1; c < N; c++) {
     const int p = c - 1;
     // base case then the parent loop overwrites slot jj < nst[p]
@@ -151,45 +216,68 @@ __device__ void chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
         for (int jj = 0; jj < S; jj++)
           s.gP[((size_t)(c * S + ii) * S + jj) * P + K] = (jj == 0 && ii < s.nst[c]) ? 1.0 : 0.0;
     __syncthreads();
-    for (int ii = 0; ii < s.nst[c]; ii++) {
-      const int si = s.states[c * S + ii];
-      for (int jj = 0; jj < s.nst[p]; jj++) {
-        const int sj = s.states[p * S + jj];
+    const int np_ = s.nst[p];
+    const int npair = s.nst[c] * np_;
+    if (p == 0 && s.fixed >= 0) {
+      for (int pi = 0; pi < npair; pi++) {
+        const int ii = pi / np_, jj = pi - ii * np_;
+        const int si = s.states[c * S + ii], sj = s.states[p * S + jj];
         const int bond = bond_of(r, si, sj);
         const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
         double* out = s.gP + ((size_t)(c * S + ii) * S + jj) * P;
-        const double* lam_j = r.lambda + (size_t)sj * P;
         const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
         const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
-        const double* tr_j = r.trapez + (size_t)sj * P;
         const double* gpp = s.gP + ((size_t)(p * S + jj) * S) * P;
-        auto fparent = [&](int K) {
-          double t = 0.0;
-          for (int q = 0; q < S; q++) t += gpp[(size_t)q * P + K];
-          return exp(-lam_j[K] + lng_pj[K] / 2.0) * t;
-        };
-        if (p == 0 && s.fixed >= 0) {
-          // parent grafted (parent_propagators.jl:72-94)
-          const int Kp = s.fixed;
-          const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
-          const double Dij2 = Dij * Dij;
-          const double renorm = 2.0 * Dij;
-          const double f = fparent(Kp);
-          for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
-            double d2 = dist2_grid(K1, Kp, r.dz);
-            if (d2 <= Dij2) {
-              double v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm / s.normative;
-              if (fabs(d2 - Dij2) <= 1e-6) v /= 2.0;
-              out[K1] = v;
-            }
+        // parent grafted (parent_propagators.jl:72-94)
+        const int Kp = s.fixed;
+        const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
+        const double Dij2 = Dij * Dij;
+        const double renorm = 2.0 * Dij;
+        double tq = 0.0;
+        for (int q = 0; q < S; q++) tq += gpp[(size_t)q * P + Kp];
+        const double f = exp(-r.lambda[(size_t)sj * P + Kp] + lng_pj[Kp] / 2.0) * tq;
+        for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+          double d2 = dist2_grid(K1, Kp, r.dz);
+          if (d2 <= Dij2) {
+            double v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm / s.normative;
+            if (fabs(d2 - Dij2) <= 1e-6) v /= 2.0;
+            out[K1] = v;
           }
-          __syncthreads();
-        } else {
-          const double* wb = r.Wbond + (size_t)bond * P;
-          dct2_convolve(
-              sh.z, r, [&](int K) { return fparent(K) * tr_j[K]; }, [&](int q) { return wb[q]; },
-              [&](int K, double y) { out[K] = fabs(y) * exp(lng_pi[K] / 2.0) * inv_norm; });
         }
+        __syncthreads();
+      }
+    } else {
+      for (int g0 = 0; g0 < npair; g0 += r.TB) {
+        const int nT = min(r.TB, npair - g0);
+        const double* lam_t[kMaxTB];
+        const double* lngj_t[kMaxTB];
+        const double* lngi_t[kMaxTB];
+        const double* tr_t[kMaxTB];
+        const double* gpp_t[kMaxTB];
+        const double* wb_t[kMaxTB];
+        double* out_t[kMaxTB];
+        for (int t = 0; t < nT; t++) {
+          const int pi = g0 + t, ii = pi / np_, jj = pi - ii * np_;
+          const int si = s.states[c * S + ii], sj = s.states[p * S + jj];
+          const int bond = bond_of(r, si, sj);
+          const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+          out_t[t] = s.gP + ((size_t)(c * S + ii) * S + jj) * P;
+          lam_t[t] = r.lambda + (size_t)sj * P;
+          lngj_t[t] = lng + (size_t)(bond * 2 + pair_j) * P;
+          lngi_t[t] = lng + (size_t)(bond * 2 + pair_i) * P;
+          tr_t[t] = r.trapez + (size_t)sj * P;
+          gpp_t[t] = s.gP + ((size_t)(p * S + jj) * S) * P;
+          wb_t[t] = r.Wbond + (size_t)bond * P;
+        }
+        dct2_convolve_b(
+            fc, nT,
+            [&](int t, int K) {
+              double q2 = 0.0;
+              for (int q = 0; q < S; q++) q2 += gpp_t[t][(size_t)q * P + K];
+              return exp(-lam_t[t][K] + lngj_t[t][K] / 2.0) * q2 * tr_t[t][K];
+            },
+            [&](int t, int q) { return wb_t[t][q]; },
+            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * exp(lngi_t[t][K] / 2.0) * inv_norm; });
       }
     }
     if (s.fixed >= 0) {
@@ -200,7 +288,13 @@ __device__ void chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
           for (int q = 0; q < S * S; q++) s.gP[((size_t)c * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
+    const int e = renormalise_block(s.gP + (size_t)c * S * S * P, S * S, P, sh.red);
+    e_parent += e;
+    scaled |= e != 0;
+    if (threadIdx.x == 0) s.expo[N + c] = e_parent;
   }
+  __syncthreads();
+  return scaled;
 }
 
 // handle_fixed (handle_fixed.jl:1-120): chain normalisation; false on lambda <= 0
@@ -240,12 +334,26 @@ __device__ bool chain_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_o
   return true;
 }
 
+// ln of the density prefactor of segment g with renormalised propagators:
+// norm e^{mu} 2^{eP_g + eC_g}; free chains norm = normative^(N-1), grafted
+// chains norm = density / lambda with lambda carrying 2^{eP_1 + eC_1}
+__device__ __forceinline__ double log_prefactor(const DSpecies& s, double norm, int g) {
+  const int N = s.n_seg;
+  const int sg = s.expo[N + g] + (g < N - 1 ? s.expo[g] : 0);
+  if (s.fixed >= 0) {
+    const int s1 = s.expo[N + 1] + (1 < N - 1 ? s.expo[1] : 0);
+    return log(norm) + s.mu_species + (double)(sg - s1) * 0.6931471805599453;
+  }
+  return s.mu_species + (double)(N - 1) * log(s.normative) + (double)sg * 0.6931471805599453;
+}
+
 // accumulate_densities! for one species: rho_seg and both bond ends
-__device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm) {
+__device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, bool scaled) {
   const int P = r.NP, S = s.S, N = s.n_seg;
   const double mu = s.mu_species;
   for (int K = threadIdx.x; K < P; K += blockDim.x) {
     for (int g = 0; g < N; g++) {
+      const double lp = scaled ? log_prefactor(s, norm, g) : 0.0;
       for (int ii = 0; ii < s.nst[g]; ii++) {
         const int si = s.states[g * S + ii];
         double sp;
@@ -255,7 +363,8 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm) 
         } else {
           sp = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
         }
-        const double contr = norm * exp(mu - r.lambda[(size_t)si * P + K]) * sp;
+        const double contr = scaled ? exp(lp - r.lambda[(size_t)si * P + K]) * sp
+                                    : norm * exp(mu - r.lambda[(size_t)si * P + K]) * sp;
         double temp;
         if (g < N - 1) {
           temp = 0.0;
@@ -273,9 +382,10 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm) 
       }
     }
     for (int c = 1; c < N; c++) {
+      const double lp = scaled ? log_prefactor(s, norm, c) : 0.0;
       for (int ii = 0; ii < s.nst[c]; ii++) {
         const int si = s.states[c * S + ii];
-        double contr = norm * exp(mu - r.lambda[(size_t)si * P + K]);
+        double contr = scaled ? exp(lp - r.lambda[(size_t)si * P + K]) : norm * exp(mu - r.lambda[(size_t)si * P + K]);
         if (c < N - 1) {
           double t = 0.0;
           for (int q = 0; q < S; q++) t += s.gC[((size_t)(c * S + ii) * S + q) * P + K];
@@ -303,9 +413,10 @@ __device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
   __syncthreads();
   for (int u = 0; u < r.NS; u++) {
     DSpecies s = r.sp[u];
+    bool scaled = false;
     if (s.n_seg > 1) {
-      chain_child(r, s, sh);
-      chain_parent(r, s, sh);
+      scaled |= chain_child(r, s, sh);
+      scaled |= chain_parent(r, s, sh);
     }
     double norm;
     bool ok = chain_norm(r, s, sh, &norm);
@@ -318,7 +429,9 @@ __device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
       w->mu_species = s.mu_species;
       w->lambda_fixed = s.lambda_fixed;
     }
-    chain_accumulate(r, s, norm);
+    // the reference's prefactor norm e^{mu - lambda} overflows beyond e^709
+    if (fabs(s.mu_species) + (double)(s.n_seg - 1) * fabs(log(s.normative)) > 600.0) scaled = true;
+    chain_accumulate(r, s, norm, scaled);
   }
   // update_spatial_structures!
   for (int K = threadIdx.x; K < P; K += blockDim.x) {
@@ -346,22 +459,31 @@ __device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
 // ---------------------------------------------------------------------------
 __device__ void stage_rho_hat(const DReq& r, Shared sh) {
   const int P = r.NP;
-  for (int j = 0; j < r.NB; j++) {
-    const double* rho = r.rho_beads + (size_t)j * P;
-    const double* tr = r.trapez + (size_t)j * P;
-    double* C = r.Cb + (size_t)j * P;
-    dct2_forward(
-        sh.z, r, [&](int K) { return rho[K] * tr[K]; }, [&](int q, double c) { C[q] = c; });
-  }
-  for (int u = 0; u < r.MB; u++)
-    for (int e = 0; e < 2; e++) {
-      const int bead = r.bonds[2 * u + e];
-      const double* rho = r.rho_bonds + (size_t)(u * 2 + e) * P;
-      const double* tr = r.trapez + (size_t)bead * P;
-      double* C = r.Cbond + (size_t)(u * 2 + e) * P;
-      dct2_forward(
-          sh.z, r, [&](int K) { return rho[K] * tr[K]; }, [&](int q, double c) { C[q] = c; });
+  const FftCtx fc = make_fft(sh.z, r);
+  const int ntot = r.NB + 2 * r.MB;
+  for (int g0 = 0; g0 < ntot; g0 += r.TB) {
+    const int nT = min(r.TB, ntot - g0);
+    const double* rho_t[kMaxTB];
+    const double* tr_t[kMaxTB];
+    double* C_t[kMaxTB];
+    for (int t = 0; t < nT; t++) {
+      const int q = g0 + t;
+      if (q < r.NB) {
+        rho_t[t] = r.rho_beads + (size_t)q * P;
+        tr_t[t] = r.trapez + (size_t)q * P;
+        C_t[t] = r.Cb + (size_t)q * P;
+      } else {
+        const int be = q - r.NB;  // bond * 2 + end
+        const int bead = r.bonds[be];
+        rho_t[t] = r.rho_bonds + (size_t)be * P;
+        tr_t[t] = r.trapez + (size_t)bead * P;
+        C_t[t] = r.Cbond + (size_t)be * P;
+      }
     }
+    dct2_forward_b(
+        fc, nT, [&](int t, int K) { return rho_t[t][K] * tr_t[t][K]; },
+        [&](int t, int q, double v) { C_t[t][q] = v; });
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -386,63 +508,89 @@ __device__ __forceinline__ void mfmt_deriv_pt(double n0, double n1, double n2, d
   d[5] = -nV1 * i1 - (l1 * i3 + i1 * i1) * n2 * nV2 * i3 * 6.0 * i36;
 }
 
-__device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
+// scalar weighted densities n0..n3, nV1, nV2 into wa[0..6P); bond weighted
+// densities into wb.  |.| is taken per bead type before the bead sum, as in
+// TPT1mfmt.jl:79-89, so each bead's two transforms go to their own scratch
+// arrays (wd) and are summed afterwards in bead order.
+__device__ void fmt_weighted(const DReq& r, Shared sh, bool tpt1) {
   const int P = r.NP, NB = r.NB, MB = r.MB;
+  const FftCtx fc = make_fft(sh.z, r);
   double* n0 = r.wa;
   double* n1 = r.wa + (size_t)1 * P;
   double* n2 = r.wa + (size_t)2 * P;
   double* n3 = r.wa + (size_t)3 * P;
   double* nV1 = r.wa + (size_t)4 * P;
   double* nV2 = r.wa + (size_t)5 * P;
-  for (int q = threadIdx.x; q < 4 * P; q += blockDim.x) r.wa[q] = 0.0;
-  __syncthreads();
-  // scalar weighted densities, |.| per bead type as in TPT1mfmt.jl:79-89
-  for (int j = 0; j < NB; j++) {
-    const double s = r.sig[j];
-    const double* C = r.Cb + (size_t)j * P;
-    const double* W1 = r.Wfmt + ((size_t)j * 3 + 0) * P;
-    const double* W2 = r.Wfmt + ((size_t)j * 3 + 1) * P;
-    dct2_inverse(
-        sh.z, r, [&](int q) { return C[q] * W1[q]; },
-        [&](int K, double y) {
-          double a = fabs(y);
-          n0[K] += a / (kPi * (s * s));
-          n1[K] += a / (2 * kPi * s);
-          n2[K] += a;
-        });
-    dct2_inverse(
-        sh.z, r, [&](int q) { return C[q] * W2[q]; }, [&](int K, double y) { n3[K] += fabs(y); });
+  const int ns = 2 * NB;  // (bead j, weight m) -> wd[(2j+m) P]
+  for (int g0 = 0; g0 < ns; g0 += r.TB) {
+    const int nT = min(r.TB, ns - g0);
+    dct2_inverse_b(
+        fc, nT,
+        [&](int t, int q) {
+          const int jm = g0 + t, j = jm >> 1, m = jm & 1;
+          return r.Cb[(size_t)j * P + q] * r.Wfmt[((size_t)j * 3 + m) * P + q];
+        },
+        [&](int t, int K, double y) { r.wd[(size_t)(g0 + t) * P + K] = fabs(y); });
+  }
+  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    for (int j = 0; j < NB; j++) {
+      const double s = r.sig[j];
+      const double a = r.wd[(size_t)(2 * j) * P + K];
+      a0 += a / (kPi * (s * s));
+      a1 += a / (2 * kPi * s);
+      a2 += a;
+      a3 += r.wd[(size_t)(2 * j + 1) * P + K];
+    }
+    n0[K] = a0;
+    n1[K] = a1;
+    n2[K] = a2;
+    n3[K] = a3;
   }
   // vector weighted densities: odd output of the odd weight; the bead sum is linear
-  for (int v = 0; v < 2; v++) {
-    double* out = v == 0 ? nV1 : nV2;
-    dct2_inverse(
-        sh.z, r,
-        [&](int q) {
+  for (int g0 = 0; g0 < 2; g0 += r.TB) {
+    const int nT = min(r.TB, 2 - g0);
+    dct2_inverse_b(
+        fc, nT,
+        [&](int t, int q) {
           if (q == 0) return 0.0;
           const int k = P - q;
-          double t = 0.0;
+          double s = 0.0;
           for (int j = 0; j < NB; j++) {
             double c = r.Cb[(size_t)j * P + k] * r.Wfmt[((size_t)j * 3 + 2) * P + k];
-            t += v == 0 ? c / (2 * kPi * r.sig[j]) : c;
+            s += g0 + t == 0 ? c / (2 * kPi * r.sig[j]) : c;
           }
-          return t;
+          return s;
         },
-        [&](int K, double y) { out[K] = (K & 1) ? y : -y; });
+        [&](int t, int K, double y) { (g0 + t == 0 ? nV1 : nV2)[K] = (K & 1) ? y : -y; });
   }
   // bond weighted densities (TPT1mfmt.jl:106-133)
   if (tpt1) {
-    for (int u = 0; u < MB; u++)
-      for (int e = 0; e < 2; e++) {
-        const int i = r.bonds[2 * u + e];
-        const double* C = r.Cbond + (size_t)(u * 2 + e) * P;
-        const double* W1 = r.Wfmt + ((size_t)i * 3 + 0) * P;
-        const double si2 = r.sig[i] * r.sig[i];
-        double* out = r.wb + (size_t)(u * 2 + e) * P;
-        dct2_inverse(
-            sh.z, r, [&](int q) { return C[q] * W1[q] / si2 / kPi; }, [&](int K, double y) { out[K] = fabs(y); });
-      }
+    const int nb2 = 2 * MB;
+    for (int g0 = 0; g0 < nb2; g0 += r.TB) {
+      const int nT = min(r.TB, nb2 - g0);
+      dct2_inverse_b(
+          fc, nT,
+          [&](int t, int q) {
+            const int be = g0 + t, i = r.bonds[be];
+            return r.Cbond[(size_t)be * P + q] * r.Wfmt[((size_t)i * 3 + 0) * P + q] / (r.sig[i] * r.sig[i]) / kPi;
+          },
+          [&](int t, int K, double y) { r.wb[(size_t)(g0 + t) * P + K] = fabs(y); });
+    }
   }
+}
+
+__device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
+  const int P = r.NP, NB = r.NB, MB = r.MB;
+  const FftCtx fc = make_fft(sh.z, r);
+  double* n0 = r.wa;
+  double* n1 = r.wa + (size_t)1 * P;
+  double* n2 = r.wa + (size_t)2 * P;
+  double* n3 = r.wa + (size_t)3 * P;
+  double* nV1 = r.wa + (size_t)4 * P;
+  double* nV2 = r.wa + (size_t)5 * P;
+  fmt_weighted(r, sh, tpt1);
+  __syncthreads();
   // point-wise derivative; fields D0..D5 and ln y_HS per bond
   double* D = r.wc;
   double* lny = r.wc + (size_t)6 * P;
@@ -487,20 +635,24 @@ __device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
   __syncthreads();
   // forward transforms: even D0..D3, odd D4, D5 (DST-II through (-1)^K and reversal)
   double* CD = r.wa;  // 6 coefficient arrays (weighted densities are dead now)
-  for (int q = 0; q < 6; q++) {
-    const double* src = D + (size_t)q * P;
-    double* dst = CD + (size_t)q * P;
-    if (q < 4) {
-      dct2_forward(
-          sh.z, r, [&](int K) { return src[K]; }, [&](int k, double c) { dst[k] = c; });
-    } else {
-      if (threadIdx.x == 0) dst[0] = 0.0;
-      dct2_forward(
-          sh.z, r, [&](int K) { return (K & 1) ? -src[K] : src[K]; },
-          [&](int k, double c) {
-            if (k > 0) dst[P - k] = c;
-          });
-    }
+  if (threadIdx.x == 0) {
+    CD[(size_t)4 * P] = 0.0;
+    CD[(size_t)5 * P] = 0.0;
+  }
+  for (int g0 = 0; g0 < 6; g0 += r.TB) {
+    const int nT = min(r.TB, 6 - g0);
+    dct2_forward_b(
+        fc, nT,
+        [&](int t, int K) {
+          const int q = g0 + t;
+          const double v = D[(size_t)q * P + K];
+          return (q >= 4 && (K & 1)) ? -v : v;
+        },
+        [&](int t, int k, double v) {
+          const int q = g0 + t;
+          if (q < 4) CD[(size_t)q * P + k] = v;
+          else if (k > 0) CD[(size_t)q * P + (P - k)] = v;
+        });
   }
   // mu_ex coefficients (accumulate_mu_ex!, TPT1mfmt.jl:244-283)
   for (int idx = threadIdx.x; idx < NB * P; idx += blockDim.x) {
@@ -517,19 +669,15 @@ __device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
   __syncthreads();
   // ln g coefficients (accumulate_lng!, TPT1mfmt.jl:286-313)
   if (tpt1) {
-    for (int u = 0; u < MB; u++) {
-      const double* src = lny + (size_t)u * P;
-      const int ia = r.bonds[2 * u], ib = r.bonds[2 * u + 1];
-      const double* Wa = r.Wfmt + ((size_t)ia * 3) * P;
-      const double* Wb = r.Wfmt + ((size_t)ib * 3) * P;
-      const double sa = kPi * (r.sig[ia] * r.sig[ia]), sb = kPi * (r.sig[ib] * r.sig[ib]);
-      double* L0 = r.Clng + (size_t)(u * 2) * P;
-      double* L1 = r.Clng + (size_t)(u * 2 + 1) * P;
-      dct2_forward(
-          sh.z, r, [&](int K) { return src[K]; },
-          [&](int k, double c) {
-            L0[k] += c * (Wa[k] / sa);
-            L1[k] += c * (Wb[k] / sb);
+    for (int g0 = 0; g0 < MB; g0 += r.TB) {
+      const int nT = min(r.TB, MB - g0);
+      dct2_forward_b(
+          fc, nT, [&](int t, int K) { return lny[(size_t)(g0 + t) * P + K]; },
+          [&](int t, int k, double c) {
+            const int u = g0 + t;
+            const int ia = r.bonds[2 * u], ib = r.bonds[2 * u + 1];
+            r.Clng[(size_t)(u * 2) * P + k] += c * (r.Wfmt[((size_t)ia * 3) * P + k] / (kPi * (r.sig[ia] * r.sig[ia])));
+            r.Clng[(size_t)(u * 2 + 1) * P + k] += c * (r.Wfmt[((size_t)ib * 3) * P + k] / (kPi * (r.sig[ib] * r.sig[ib])));
           });
     }
   }
@@ -593,25 +741,33 @@ __device__ __forceinline__ MsaGamma gamma_msa_pt(const double* rho, const double
   return out;
 }
 
+__device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
+  const int P = r.NP, NB = r.NB, MB = r.MB;
+  const FftCtx fc = make_fft(sh.z, r);
+  const int ntot = NB + (tpt1 ? 2 * MB : 0);
+  for (int g0 = 0; g0 < ntot; g0 += r.TB) {
+    const int nT = min(r.TB, ntot - g0);
+    dct2_inverse_b(
+        fc, nT,
+        [&](int t, int q) {
+          const int w = g0 + t;
+          if (w < NB) return r.Cb[(size_t)w * P + q] * r.Wmsa[(size_t)w * P + q];
+          const int be = w - NB;
+          return r.Cbond[(size_t)be * P + q] * r.Wmsa[(size_t)r.bonds[be] * P + q];
+        },
+        [&](int t, int K, double y) {
+          const int w = g0 + t;
+          if (w < NB) r.wa[(size_t)w * P + K] = fabs(y);
+          else r.wb[(size_t)(w - NB) * P + K] = fabs(y);
+        });
+  }
+}
+
 __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
   const int P = r.NP, NB = r.NB, MB = r.MB;
-  for (int j = 0; j < NB; j++) {
-    const double* C = r.Cb + (size_t)j * P;
-    const double* W = r.Wmsa + (size_t)j * P;
-    double* out = r.wa + (size_t)j * P;
-    dct2_inverse(
-        sh.z, r, [&](int q) { return C[q] * W[q]; }, [&](int K, double y) { out[K] = fabs(y); });
-  }
-  if (tpt1)
-    for (int u = 0; u < MB; u++)
-      for (int e = 0; e < 2; e++) {
-        const int i = r.bonds[2 * u + e];
-        const double* C = r.Cbond + (size_t)(u * 2 + e) * P;
-        const double* W = r.Wmsa + (size_t)i * P;
-        double* out = r.wb + (size_t)(u * 2 + e) * P;
-        dct2_inverse(
-            sh.z, r, [&](int q) { return C[q] * W[q]; }, [&](int K, double y) { out[K] = fabs(y); });
-      }
+  const FftCtx fc = make_fft(sh.z, r);
+  msa_weighted(r, sh, tpt1);
+  __syncthreads();
   // point-wise derivative (TPT1msa.jl:129-156 -> iLST TPT1msa.jl:200-282)
   const double* sig = r.sig;
   const double* Z = r.z;
@@ -686,27 +842,22 @@ __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
     for (int j = 0; j < NB; j++) r.wc[(size_t)j * P + K] = dphi[j];
   }
   __syncthreads();
-  for (int j = 0; j < NB; j++) {
-    const double* src = r.wc + (size_t)j * P;
-    const double* W = r.Wmsa + (size_t)j * P;
-    double* Cm = r.Cmu + (size_t)j * P;
-    dct2_forward(
-        sh.z, r, [&](int K) { return src[K]; }, [&](int k, double c) { Cm[k] += c * W[k]; });
+  const int nf = NB + (tpt1 ? MB : 0);
+  for (int g0 = 0; g0 < nf; g0 += r.TB) {
+    const int nT = min(r.TB, nf - g0);
+    dct2_forward_b(
+        fc, nT, [&](int t, int K) { return r.wc[(size_t)(g0 + t) * P + K]; },
+        [&](int t, int k, double c) {
+          const int w = g0 + t;
+          if (w < NB) {
+            r.Cmu[(size_t)w * P + k] += c * r.Wmsa[(size_t)w * P + k];
+          } else {
+            const int u = w - NB;
+            r.Clng[(size_t)(u * 2) * P + k] += c * r.Wmsa[(size_t)r.bonds[2 * u] * P + k];
+            r.Clng[(size_t)(u * 2 + 1) * P + k] += c * r.Wmsa[(size_t)r.bonds[2 * u + 1] * P + k];
+          }
+        });
   }
-  if (tpt1)
-    for (int u = 0; u < MB; u++) {
-      const double* src = r.wc + (size_t)(NB + u) * P;
-      const double* Wa = r.Wmsa + (size_t)r.bonds[2 * u] * P;
-      const double* Wb = r.Wmsa + (size_t)r.bonds[2 * u + 1] * P;
-      double* L0 = r.Clng + (size_t)(u * 2) * P;
-      double* L1 = r.Clng + (size_t)(u * 2 + 1) * P;
-      dct2_forward(
-          sh.z, r, [&](int K) { return src[K]; },
-          [&](int k, double c) {
-            L0[k] += c * Wa[k];
-            L1[k] += c * Wb[k];
-          });
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -794,29 +945,24 @@ __device__ bool objective(const DReq& r, Shared sh) {
   if (r.funcs & 0x4) stage_msa(r, sh, false);
   if (r.funcs & 0x8) stage_msa(r, sh, true);
   double* g = r.g;
-  for (int j = 0; j < r.NB; j++) {
-    const double* C = r.Cmu + (size_t)j * P;
-    double* out = g + (size_t)j * P;
-    dct2_inverse(
-        sh.z, r, [&](int q) { return C[q]; }, [&](int K, double y) { out[K] = y; });
+  const FftCtx fc = make_fft(sh.z, r);
+  // mu_ex (NB), ln g (2 MB) and Psi (1): independent inverse transforms
+  const int nout = r.NB + 2 * r.MB + 1;
+  for (int g0 = 0; g0 < nout; g0 += r.TB) {
+    const int nT = min(r.TB, nout - g0);
+    dct2_inverse_b(
+        fc, nT,
+        [&](int t, int k) {
+          const int w = g0 + t;
+          if (w < r.NB) return r.Cmu[(size_t)w * P + k];
+          if (w < r.NB + 2 * r.MB) return r.Clng[(size_t)(w - r.NB) * P + k];
+          // Poisson (solve_poisson_eq): (surf + sum_j z_j rho_hat_j) * w_coul
+          double f = r.Csurf[k];
+          for (int j = 0; j < r.NB; j++) f += r.Cb[(size_t)j * P + k] * r.z[j];
+          return f * r.Wcoul[k];
+        },
+        [&](int t, int K, double y) { g[(size_t)(g0 + t) * P + K] = y; });
   }
-  double* gl = g + (size_t)P * r.NB;
-  for (int q = 0; q < 2 * r.MB; q++) {
-    const double* C = r.Clng + (size_t)q * P;
-    double* out = gl + (size_t)q * P;
-    dct2_inverse(
-        sh.z, r, [&](int k) { return C[k]; }, [&](int K, double y) { out[K] = y; });
-  }
-  // Poisson (solve_poisson_eq): (surf + sum_j z_j rho_hat_j) * w_coul
-  double* gpsi = g + (size_t)P * (r.NB + 2 * r.MB);
-  dct2_inverse(
-      sh.z, r,
-      [&](int k) {
-        double f = r.Csurf[k];
-        for (int j = 0; j < r.NB; j++) f += r.Cb[(size_t)j * P + k] * r.z[j];
-        return f * r.Wcoul[k];
-      },
-      [&](int K, double y) { gpsi[K] = y; });
   const double shift = stage_neutrality(r, sh);
   if (threadIdx.x == 0) g[off_psic(r)] = r.x[off_psic(r)] + shift;
   __syncthreads();

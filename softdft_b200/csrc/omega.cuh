@@ -13,83 +13,6 @@
 
 namespace sdft {
 
-// scalar weighted densities n0..n3, nV1, nV2 into wa[0..6P), bond weighted into wb
-__device__ void fmt_weighted(const DReq& r, Shared sh, bool tpt1) {
-  const int P = r.NP, NB = r.NB, MB = r.MB;
-  double* n0 = r.wa;
-  double* n1 = r.wa + (size_t)1 * P;
-  double* n2 = r.wa + (size_t)2 * P;
-  double* n3 = r.wa + (size_t)3 * P;
-  double* nV1 = r.wa + (size_t)4 * P;
-  double* nV2 = r.wa + (size_t)5 * P;
-  for (int q = threadIdx.x; q < 4 * P; q += blockDim.x) r.wa[q] = 0.0;
-  __syncthreads();
-  for (int j = 0; j < NB; j++) {
-    const double s = r.sig[j];
-    const double* C = r.Cb + (size_t)j * P;
-    const double* W1 = r.Wfmt + ((size_t)j * 3 + 0) * P;
-    const double* W2 = r.Wfmt + ((size_t)j * 3 + 1) * P;
-    dct2_inverse(
-        sh.z, r, [&](int q) { return C[q] * W1[q]; },
-        [&](int K, double y) {
-          double a = fabs(y);
-          n0[K] += a / (kPi * (s * s));
-          n1[K] += a / (2 * kPi * s);
-          n2[K] += a;
-        });
-    dct2_inverse(
-        sh.z, r, [&](int q) { return C[q] * W2[q]; }, [&](int K, double y) { n3[K] += fabs(y); });
-  }
-  for (int v = 0; v < 2; v++) {
-    double* out = v == 0 ? nV1 : nV2;
-    dct2_inverse(
-        sh.z, r,
-        [&](int q) {
-          if (q == 0) return 0.0;
-          const int k = P - q;
-          double t = 0.0;
-          for (int j = 0; j < NB; j++) {
-            double c = r.Cb[(size_t)j * P + k] * r.Wfmt[((size_t)j * 3 + 2) * P + k];
-            t += v == 0 ? c / (2 * kPi * r.sig[j]) : c;
-          }
-          return t;
-        },
-        [&](int K, double y) { out[K] = (K & 1) ? y : -y; });
-  }
-  if (tpt1)
-    for (int u = 0; u < MB; u++)
-      for (int e = 0; e < 2; e++) {
-        const int i = r.bonds[2 * u + e];
-        const double* C = r.Cbond + (size_t)(u * 2 + e) * P;
-        const double* W1 = r.Wfmt + ((size_t)i * 3 + 0) * P;
-        const double si2 = r.sig[i] * r.sig[i];
-        double* out = r.wb + (size_t)(u * 2 + e) * P;
-        dct2_inverse(
-            sh.z, r, [&](int q) { return C[q] * W1[q] / si2 / kPi; }, [&](int K, double y) { out[K] = fabs(y); });
-      }
-}
-
-__device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
-  const int P = r.NP;
-  for (int j = 0; j < r.NB; j++) {
-    const double* C = r.Cb + (size_t)j * P;
-    const double* W = r.Wmsa + (size_t)j * P;
-    double* out = r.wa + (size_t)j * P;
-    dct2_inverse(
-        sh.z, r, [&](int q) { return C[q] * W[q]; }, [&](int K, double y) { out[K] = fabs(y); });
-  }
-  if (tpt1)
-    for (int u = 0; u < r.MB; u++)
-      for (int e = 0; e < 2; e++) {
-        const int i = r.bonds[2 * u + e];
-        const double* C = r.Cbond + (size_t)(u * 2 + e) * P;
-        const double* W = r.Wmsa + (size_t)i * P;
-        double* out = r.wb + (size_t)(u * 2 + e) * P;
-        dct2_inverse(
-            sh.z, r, [&](int q) { return C[q] * W[q]; }, [&](int K, double y) { out[K] = fabs(y); });
-      }
-}
-
 // out[0] = Omega, out[1 + u] = N_u
 __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
   const int P = r.NP, NB = r.NB, MB = r.MB;

@@ -59,7 +59,7 @@ extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_objective(const DR
   if (threadIdx.x == 0) *r.status = ok ? ST_OK : ST_NORM;
 }
 
-extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_solve(const DReq* reqs, SolveSlot* slots, SolveCfg cfg,
+extern "C" __global__ void __launch_bounds__(kThreads, 2) sdft_k_solve(const DReq* reqs, SolveSlot* slots, SolveCfg cfg,
                                                                     int max_chunk) {
   extern __shared__ double smem[];
   const DReq& r = reqs[blockIdx.x];
@@ -125,6 +125,9 @@ static int set_err(int code, const std::string& msg) {
     if (e_ != cudaSuccess)                                                             \
       return set_err(SDFT_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+static int tb_for(int M);
+static size_t smem_bytes(int M);
 
 struct SpeciesHost {
   int n_seg, S, fixed;
@@ -343,7 +346,7 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
   size_t o_sig = lay.take<double>(NB), o_z = lay.take<double>(NB), o_dmu = lay.take<double>(NB);
   size_t o_bonds = lay.take<int>(2 * MB + 2);
   size_t o_sp = lay.take<DSpecies>(NS);
-  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS);
+  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS), o_expo(NS);
   for (int u = 0; u < NS; u++) {
     const SpeciesHost& h = q->sp[u];
     o_states[u] = lay.take<int>(h.states.size());
@@ -353,6 +356,7 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
     o_gC[u] = lay.take<double>(gsz);
     o_gP[u] = lay.take<double>(gsz);
     o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
+    o_expo[u] = lay.take<int>((size_t)2 * h.n_seg);
   }
   size_t o_Ext = lay.take<double>((size_t)NB * P), o_tr = lay.take<double>((size_t)NB * P);
   size_t o_Csurf = lay.take<double>(P);
@@ -366,6 +370,7 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
   size_t o_Cmu = lay.take<double>((size_t)NB * P), o_Clng = lay.take<double>((size_t)MB * 2 * P + 1);
   size_t o_wa = lay.take<double>((size_t)nwa * P), o_wb = lay.take<double>((size_t)MB * 2 * P + 1);
   size_t o_wc = lay.take<double>((size_t)nwc * P);
+  size_t o_wd = lay.take<double>((size_t)2 * NB * P);
   size_t o_hx = lay.take<double>((size_t)m_alloc * q->n), o_hg = lay.take<double>((size_t)m_alloc * q->n);
   size_t o_u = lay.take<double>(q->n);
   size_t o_status = lay.take<int>(4), o_iters = lay.take<int>(4), o_err = lay.take<double>(4);
@@ -471,6 +476,7 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
     s.gC = h.n_seg > 1 ? (double*)P_(o_gC[u]) : nullptr;
     s.gP = h.n_seg > 1 ? (double*)P_(o_gP[u]) : nullptr;
     s.rho_seg = (double*)P_(o_rho[u]);
+    s.expo = (int*)P_(o_expo[u]);
   }
   DReq& r = q->h;
   r.NP = P;
@@ -511,6 +517,8 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
   r.wa = (double*)P_(o_wa);
   r.wb = (double*)P_(o_wb);
   r.wc = (double*)P_(o_wc);
+  r.wd = (double*)P_(o_wd);
+  r.TB = tb_for(M);
   r.hx = (double*)P_(o_hx);
   r.hg = (double*)P_(o_hg);
   r.lsq_u = (double*)P_(o_u);
@@ -578,7 +586,18 @@ extern "C" int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* d
   return SDFT_OK;
 }
 
-static size_t smem_bytes(int M) { return sizeof(double) * kRedDoubles + sizeof(double2) * (size_t)M; }
+// transform buffers per CTA: up to kMaxTB, keeping the buffers near 96 KB so
+// that two CTAs fit on an SM; one buffer of M + M/8 complex values minimum
+static int tb_for(int M) {
+  const size_t buf = sizeof(double2) * (size_t)(M + M / 8);
+  size_t tb = (96 * 1024) / buf;
+  if (tb < 1) tb = 1;
+  if (tb > (size_t)kMaxTB) tb = kMaxTB;
+  return (int)tb;
+}
+static size_t smem_bytes(int M) {
+  return sizeof(double) * kRedDoubles + sizeof(double2) * (size_t)(M + M / 8) * (size_t)tb_for(M);
+}
 
 static int prepare_kernel(const void* fn, size_t smem) {
   if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -643,9 +662,8 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
   int rc = validate_numerics(num);
   if (rc) return rc;
   cudaStream_t stream = hs[0]->stream;
-  int maxM = 0;
-  for (int i = 0; i < n; i++) maxM = std::max(maxM, hs[i]->M);
-  size_t sm = smem_bytes(maxM);
+  size_t sm = 0;
+  for (int i = 0; i < n; i++) sm = std::max(sm, smem_bytes(hs[i]->M));
   rc = prepare_kernel((const void*)sdft_k_solve, sm);
   if (rc) return rc;
   DReq* dreqs = nullptr;
@@ -914,7 +932,7 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
   size_t o_sig = lay.take<double>(NB), o_z = lay.take<double>(NB), o_dmu = lay.take<double>(NB);
   size_t o_bonds = lay.take<int>(2 * MB + 2);
   size_t o_sp = lay.take<DSpecies>(NS);
-  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS);
+  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS), o_expo(NS);
   for (int u = 0; u < NS; u++) {
     const SpeciesHost& h = sp[u];
     o_states[u] = lay.take<int>(h.states.size());
@@ -924,6 +942,7 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
     o_gC[u] = lay.take<double>(gsz);
     o_gP[u] = lay.take<double>(gsz);
     o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
+    o_expo[u] = lay.take<int>((size_t)2 * h.n_seg);
   }
   size_t o_Ext = lay.take<double>((size_t)NB * P), o_tr = lay.take<double>((size_t)NB * P);
   size_t o_Csurf = lay.take<double>(P);
@@ -936,6 +955,7 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
   size_t o_Cmu = lay.take<double>((size_t)NB * P), o_Clng = lay.take<double>((size_t)MB * 2 * P + 1);
   size_t o_wa = lay.take<double>((size_t)nwa * P), o_wb = lay.take<double>((size_t)MB * 2 * P + 1);
   size_t o_wc = lay.take<double>((size_t)nwc * P);
+  size_t o_wd = lay.take<double>((size_t)2 * NB * P);
   size_t o_status = lay.take<int>(4), o_iters = lay.take<int>(4), o_err = lay.take<double>(4);
   size_t o_scal = lay.take<double>(8);
   size_t o_dreq = lay.take<DReq>(1);
@@ -1021,6 +1041,7 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
     s.gC = h.n_seg > 1 ? (double*)at(o_gC[u]) : nullptr;
     s.gP = h.n_seg > 1 ? (double*)at(o_gP[u]) : nullptr;
     s.rho_seg = (double*)at(o_rho[u]);
+    s.expo = (int*)at(o_expo[u]);
   }
   DReq r{};
   r.NP = P;
@@ -1061,6 +1082,8 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
   r.wa = (double*)at(o_wa);
   r.wb = (double*)at(o_wb);
   r.wc = (double*)at(o_wc);
+  r.wd = (double*)at(o_wd);
+  r.TB = tb_for(M);
   r.hx = nullptr;
   r.hg = nullptr;
   r.lsq_u = nullptr;

@@ -317,6 +317,106 @@ def _fj_propagators(ms: MolecularSystem, bulk: BulkState, u: int):
     return gC, gP, Xi
 
 
+def _lse(vals):
+    """log(sum(exp(v))) over finite-or--inf entries."""
+    v = np.asarray(vals, dtype=np.float64)
+    m = np.max(v) if v.size else -np.inf
+    if not np.isfinite(m):
+        return m
+    return float(m + np.log(np.sum(np.exp(v - m))))
+
+
+def _fj_log_propagators(ms: MolecularSystem, bulk: BulkState, u: int):
+    """The propagators of `_fj_propagators` as natural logarithms, for chains
+    whose products leave the double range (the reference's unscaled products
+    underflow past ~100 segments at mu_ex ~ 6 and then yield NaN).  Zero
+    entries are -inf."""
+    cfg = ms.configurations[u]
+    fam = cfg.state_family
+    topo = cfg.topology
+    n = len(cfg.sequence)
+    ms_ = max(max(len(f) for f in fam), 1)
+    mc = max(max(len(c) for c in topo.children), 1)
+    dm, mu, lng = ms.delta_muH, bulk.mu_ex, bulk.lng
+    lC = np.full((ms_, mc, ms_, n), -np.inf)
+    for level in reversed(topo.levels):
+        for p in level:
+            for ii, s_i in enumerate(fam[p]):
+                lC[0, 0, ii, p] = 0.0
+                for ic, c in enumerate(topo.children[p]):
+                    for ij, s_j in enumerate(fam[c]):
+                        b = _bond_index(ms.bond_types, s_i, s_j)
+                        val = -dm[s_j] - mu[s_j] + lng[b]
+                        for igc, _ in enumerate(topo.children[c]):
+                            val += _lse(lC[:, igc, ij, c])
+                        lC[ij, ic, ii, p] = val
+    lP = np.full((ms_, ms_, n), -np.inf)
+    for level in topo.levels:
+        for c in level:
+            for ij, s_j in enumerate(fam[c]):
+                lP[0, ij, c] = 0.0
+                for p in topo.parents[c]:
+                    for ii, s_i in enumerate(fam[p]):
+                        b = _bond_index(ms.bond_types, s_i, s_j)
+                        val = -dm[s_i] - mu[s_i] + lng[b] + _lse(lP[:, ii, p])
+                        for ioc, oc in enumerate(topo.children[p]):
+                            if oc != c:
+                                val += _lse(lC[:, ioc, ii, p])
+                        lP[ii, ij, c] = val
+    terms = []
+    for ii, s_i in enumerate(fam[0]):
+        t = -(mu[s_i] + dm[s_i]) + _lse(lP[:, ii, 0])
+        for ic, _ in enumerate(topo.children[0]):
+            t += _lse(lC[:, ic, ii, 0])
+        terms.append(t)
+    return lC, lP, _lse(terms)
+
+
+def _fj_accumulate_log(ms: MolecularSystem, bulk: BulkState, u: int, seg: np.ndarray) -> None:
+    """`accumulate_densities!` of the bulk freely-jointed chain evaluated with
+    log-domain propagators."""
+    cfg = ms.configurations[u]
+    fam = cfg.state_family
+    topo = cfg.topology
+    lC, lP, lXi = _fj_log_propagators(ms, bulk, u)
+    bulk.Xi[u] = math.exp(lXi) if lXi < 700 else math.inf
+    for si in range(len(cfg.sequence)):
+        for ii, s_i in enumerate(fam[si]):
+            lam = bulk.mu_ex[s_i] + ms.delta_muH[s_i]
+            lpref = math.log(bulk.rho_species[u]) - lam + _lse(lP[:, ii, si]) - lXi
+            if topo.children[si]:
+                child = topo.children[si][0]
+                terms = []
+                for ij, _ in enumerate(fam[child]):
+                    t = lC[ij, 0, ii, si]
+                    for ioc, oc in enumerate(topo.children[si]):
+                        if oc != child:
+                            t += _lse(lC[:, ioc, ii, si])
+                    terms.append(t)
+                lcc = _lse(terms)
+            else:
+                lcc = 0.0
+            lval = lpref + lcc
+            val = math.exp(lval)
+            seg[ii, si] = val
+            bulk.rho_beads[s_i] += val
+            for ic, c in enumerate(topo.children[si]):
+                lQ = _lse(lC[:, ic, ii, si])
+                for ij, s_j in enumerate(fam[c]):
+                    f = math.exp(lval + lC[ij, ic, ii, si] - lQ)
+                    bulk.rho_bonds[:, _bond_index(ms.bond_types, s_i, s_j)] += f
+
+
+def _fj_log_xi(ms, bulk, u) -> float:
+    """ln Xi of a freely-jointed species: direct products when finite, else
+    log-domain propagators."""
+    with np.errstate(all="ignore"):
+        _, _, Xi = _fj_propagators(ms, bulk, u)
+    if np.isfinite(Xi) and Xi > 0:
+        return math.log(Xi)
+    return _fj_log_propagators(ms, bulk, u)[2]
+
+
 def _monomerbead_xi(ms, bulk, u):
     """`src/iLST/species_model/monomerbead/partition_function.jl:17-38`."""
     cfg = ms.configurations[u]
@@ -344,7 +444,15 @@ def eval_bulk_density(ms: MolecularSystem, bulk: BulkState) -> None:
                     bulk.rho_beads[s_i] += val
                     seg[ii, si] += val
             continue
-        gC, gP, Xi = _fj_propagators(ms, bulk, u)
+        with np.errstate(all="ignore"):
+            gC, gP, Xi = _fj_propagators(ms, bulk, u)
+        if not (np.isfinite(Xi) and Xi > 0 and np.all(np.isfinite(gC)) and np.all(np.isfinite(gP))
+                and bulk.rho_species[u] > 0):
+            if bulk.rho_species[u] > 0:
+                _fj_accumulate_log(ms, bulk, u, seg)
+            else:
+                bulk.Xi[u] = Xi
+            continue
         bulk.Xi[u] = Xi
         for si in range(len(cfg.sequence)):
             for ii, s_i in enumerate(fam[si]):
@@ -407,10 +515,12 @@ def bulk_chemical_potential(ms: MolecularSystem, bulk: BulkState) -> None:
     for u, cfg in enumerate(ms.configurations):
         if cfg.model == "monomerbead":
             Xi = _monomerbead_xi(ms, bulk, u)
+            bulk.Xi[u] = Xi
+            bulk.mu_species[u] -= math.log(Xi)
         else:
-            _, _, Xi = _fj_propagators(ms, bulk, u)
-        bulk.Xi[u] = Xi
-        bulk.mu_species[u] -= math.log(Xi)
+            lxi = _fj_log_xi(ms, bulk, u)
+            bulk.Xi[u] = math.exp(lxi) if lxi < 700 else math.inf
+            bulk.mu_species[u] -= lxi
 
 
 def _species_in_reactions(ms: MolecularSystem) -> set:

@@ -40,6 +40,16 @@ def _diblock_small():
 
 
 CASES["diblock_small"] = _diblock_small()
+# 200-segment diblock in a 10-sigma slit: renormalised propagators
+CASES["long_diblock"] = workloads.diblock_slit(1024)
+# grid sizes that exercise every FFT pass mix (log2 M = 10, 11, 12, 13: radix-8
+# passes with a radix-2 / radix-4 / no tail) and 4, 2, 1 transform buffers
+CASES["grid_2048_mfmt_msa"] = small_slit(np_=2048, dz=0.01, models=["ideal", "mfmt", "msa"])
+CASES["grid_4096"] = small_slit(np_=4096, dz=0.005)
+CASES["grid_8192"] = small_slit(np_=8192, dz=0.02)
+CASES["grid_16384"] = small_slit(np_=16384, dz=0.02)
+# the 200-segment diblock on the 16384-point grid (one transform buffer)
+CASES["diblock_16384"] = workloads.diblock_slit(16384)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

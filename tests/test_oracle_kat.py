@@ -104,3 +104,25 @@ def test_walls_zero_density_inside():
     assert np.all(b[ext > 1e19] == 0.0)
     # contact points carry trapezoid weight 1/2
     assert np.count_nonzero(tr.reshape(d.nb, d.np_)[0] == 0.5) == 2
+
+
+def test_bulk_fixed_point_long_chain_renormalised():
+    """150-segment chain in a dense fluid: the reference's unscaled propagator
+    products leave the double range here; the renormalised path must still
+    return the bulk state in a wall-free box."""
+    ds = small_slit(models=["ideal", "TPT1mfmt"], walls=False, n_chain=150, np_=256)
+    dft = descriptor(ds)
+    bulk = dft.bulk_system.bulk
+    # unscaled propagator products ~ exp(-(N-1)(mu_ex - lng)) fall below the double range
+    assert 149 * (bulk.mu_ex[0] - bulk.lng[0]) > 745
+    o = OracleSystem(dft.descriptor)
+    x0 = o.get_x()
+    g = o.objective()
+    assert np.all(np.isfinite(g))
+    mu0, lng0, _, _ = dft.split(x0)
+    mu, lng, psi, _ = dft.split(g)
+    assert rel(mu, mu0) < 1e-8
+    assert rel(lng, lng0) < 1e-8
+    segs, beads, _ = o.densities()
+    d = dft.descriptor
+    assert rel(beads.reshape(d.nb, d.np_)[:, d.np_ // 2], dft.bulk_system.bulk.rho_beads) < 1e-8
