@@ -39,6 +39,7 @@ struct DSpecies {
   int pad0;
   const int* states;  // [n_seg * S] bead type per (segment, slot), -1 padding
   const int* nst;     // [n_seg] states per segment
+  const int* bnd;     // [(g * S + i) * S + j] bond type between state i of segment g and state j of g+1, -1 if none
   const double* md;   // [n_seg] max path distance from segment g to segment 0 (fixed species)
   double fixed_density;
   double mu_species;  // bulk chemical potential (set to 0 for grafted species each evaluation)
@@ -57,6 +58,7 @@ struct DReq {
   int NB, MB, NS;
   int funcs;          // SDFT_FUNC_* bits
   int TB;             // transform buffers in shared memory for this launch (1..kMaxTB)
+  int ngrp;           // distinct bead diameters
   double dz, lB, total_charge;
   long long n;        // Anderson unknowns
   // per-bead / per-bond constants
@@ -64,6 +66,8 @@ struct DReq {
   const double* z;    // [NB]
   const double* dmu;  // [NB]
   const int* bonds;   // [MB * 2]
+  const int* grp;     // [NB] index of the bead's diameter in grp_sig
+  const double* grp_sig;  // [ngrp] distinct diameters
   const DSpecies* sp; // [NS]
   // fixed fields
   const double* Ext;      // [NB * P]
@@ -92,6 +96,7 @@ struct DReq {
   double* wb;             // [MB * 2 * P]  scratch (bond weighted densities)
   double* wc;             // [max(NB, 6 + MB) * P] scratch (derivative fields)
   double* wd;             // [2 * NB * P] scratch (per-bead FMT weighted densities)
+  double* fbe;            // [4 * MB * P] bond-end factors of the current x: e^{-lambda_j + lng/2} trapez_j, then e^{lng/2}
   // Anderson
   double* hx;             // [m * n] history of x
   double* hg;             // [m * n] history of G(x) - x

@@ -33,14 +33,6 @@ __device__ __forceinline__ const double* xs_psi(const DReq& r, const double* x) 
 }
 __device__ __forceinline__ size_t off_psic(const DReq& r) { return (size_t)r.NP * (r.NB + 2 * r.MB + 1); }
 
-__device__ __forceinline__ int bond_of(const DReq& r, int a, int b) {
-  // bond table: sorted (min, max) pairs
-  int lo = a < b ? a : b, hi = a < b ? b : a;
-  for (int u = 0; u < r.MB; u++)
-    if (r.bonds[2 * u] == lo && r.bonds[2 * u + 1] == hi) return u;
-  return -1;
-}
-
 __device__ __forceinline__ double dist2_grid(int K, int c, double dz) {
   double d = (double)(K - c) * dz;
   return d * d;
@@ -58,6 +50,25 @@ __device__ void stage_lambda(const DReq& r) {
     int j = idx / P, K = idx - j * P;
     double p = psi[K] + psic;
     r.lambda[idx] = mu[idx] + p * r.z[j] + r.Ext[idx] + r.dmu[j];
+  }
+  __syncthreads();
+}
+
+// Bond-end factors of the propagator convolutions for the current x, one pair
+// of fields per bond end (b, e) with bead j = bonds[2b + e]:
+//   Fin  = e^{-lambda_j + lng_{b,e}/2} trapez_j   (the input factor of a
+//          convolution towards the bead at this end, child_propagators.jl:118-133)
+//   Fout = e^{lng_{b,e}/2}                          (the output factor at this end)
+// computed once per evaluation instead of once per (segment, state pair).
+__device__ void stage_bond_factors(const DReq& r) {
+  const int P = r.NP, nbe = 2 * r.MB;
+  const double* lng = xs_lng(r, r.x);
+  for (int idx = threadIdx.x; idx < nbe * P; idx += blockDim.x) {
+    const int be = idx / P, K = idx - be * P;
+    const int j = r.bonds[be];
+    const double l = lng[idx];
+    r.fbe[idx] = exp(-r.lambda[(size_t)j * P + K] + l / 2.0) * r.trapez[(size_t)j * P + K];
+    r.fbe[(size_t)nbe * P + idx] = exp(l / 2.0);
   }
   __syncthreads();
 }
@@ -102,7 +113,7 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
       for (int pi = 0; pi < npair; pi++) {
         const int ii = pi / nc, jj = pi - ii * nc;
         const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
-        const int bond = bond_of(r, si, sj);
+        const int bond = s.bnd[(p * S + ii) * S + jj];
         const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
         double* out = s.gC + ((size_t)(p * S + ii) * S + jj) * P;
         const double* lam_j = r.lambda + (size_t)sj * P;
@@ -135,41 +146,39 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
         for (int K = threadIdx.x; K < P; K += blockDim.x) out[K] = (K == Kp) ? acc : 0.0;
       }
     } else {
+      const double* fin = r.fbe;
+      const double* fout = r.fbe + (size_t)2 * r.MB * P;
       for (int g0 = 0; g0 < npair; g0 += r.TB) {
         const int nT = min(r.TB, npair - g0);
-        const double* lam_t[kMaxTB];
-        const double* lngj_t[kMaxTB];
-        const double* lngi_t[kMaxTB];
-        const double* tr_t[kMaxTB];
+        const double* in_t[kMaxTB];
+        const double* out_f[kMaxTB];
         const double* gcc_t[kMaxTB];
         const double* wb_t[kMaxTB];
         double* out_t[kMaxTB];
         for (int t = 0; t < nT; t++) {
           const int pi = g0 + t, ii = pi / nc, jj = pi - ii * nc;
           const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
-          const int bond = bond_of(r, si, sj);
+          const int bond = s.bnd[(p * S + ii) * S + jj];
           const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
           out_t[t] = s.gC + ((size_t)(p * S + ii) * S + jj) * P;
-          lam_t[t] = r.lambda + (size_t)sj * P;
-          lngj_t[t] = lng + (size_t)(bond * 2 + pair_j) * P;
-          lngi_t[t] = lng + (size_t)(bond * 2 + pair_i) * P;
-          tr_t[t] = r.trapez + (size_t)sj * P;
+          in_t[t] = fin + (size_t)(bond * 2 + pair_j) * P;
+          out_f[t] = fout + (size_t)(bond * 2 + pair_i) * P;
           gcc_t[t] = (c < N - 1) ? s.gC + ((size_t)(c * S + jj) * S) * P : nullptr;
           wb_t[t] = r.Wbond + (size_t)bond * P;
         }
         dct2_convolve_b(
             fc, nT,
             [&](int t, int K) {
-              double f = exp(-lam_t[t][K] + lngj_t[t][K] / 2.0);
+              double f = in_t[t][K];
               if (gcc_t[t]) {
                 double q2 = 0.0;
                 for (int q = 0; q < S; q++) q2 += gcc_t[t][(size_t)q * P + K];
                 f *= q2;
               }
-              return f * tr_t[t][K];
+              return f;
             },
-            [&](int t, int q) { return wb_t[t][q]; },
-            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * exp(lngi_t[t][K] / 2.0) * inv_norm; });
+            [&](int t, int q) { return __ldg(&wb_t[t][q]); },
+            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * out_f[t][K] * inv_norm; });
       }
     }
     if (s.fixed >= 0) {  // max-distance mask (child_propagators.jl:147-157)
@@ -222,7 +231,7 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
       for (int pi = 0; pi < npair; pi++) {
         const int ii = pi / np_, jj = pi - ii * np_;
         const int si = s.states[c * S + ii], sj = s.states[p * S + jj];
-        const int bond = bond_of(r, si, sj);
+        const int bond = s.bnd[(p * S + jj) * S + ii];
         const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
         double* out = s.gP + ((size_t)(c * S + ii) * S + jj) * P;
         const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
@@ -247,25 +256,23 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
         __syncthreads();
       }
     } else {
+      const double* fin = r.fbe;
+      const double* fout = r.fbe + (size_t)2 * r.MB * P;
       for (int g0 = 0; g0 < npair; g0 += r.TB) {
         const int nT = min(r.TB, npair - g0);
-        const double* lam_t[kMaxTB];
-        const double* lngj_t[kMaxTB];
-        const double* lngi_t[kMaxTB];
-        const double* tr_t[kMaxTB];
+        const double* in_t[kMaxTB];
+        const double* out_f[kMaxTB];
         const double* gpp_t[kMaxTB];
         const double* wb_t[kMaxTB];
         double* out_t[kMaxTB];
         for (int t = 0; t < nT; t++) {
           const int pi = g0 + t, ii = pi / np_, jj = pi - ii * np_;
           const int si = s.states[c * S + ii], sj = s.states[p * S + jj];
-          const int bond = bond_of(r, si, sj);
+          const int bond = s.bnd[(p * S + jj) * S + ii];
           const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
           out_t[t] = s.gP + ((size_t)(c * S + ii) * S + jj) * P;
-          lam_t[t] = r.lambda + (size_t)sj * P;
-          lngj_t[t] = lng + (size_t)(bond * 2 + pair_j) * P;
-          lngi_t[t] = lng + (size_t)(bond * 2 + pair_i) * P;
-          tr_t[t] = r.trapez + (size_t)sj * P;
+          in_t[t] = fin + (size_t)(bond * 2 + pair_j) * P;
+          out_f[t] = fout + (size_t)(bond * 2 + pair_i) * P;
           gpp_t[t] = s.gP + ((size_t)(p * S + jj) * S) * P;
           wb_t[t] = r.Wbond + (size_t)bond * P;
         }
@@ -274,10 +281,10 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
             [&](int t, int K) {
               double q2 = 0.0;
               for (int q = 0; q < S; q++) q2 += gpp_t[t][(size_t)q * P + K];
-              return exp(-lam_t[t][K] + lngj_t[t][K] / 2.0) * q2 * tr_t[t][K];
+              return in_t[t][K] * q2;
             },
-            [&](int t, int q) { return wb_t[t][q]; },
-            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * exp(lngi_t[t][K] / 2.0) * inv_norm; });
+            [&](int t, int q) { return __ldg(&wb_t[t][q]); },
+            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * out_f[t][K] * inv_norm; });
       }
     }
     if (s.fixed >= 0) {
@@ -369,8 +376,7 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, 
         if (g < N - 1) {
           temp = 0.0;
           for (int jj = 0; jj < s.nst[g + 1]; jj++) {
-            const int sj = s.states[(g + 1) * S + jj];
-            const int bond = bond_of(r, si, sj);
+            const int bond = s.bnd[(g * S + ii) * S + jj];
             const double t2 = s.gC[((size_t)(g * S + ii) * S + jj) * P + K];
             r.rho_bonds[(size_t)(bond * 2 + 0) * P + K] += contr * t2;
             temp += t2;
@@ -392,8 +398,7 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, 
           contr *= t;
         }
         for (int jj = 0; jj < s.nst[c - 1]; jj++) {
-          const int sj = s.states[(c - 1) * S + jj];
-          const int bond = bond_of(r, si, sj);
+          const int bond = s.bnd[((c - 1) * S + jj) * S + ii];
           r.rho_bonds[(size_t)(bond * 2 + 1) * P + K] += contr * s.gP[((size_t)(c * S + ii) * S + jj) * P + K];
         }
       }
@@ -741,6 +746,93 @@ __device__ __forceinline__ MsaGamma gamma_msa_pt(const double* rho, const double
   return out;
 }
 
+// The same damped iteration with the bead sums taken per diameter group: with
+// c_g = sum rho_j, b_g = sum rho_j z_j, a_g = sum rho_j z_j^2 over the beads of
+// diameter s_g,
+//   sum_j rho_j s_j^3 / (1 + G s_j)          = sum_g c_g s_g^3 / (1 + G s_g)
+//   sum_j rho_j z_j s_j / (1 + G s_j)        = sum_g b_g s_g / (1 + G s_g)
+//   sum_j rho_j (z_j - eta s_j^2)^2 / (1 + G s_j)^2
+//                        = sum_g (a_g - 2 eta s_g^2 b_g + eta^2 s_g^4 c_g) / (1 + G s_g)^2,
+// so an iteration costs O(groups) instead of O(beads) (equal up to rounding).
+constexpr int kMaxGroups = 4;
+
+__device__ __forceinline__ MsaGamma gamma_msa_grouped(const DReq& r, const double* rho) {
+  const int nb = r.NB;
+  const double lB = r.lB;
+  const double tol = 1e-10;
+  double s = 0.0, sr = 0.0, srs = 0.0, s3 = 0.0;
+  double cg[kMaxGroups], bg[kMaxGroups], ag[kMaxGroups], sg[kMaxGroups];
+#pragma unroll
+  for (int q = 0; q < kMaxGroups; q++) {
+    cg[q] = bg[q] = ag[q] = 0.0;
+    sg[q] = q < r.ngrp ? r.grp_sig[q] : 0.0;
+  }
+  for (int j = 0; j < nb; j++) {
+    const double rj = rho[j], zj = r.z[j], sj = r.sig[j];
+    const int gj = r.grp[j];
+    s += rj * zj * zj;
+    sr += rj * sj;
+    srs += rj;
+    s3 += rj * sj * sj * sj;
+#pragma unroll
+    for (int q = 0; q < kMaxGroups; q++)
+      if (q == gj) {
+        cg[q] += rj;
+        bg[q] += rj * zj;
+        ag[q] += rj * zj * zj;
+      }
+  }
+  const double kappa = sqrt(4.0 * kPi * lB * s);
+  MsaGamma out;
+  if (kappa < tol) {
+    out.G = kappa / 2.0;
+    out.eta = 0.0;
+    out.H = 2.0 / kPi;
+    return out;
+  }
+  const double sig_eff = sr / srs;
+  const double xx = sig_eff * sqrt(4.0 * kPi * lB * s);
+  double G = (sqrt(1.0 + 2.0 * xx) - 1.0) / (2.0 * sig_eff);
+  const double term2 = 2.0 / kPi * (1.0 - kPi / 6.0 * s3);
+  double eta = 0.0, H = 0.0;
+  for (int it = 1;; it++) {
+    double hs = 0.0, es = 0.0, inv[kMaxGroups];
+#pragma unroll
+    for (int q = 0; q < kMaxGroups; q++)
+      if (q < r.ngrp) {
+        inv[q] = 1.0 / (1.0 + G * sg[q]);
+        hs += cg[q] * sg[q] * sg[q] * sg[q] * inv[q];
+        es += bg[q] * sg[q] * inv[q];
+      }
+    H = hs + term2;
+    eta = es / H;
+    double gs = 0.0;
+#pragma unroll
+    for (int q = 0; q < kMaxGroups; q++)
+      if (q < r.ngrp) {
+        const double s2 = sg[q] * sg[q];
+        gs += (ag[q] - 2.0 * eta * s2 * bg[q] + eta * eta * s2 * s2 * cg[q]) * (inv[q] * inv[q]);
+      }
+    const double G1 = sqrt(kPi * lB * gs);
+    const double Gn = 0.9 * G + 0.1 * G1;
+    if (fabs(G1 - G) < tol || it >= 1000) {
+      G = Gn;
+      break;
+    }
+    G = Gn;
+  }
+  out.G = G;
+  out.eta = eta;
+  out.H = H;
+  return out;
+}
+
+// Gamma at one point: grouped when the diameters fall into few groups
+__device__ __forceinline__ MsaGamma gamma_msa_point(const DReq& r, const double* rho) {
+  if (r.ngrp <= kMaxGroups) return gamma_msa_grouped(r, rho);
+  return gamma_msa_pt(rho, r.sig, r.z, r.NB, r.lB);
+}
+
 __device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
   const int P = r.NP, NB = r.NB, MB = r.MB;
   const FftCtx fc = make_fft(sh.z, r);
@@ -775,7 +867,7 @@ __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
   for (int K = threadIdx.x; K < P; K += blockDim.x) {
     double rho[kMaxBeads], dphi[kMaxBeads];
     for (int j = 0; j < NB; j++) rho[j] = r.wa[(size_t)j * P + K];
-    const MsaGamma gm = gamma_msa_pt(rho, sig, Z, NB, lB);
+    const MsaGamma gm = gamma_msa_point(r, rho);
     const double G = gm.G, eta = gm.eta, H = gm.H;
     double us = 0.0;
     for (int j = 0; j < NB; j++)
@@ -934,6 +1026,7 @@ __device__ double stage_neutrality(const DReq& r, Shared sh) {
 __device__ bool objective(const DReq& r, Shared sh) {
   const int P = r.NP;
   stage_lambda(r);
+  stage_bond_factors(r);
   int bad = -1;
   if (!stage_densities(r, sh, &bad)) return false;
   stage_rho_hat(r, sh);

@@ -59,7 +59,7 @@ __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
     for (int K = threadIdx.x; K < P; K += blockDim.x) {
       double rho[kMaxBeads];
       for (int j = 0; j < NB; j++) rho[j] = r.wa[(size_t)j * P + K];
-      const MsaGamma gm = gamma_msa_pt(rho, r.sig, r.z, NB, r.lB);
+      const MsaGamma gm = gamma_msa_point(r, rho);
       double s = 0.0;
       for (int j = 0; j < NB; j++) s += rho[j] * r.z[j] * (r.z[j] * gm.G + gm.eta * r.sig[j]) / (1.0 + gm.G * r.sig[j]);
       double f = (gm.G * gm.G * gm.G) / (3.0 * kPi) - r.lB * s;

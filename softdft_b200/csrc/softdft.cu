@@ -131,50 +131,10 @@ static size_t smem_bytes(int M);
 
 struct SpeciesHost {
   int n_seg, S, fixed;
-  std::vector<int> states, nst;
+  std::vector<int> states, nst, bnd;
   std::vector<double> md;
   double fixed_density, mu_species, normative, norm_free;
 };
-
-struct sdft_request {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int precision = SDFT_PREC_FP64;
-  int NP = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
-  long long n = 0;
-  std::vector<SpeciesHost> sp;
-  char* dmem = nullptr;
-  size_t bytes = 0;
-  DReq h{};            // host copy of the device descriptor
-  DReq* dreq = nullptr;
-  SolveSlot* dslot = nullptr;
-  double* dout = nullptr;  // omega + num species
-  int anderm_alloc = 0;
-  size_t hist_off = 0;
-};
-
-extern "C" int32_t sdft_abi_version(void) { return SDFT_ABI_VERSION; }
-extern "C" const char* sdft_last_error(void) { return g_err.c_str(); }
-
-extern "C" int sdft_device_count(int32_t* count) {
-  int c = 0;
-  cudaError_t e = cudaGetDeviceCount(&c);
-  if (e != cudaSuccess) {
-    *count = 0;
-    return set_err(SDFT_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
-  }
-  *count = c;
-  return SDFT_OK;
-}
-
-extern "C" void sdft_numerics_default(sdft_numerics* o) {
-  o->max_iters = 100000;
-  o->anderm = 5;
-  o->damping = 0.5;
-  o->mixing_max = 1.0;
-  o->switch_tole = 1e-3;
-  o->tole = 1e-6;
-}
 
 namespace {
 
@@ -230,14 +190,35 @@ int bond_lookup(const std::vector<int>& bonds, int a, int b) {
   return -1;
 }
 
-}  // namespace
+// Everything a request needs on the device, derived from the descriptor once:
+// validated species, the byte layout of one device block and the host-built
+// tables.  sdft_request_create places it in its own allocation (with Anderson
+// history), sdft_objective_noalloc in the library's static scratch array.
+struct Plan {
+  int P = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
+  long long n = 0;
+  bool history = false;
+  std::vector<int> bonds;
+  std::vector<SpeciesHost> sp;
+  std::vector<int> grp;          // [NB] diameter group of each bead type
+  std::vector<double> grp_sig;   // [ngrp] group diameters
+  // layout
+  size_t o_sig = 0, o_z = 0, o_dmu = 0, o_bonds = 0, o_grp = 0, o_grp_sig = 0, o_sp = 0;
+  std::vector<size_t> o_states, o_nst, o_bnd, o_md, o_gC, o_gP, o_rho, o_expo;
+  size_t o_Ext = 0, o_tr = 0, o_Csurf = 0, o_Wbond = 0, o_Wfmt = 0, o_Wmsa = 0, o_Wcoul = 0, o_tw = 0, o_twP = 0, o_twD = 0;
+  size_t o_x = 0, o_g = 0, o_lam = 0, o_rb = 0, o_rbo = 0, o_Cb = 0, o_Cbond = 0, o_Cmu = 0, o_Clng = 0;
+  size_t o_wa = 0, o_wb = 0, o_wc = 0, o_wd = 0, o_fbe = 0;
+  size_t o_hx = 0, o_hg = 0, o_u = 0;
+  size_t o_status = 0, o_iters = 0, o_err = 0, o_scal = 0, o_dreq = 0, o_slot = 0, o_out = 0;
+  size_t bytes = 0;
+  // host tables
+  std::vector<double> Ext, tr, Csurf, Wbond, Wfmt, Wmsa, Wcoul, x0;
+  std::vector<double2> tw, twP, twD;
+};
 
-extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
-  if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
-  *out = nullptr;
-  if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
-  if (precision != SDFT_PREC_FP64)
-    return set_err(SDFT_ERR_UNSUPPORTED, "only the FP64 precision is available in this build");
+// validation of the descriptor (the device solve's supported subset) and the
+// per-species host data
+int plan_species(const sdft_system_desc* d, Plan& pl) {
   const int P = d->np;
   if (P < 16 || (P & (P - 1)) != 0)
     return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP = 2^k >= 16 (got " + std::to_string(P) + ")");
@@ -246,64 +227,40 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
   if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
   if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
   if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(SDFT_ERR_CUDA, "no CUDA device");
-  auto* q = new sdft_request();
-  cudaGetDevice(&q->device);
-  q->precision = precision;
-  q->NP = P;
-  q->M = P / 2;
-  q->L = 0;
-  while ((1 << q->L) < q->M) q->L++;
-  q->NB = d->nb;
-  q->MB = d->mb;
-  q->NS = d->n_species;
-  const int NB = q->NB, MB = q->MB, NS = q->NS, M = q->M;
-  const int NPS = 2 * P;
-  q->n = (long long)P * (NB + 2 * MB + 1) + 1;
-  std::vector<int> bonds(d->bond_types, d->bond_types + 2 * MB);
-  // species
-  size_t gC_elems = 0, rho_elems = 0;
-  for (int u = 0; u < NS; u++) {
+  pl.P = P;
+  pl.M = P / 2;
+  pl.L = 0;
+  while ((1 << pl.L) < pl.M) pl.L++;
+  pl.NB = d->nb;
+  pl.MB = d->mb;
+  pl.NS = d->n_species;
+  pl.n = (long long)P * (pl.NB + 2 * pl.MB + 1) + 1;
+  pl.bonds.assign(d->bond_types, d->bond_types + 2 * pl.MB);
+  const int NB = pl.NB;
+  for (int u = 0; u < pl.NS; u++) {
     const sdft_species_desc& s = d->species[u];
     SpeciesHost h;
     h.n_seg = s.n_seg;
     h.S = s.max_states;
-    if (h.n_seg < 1 || h.S < 1 || h.S > kMaxStates) {
-      delete q;
+    if (h.n_seg < 1 || h.S < 1 || h.S > kMaxStates)
       return set_err(SDFT_ERR_UNSUPPORTED, "segments >= 1 and 1 <= states <= 4 per segment are required");
-    }
     for (int g = 0; g < h.n_seg; g++) {
-      if (s.parent[g] != g - 1) {
-        delete q;
+      if (s.parent[g] != g - 1)
         return set_err(SDFT_ERR_UNSUPPORTED, "the device solve supports linear chains (parent of segment g is g-1)");
-      }
-      if (s.n_states[g] < 1 || s.n_states[g] > h.S) {
-        delete q;
-        return set_err(SDFT_ERR_ARG, "n_states out of range");
-      }
+      if (s.n_states[g] < 1 || s.n_states[g] > h.S) return set_err(SDFT_ERR_ARG, "n_states out of range");
     }
     h.nst.assign(s.n_states, s.n_states + h.n_seg);
     h.states.assign(s.states, s.states + (size_t)h.n_seg * h.S);
     h.fixed = -1;
     if (s.fixed_coord) {
-      for (int g = 0; g < h.n_seg; g++) {
-        if (s.fixed_coord[g] >= 0 && g != 0) {
-          delete q;
-          return set_err(SDFT_ERR_UNSUPPORTED, "only segment 0 can be fixed in a 1D slit");
-        }
-      }
+      for (int g = 1; g < h.n_seg; g++)
+        if (s.fixed_coord[g] >= 0) return set_err(SDFT_ERR_UNSUPPORTED, "only segment 0 can be fixed in a 1D slit");
       h.fixed = s.fixed_coord[0];
     }
     if (h.fixed >= 0) {
-      if (h.fixed >= P || h.n_seg < 2 || !s.max_distance) {
-        delete q;
+      if (h.fixed >= P || h.n_seg < 2 || !s.max_distance)
         return set_err(SDFT_ERR_ARG, "fixed segment needs a grid point, a free segment and max_distance");
-      }
-      if (h.n_seg == 2 && h.nst[1] > 1) {
-        delete q;
-        return set_err(SDFT_ERR_UNSUPPORTED, "grafted dimer with a multi-state free segment");
-      }
+      if (h.n_seg == 2 && h.nst[1] > 1) return set_err(SDFT_ERR_UNSUPPORTED, "grafted dimer with a multi-state free segment");
       h.md.resize(h.n_seg);
       for (int g = 0; g < h.n_seg; g++) h.md[g] = s.max_distance[(size_t)g * h.n_seg + 0];
     } else {
@@ -312,17 +269,19 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
     for (int g = 0; g < h.n_seg; g++)
       for (int i = 0; i < h.nst[g]; i++) {
         int st = h.states[(size_t)g * h.S + i];
-        if (st < 0 || st >= NB) {
-          delete q;
-          return set_err(SDFT_ERR_ARG, "state bead type out of range");
-        }
+        if (st < 0 || st >= NB) return set_err(SDFT_ERR_ARG, "state bead type out of range");
         if (g > 0)
           for (int j = 0; j < h.nst[g - 1]; j++)
-            if (bond_lookup(bonds, st, h.states[(size_t)(g - 1) * h.S + j]) < 0) {
-              delete q;
+            if (bond_lookup(pl.bonds, st, h.states[(size_t)(g - 1) * h.S + j]) < 0)
               return set_err(SDFT_ERR_ARG, "bond missing from bond_types");
-            }
       }
+    // bond type between state i of segment g and state j of segment g + 1
+    h.bnd.assign((size_t)h.n_seg * h.S * h.S, -1);
+    for (int g = 0; g + 1 < h.n_seg; g++)
+      for (int i = 0; i < h.nst[g]; i++)
+        for (int j = 0; j < h.nst[g + 1]; j++)
+          h.bnd[((size_t)g * h.S + i) * h.S + j] =
+              bond_lookup(pl.bonds, h.states[(size_t)g * h.S + i], h.states[(size_t)(g + 1) * h.S + j]);
     h.fixed_density = s.fixed_density;
     h.mu_species = s.mu_species;
     // normative (child_propagators.jl:41-50): levels are visited leaves first
@@ -334,49 +293,358 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
     }
     h.normative = nv;
     h.norm_free = std::pow(nv, (double)(h.n_seg - 1));
-    if (h.n_seg > 1) gC_elems += (size_t)h.n_seg * h.S * h.S * P;
-    rho_elems += (size_t)h.n_seg * h.S * P;
-    q->sp.push_back(h);
+    pl.sp.push_back(h);
   }
-  // ---- layout
-  const int m_alloc = kMaxAnderson;
-  q->anderm_alloc = m_alloc;
+  // bead types of equal diameter share the MSA screening sums
+  pl.grp.assign(NB, 0);
+  pl.grp_sig.clear();
+  for (int j = 0; j < NB; j++) {
+    int g = -1;
+    for (size_t q = 0; q < pl.grp_sig.size(); q++)
+      if (pl.grp_sig[q] == d->diameter[j]) g = (int)q;
+    if (g < 0) {
+      g = (int)pl.grp_sig.size();
+      pl.grp_sig.push_back(d->diameter[j]);
+    }
+    pl.grp[j] = g;
+  }
+  return SDFT_OK;
+}
+
+void plan_layout(Plan& pl, bool history) {
+  const int P = pl.P, NB = pl.NB, MB = pl.MB, NS = pl.NS, M = pl.M;
+  pl.history = history;
   const int nwa = std::max(NB, 6), nwc = std::max(NB + MB, 6 + MB);
   Layout lay;
-  size_t o_sig = lay.take<double>(NB), o_z = lay.take<double>(NB), o_dmu = lay.take<double>(NB);
-  size_t o_bonds = lay.take<int>(2 * MB + 2);
-  size_t o_sp = lay.take<DSpecies>(NS);
-  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS), o_expo(NS);
+  pl.o_sig = lay.take<double>(NB);
+  pl.o_z = lay.take<double>(NB);
+  pl.o_dmu = lay.take<double>(NB);
+  pl.o_bonds = lay.take<int>(2 * MB + 2);
+  pl.o_grp = lay.take<int>(NB);
+  pl.o_grp_sig = lay.take<double>(NB);
+  pl.o_sp = lay.take<DSpecies>(NS);
+  pl.o_states.resize(NS);
+  pl.o_nst.resize(NS);
+  pl.o_bnd.resize(NS);
+  pl.o_md.resize(NS);
+  pl.o_gC.resize(NS);
+  pl.o_gP.resize(NS);
+  pl.o_rho.resize(NS);
+  pl.o_expo.resize(NS);
   for (int u = 0; u < NS; u++) {
-    const SpeciesHost& h = q->sp[u];
-    o_states[u] = lay.take<int>(h.states.size());
-    o_nst[u] = lay.take<int>(h.nst.size());
-    o_md[u] = lay.take<double>(h.md.size());
+    const SpeciesHost& h = pl.sp[u];
+    pl.o_states[u] = lay.take<int>(h.states.size());
+    pl.o_nst[u] = lay.take<int>(h.nst.size());
+    pl.o_bnd[u] = lay.take<int>(h.bnd.size());
+    pl.o_md[u] = lay.take<double>(h.md.size());
     size_t gsz = h.n_seg > 1 ? (size_t)h.n_seg * h.S * h.S * P : 0;
-    o_gC[u] = lay.take<double>(gsz);
-    o_gP[u] = lay.take<double>(gsz);
-    o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
-    o_expo[u] = lay.take<int>((size_t)2 * h.n_seg);
+    pl.o_gC[u] = lay.take<double>(gsz);
+    pl.o_gP[u] = lay.take<double>(gsz);
+    pl.o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
+    pl.o_expo[u] = lay.take<int>((size_t)2 * h.n_seg);
   }
-  size_t o_Ext = lay.take<double>((size_t)NB * P), o_tr = lay.take<double>((size_t)NB * P);
-  size_t o_Csurf = lay.take<double>(P);
-  size_t o_Wbond = lay.take<double>((size_t)MB * P + 1), o_Wfmt = lay.take<double>((size_t)NB * 3 * P);
-  size_t o_Wmsa = lay.take<double>((size_t)NB * P), o_Wcoul = lay.take<double>(P);
-  size_t o_tw = lay.take<double2>(M / 2 + 1), o_twP = lay.take<double2>(M + 1), o_twD = lay.take<double2>(M + 1);
-  size_t o_x = lay.take<double>(q->n), o_g = lay.take<double>(q->n);
-  size_t o_lam = lay.take<double>((size_t)NB * P), o_rb = lay.take<double>((size_t)NB * P);
-  size_t o_rbo = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_Cb = lay.take<double>((size_t)NB * P), o_Cbond = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_Cmu = lay.take<double>((size_t)NB * P), o_Clng = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_wa = lay.take<double>((size_t)nwa * P), o_wb = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_wc = lay.take<double>((size_t)nwc * P);
-  size_t o_wd = lay.take<double>((size_t)2 * NB * P);
-  size_t o_hx = lay.take<double>((size_t)m_alloc * q->n), o_hg = lay.take<double>((size_t)m_alloc * q->n);
-  size_t o_u = lay.take<double>(q->n);
-  size_t o_status = lay.take<int>(4), o_iters = lay.take<int>(4), o_err = lay.take<double>(4);
-  size_t o_scal = lay.take<double>(8);
-  size_t o_dreq = lay.take<DReq>(1), o_slot = lay.take<SolveSlot>(1), o_out = lay.take<double>(1 + NS);
-  q->bytes = lay.off;
+  pl.o_Ext = lay.take<double>((size_t)NB * P);
+  pl.o_tr = lay.take<double>((size_t)NB * P);
+  pl.o_Csurf = lay.take<double>(P);
+  pl.o_Wbond = lay.take<double>((size_t)MB * P + 1);
+  pl.o_Wfmt = lay.take<double>((size_t)NB * 3 * P);
+  pl.o_Wmsa = lay.take<double>((size_t)NB * P);
+  pl.o_Wcoul = lay.take<double>(P);
+  pl.o_tw = lay.take<double2>(M / 2 + 1);
+  pl.o_twP = lay.take<double2>(M + 1);
+  pl.o_twD = lay.take<double2>(M + 1);
+  if (history) {
+    pl.o_x = lay.take<double>(pl.n);
+    pl.o_g = lay.take<double>(pl.n);
+  }
+  pl.o_lam = lay.take<double>((size_t)NB * P);
+  pl.o_rb = lay.take<double>((size_t)NB * P);
+  pl.o_rbo = lay.take<double>((size_t)MB * 2 * P + 1);
+  pl.o_Cb = lay.take<double>((size_t)NB * P);
+  pl.o_Cbond = lay.take<double>((size_t)MB * 2 * P + 1);
+  pl.o_Cmu = lay.take<double>((size_t)NB * P);
+  pl.o_Clng = lay.take<double>((size_t)MB * 2 * P + 1);
+  pl.o_wa = lay.take<double>((size_t)nwa * P);
+  pl.o_wb = lay.take<double>((size_t)MB * 2 * P + 1);
+  pl.o_wc = lay.take<double>((size_t)nwc * P);
+  pl.o_wd = lay.take<double>((size_t)2 * NB * P);
+  pl.o_fbe = lay.take<double>((size_t)4 * MB * P + 1);
+  if (history) {
+    pl.o_hx = lay.take<double>((size_t)kMaxAnderson * pl.n);
+    pl.o_hg = lay.take<double>((size_t)kMaxAnderson * pl.n);
+    pl.o_u = lay.take<double>(pl.n);
+  }
+  pl.o_status = lay.take<int>(4);
+  pl.o_iters = lay.take<int>(4);
+  pl.o_err = lay.take<double>(4);
+  pl.o_scal = lay.take<double>(8);
+  pl.o_dreq = lay.take<DReq>(1);
+  if (history) {
+    pl.o_slot = lay.take<SolveSlot>(1);
+    pl.o_out = lay.take<double>(1 + NS);
+  }
+  pl.bytes = lay.off;
+}
+
+void plan_tables(const sdft_system_desc* d, Plan& pl) {
+  const int P = pl.P, NB = pl.NB, MB = pl.MB, M = pl.M, NPS = 2 * P;
+  pl.Ext.assign((size_t)NB * P, 0.0);
+  pl.tr.assign((size_t)NB * P, 1.0);
+  if (d->hard_walls) {  // hard_walls.jl:6-46
+    for (int K = 0; K < P; K++) {
+      int idx = K + 1;
+      for (int j = 0; j < NB; j++) {
+        double dd = d->diameter[j];
+        int lo = jround((0.0 + dd / 2.0) / d->bin_width) + 1;
+        int hi = jround((d->length - dd / 2.0) / d->bin_width) + 1;
+        size_t qq = (size_t)j * P + K;
+        if (idx < lo) {
+          pl.Ext[qq] += 1.0e20;
+          pl.tr[qq] = 1.0;
+        } else if (idx == lo) {
+          pl.tr[qq] = 0.5;
+        }
+        if (idx > hi) {
+          pl.Ext[qq] += 1.0e20;
+          pl.tr[qq] = 1.0;
+        } else if (idx == hi) {
+          pl.tr[qq] = 0.5;
+        }
+      }
+    }
+  }
+  std::vector<double> surf(P, 0.0);
+  pl.Csurf.assign(P, 0.0);
+  if (d->charged_walls) {  // charged_walls.jl:7-57
+    double pos[2] = {0.0, d->length};
+    for (int w = 0; w < 2; w++) {
+      int gp = jround(pos[w] / d->bin_width) + 1;
+      if (gp >= 1 && gp <= P) surf[gp - 1] += d->wall_charge[w] * (1.0 / d->bin_width);
+    }
+    for (int k = 0; k < P; k++) {
+      long double acc = 0.0L;
+      for (int K = 0; K < P; K++)
+        if (surf[K] != 0.0) acc += (long double)surf[K] * cosl(3.14159265358979323846264338327950288L * k * (2 * K + 1) / (2.0L * P));
+      pl.Csurf[k] = (double)acc;
+    }
+  }
+  pl.Wbond.assign((size_t)MB * P + 1, 0.0);
+  pl.Wfmt.assign((size_t)NB * 3 * P, 0.0);
+  pl.Wmsa.assign((size_t)NB * P, 0.0);
+  pl.Wcoul.assign(P, 0.0);
+  for (int u = 0; u < MB; u++) {
+    double sij = (d->diameter[pl.bonds[2 * u]] + d->diameter[pl.bonds[2 * u + 1]]) / 2.0;
+    for (int k = 0; k < P; k++)
+      pl.Wbond[(size_t)u * P + k] = filter_k(k, NPS, d->bin_width) * (w_delta(k, NPS, d->bin_width, sij) / (4.0 * kPi * (sij * sij)));
+  }
+  for (int j = 0; j < NB; j++) {
+    double b = d->diameter[j] / 2.0;
+    for (int k = 0; k < P; k++) {
+      pl.Wfmt[((size_t)j * 3 + 0) * P + k] = w_delta(k, NPS, d->bin_width, b);
+      pl.Wfmt[((size_t)j * 3 + 1) * P + k] = w_step(k, NPS, d->bin_width, b);
+      pl.Wfmt[((size_t)j * 3 + 2) * P + k] = w_vec(k, NPS, d->bin_width, b);
+      pl.Wmsa[(size_t)j * P + k] = w_delta(k, NPS, d->bin_width, b) / (4.0 * kPi * (b * b));
+    }
+  }
+  for (int k = 0; k < P; k++) pl.Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
+  const long double PI_L = 3.14159265358979323846264338327950288L;
+  pl.tw.resize(M / 2 + 1);
+  pl.twP.resize(M + 1);
+  pl.twD.resize(M + 1);
+  for (int k = 0; k <= M / 2; k++) pl.tw[k] = cis(-2.0L * PI_L * k / M);
+  for (int k = 0; k <= M; k++) pl.twP[k] = cis(-2.0L * PI_L * k / P);
+  for (int k = 0; k <= M; k++) pl.twD[k] = cis(-PI_L * k / (2.0L * P));
+  if (pl.history) {
+    pl.x0.assign(pl.n, 0.0);
+    for (int j = 0; j < NB; j++)
+      for (int K = 0; K < P; K++) pl.x0[(size_t)j * P + K] = d->mu_ex_bulk[j];
+    for (int u = 0; u < MB; u++)
+      for (int e2 = 0; e2 < 2; e2++)
+        for (int K = 0; K < P; K++) pl.x0[(size_t)P * NB + (size_t)(u * 2 + e2) * P + K] = d->lng_bulk[u];
+  }
+}
+
+// device descriptor of a plan placed at `base`; x and g given for the no-alloc form
+DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x, double* g, std::vector<DSpecies>& dsp) {
+  auto at = [&](size_t o) { return (void*)(base + o); };
+  dsp.assign(pl.NS, DSpecies{});
+  for (int u = 0; u < pl.NS; u++) {
+    const SpeciesHost& h = pl.sp[u];
+    DSpecies& s = dsp[u];
+    s.n_seg = h.n_seg;
+    s.S = h.S;
+    s.fixed = h.fixed;
+    s.states = (const int*)at(pl.o_states[u]);
+    s.nst = (const int*)at(pl.o_nst[u]);
+    s.bnd = (const int*)at(pl.o_bnd[u]);
+    s.md = (const double*)at(pl.o_md[u]);
+    s.fixed_density = h.fixed_density;
+    s.mu_species = h.mu_species;
+    s.normative = h.normative;
+    s.norm_free = h.norm_free;
+    s.lambda_fixed = 1.0;
+    s.gC = h.n_seg > 1 ? (double*)at(pl.o_gC[u]) : nullptr;
+    s.gP = h.n_seg > 1 ? (double*)at(pl.o_gP[u]) : nullptr;
+    s.rho_seg = (double*)at(pl.o_rho[u]);
+    s.expo = (int*)at(pl.o_expo[u]);
+  }
+  DReq r{};
+  r.NP = pl.P;
+  r.M = pl.M;
+  r.L = pl.L;
+  r.NB = pl.NB;
+  r.MB = pl.MB;
+  r.NS = pl.NS;
+  r.funcs = (int)d->functionals;
+  r.TB = tb_for(pl.M);
+  r.ngrp = (int)pl.grp_sig.size();
+  r.dz = d->bin_width;
+  r.lB = d->bjerrum_length;
+  r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
+  r.n = pl.n;
+  r.sig = (const double*)at(pl.o_sig);
+  r.z = (const double*)at(pl.o_z);
+  r.dmu = (const double*)at(pl.o_dmu);
+  r.bonds = (const int*)at(pl.o_bonds);
+  r.grp = (const int*)at(pl.o_grp);
+  r.grp_sig = (const double*)at(pl.o_grp_sig);
+  r.sp = (const DSpecies*)at(pl.o_sp);
+  r.Ext = (const double*)at(pl.o_Ext);
+  r.trapez = (const double*)at(pl.o_tr);
+  r.Csurf = (const double*)at(pl.o_Csurf);
+  r.Wbond = (const double*)at(pl.o_Wbond);
+  r.Wfmt = (const double*)at(pl.o_Wfmt);
+  r.Wmsa = (const double*)at(pl.o_Wmsa);
+  r.Wcoul = (const double*)at(pl.o_Wcoul);
+  r.tw = (const double2*)at(pl.o_tw);
+  r.twP = (const double2*)at(pl.o_twP);
+  r.twD = (const double2*)at(pl.o_twD);
+  r.x = pl.history ? (double*)at(pl.o_x) : x;
+  r.g = pl.history ? (double*)at(pl.o_g) : g;
+  r.lambda = (double*)at(pl.o_lam);
+  r.rho_beads = (double*)at(pl.o_rb);
+  r.rho_bonds = (double*)at(pl.o_rbo);
+  r.Cb = (double*)at(pl.o_Cb);
+  r.Cbond = (double*)at(pl.o_Cbond);
+  r.Cmu = (double*)at(pl.o_Cmu);
+  r.Clng = (double*)at(pl.o_Clng);
+  r.wa = (double*)at(pl.o_wa);
+  r.wb = (double*)at(pl.o_wb);
+  r.wc = (double*)at(pl.o_wc);
+  r.wd = (double*)at(pl.o_wd);
+  r.fbe = (double*)at(pl.o_fbe);
+  r.hx = pl.history ? (double*)at(pl.o_hx) : nullptr;
+  r.hg = pl.history ? (double*)at(pl.o_hg) : nullptr;
+  r.lsq_u = pl.history ? (double*)at(pl.o_u) : nullptr;
+  r.status = (int*)at(pl.o_status);
+  r.iters = (int*)at(pl.o_iters);
+  r.err = (double*)at(pl.o_err);
+  r.scal = (double*)at(pl.o_scal);
+  return r;
+}
+
+// copies the tables and the descriptor of a bound plan; stream-ordered
+cudaError_t plan_upload(const sdft_system_desc* d, const Plan& pl, char* base, const DReq& r,
+                        const std::vector<DSpecies>& dsp, cudaStream_t stream) {
+  const int NB = pl.NB, MB = pl.MB, P = pl.P;
+  cudaError_t ce = cudaSuccess;
+  auto up = [&](size_t o, const void* src, size_t nbytes) {
+    if (ce == cudaSuccess && nbytes) ce = cudaMemcpyAsync(base + o, src, nbytes, cudaMemcpyHostToDevice, stream);
+  };
+  up(pl.o_sig, d->diameter, sizeof(double) * NB);
+  up(pl.o_z, d->valence, sizeof(double) * NB);
+  up(pl.o_dmu, d->delta_muH, sizeof(double) * NB);
+  up(pl.o_bonds, pl.bonds.data(), sizeof(int) * 2 * MB);
+  up(pl.o_grp, pl.grp.data(), sizeof(int) * NB);
+  up(pl.o_grp_sig, pl.grp_sig.data(), sizeof(double) * pl.grp_sig.size());
+  for (int u = 0; u < pl.NS; u++) {
+    const SpeciesHost& h = pl.sp[u];
+    up(pl.o_states[u], h.states.data(), sizeof(int) * h.states.size());
+    up(pl.o_nst[u], h.nst.data(), sizeof(int) * h.nst.size());
+    up(pl.o_bnd[u], h.bnd.data(), sizeof(int) * h.bnd.size());
+    up(pl.o_md[u], h.md.data(), sizeof(double) * h.md.size());
+  }
+  up(pl.o_sp, dsp.data(), sizeof(DSpecies) * pl.NS);
+  up(pl.o_Ext, pl.Ext.data(), sizeof(double) * pl.Ext.size());
+  up(pl.o_tr, pl.tr.data(), sizeof(double) * pl.tr.size());
+  up(pl.o_Csurf, pl.Csurf.data(), sizeof(double) * P);
+  up(pl.o_Wbond, pl.Wbond.data(), sizeof(double) * pl.Wbond.size());
+  up(pl.o_Wfmt, pl.Wfmt.data(), sizeof(double) * pl.Wfmt.size());
+  up(pl.o_Wmsa, pl.Wmsa.data(), sizeof(double) * pl.Wmsa.size());
+  up(pl.o_Wcoul, pl.Wcoul.data(), sizeof(double) * P);
+  up(pl.o_tw, pl.tw.data(), sizeof(double2) * pl.tw.size());
+  up(pl.o_twP, pl.twP.data(), sizeof(double2) * pl.twP.size());
+  up(pl.o_twD, pl.twD.data(), sizeof(double2) * pl.twD.size());
+  if (pl.history) up(pl.o_x, pl.x0.data(), sizeof(double) * pl.n);
+  up(pl.o_dreq, &r, sizeof(DReq));
+  return ce;
+}
+
+}  // namespace
+
+struct sdft_request {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int precision = SDFT_PREC_FP64;
+  int NP = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
+  long long n = 0;
+  std::vector<SpeciesHost> sp;
+  char* dmem = nullptr;
+  size_t bytes = 0;
+  DReq h{};            // host copy of the device descriptor
+  DReq* dreq = nullptr;
+  SolveSlot* dslot = nullptr;
+  double* dout = nullptr;  // omega + num species
+};
+
+extern "C" int32_t sdft_abi_version(void) { return SDFT_ABI_VERSION; }
+extern "C" const char* sdft_last_error(void) { return g_err.c_str(); }
+
+extern "C" int sdft_device_count(int32_t* count) {
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    *count = 0;
+    return set_err(SDFT_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  }
+  *count = c;
+  return SDFT_OK;
+}
+
+extern "C" void sdft_numerics_default(sdft_numerics* o) {
+  o->max_iters = 100000;
+  o->anderm = 5;
+  o->damping = 0.5;
+  o->mixing_max = 1.0;
+  o->switch_tole = 1e-3;
+  o->tole = 1e-6;
+}
+
+extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
+  if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
+  if (precision != SDFT_PREC_FP64)
+    return set_err(SDFT_ERR_UNSUPPORTED, "only the FP64 precision is available in this build");
+  Plan pl;
+  int rc = plan_species(d, pl);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(SDFT_ERR_CUDA, "no CUDA device");
+  plan_layout(pl, true);
+  plan_tables(d, pl);
+  auto* q = new sdft_request();
+  cudaGetDevice(&q->device);
+  q->precision = precision;
+  q->NP = pl.P;
+  q->M = pl.M;
+  q->L = pl.L;
+  q->NB = pl.NB;
+  q->MB = pl.MB;
+  q->NS = pl.NS;
+  q->n = pl.n;
+  q->sp = pl.sp;
+  q->bytes = pl.bytes;
   cudaError_t e = cudaMalloc(&q->dmem, q->bytes);
   if (e != cudaSuccess) {
     delete q;
@@ -388,178 +656,14 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
     delete q;
     return set_err(SDFT_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
-  cudaMemsetAsync(q->dmem, 0, q->bytes, q->stream);
-  char* base = q->dmem;
-  auto P_ = [&](size_t o) { return (void*)(base + o); };
-  // ---- host tables
-  std::vector<double> Ext((size_t)NB * P, 0.0), tr((size_t)NB * P, 1.0);
-  if (d->hard_walls) {  // hard_walls.jl:6-46
-    for (int K = 0; K < P; K++) {
-      int idx = K + 1;
-      for (int j = 0; j < NB; j++) {
-        double dd = d->diameter[j];
-        int lo = jround((0.0 + dd / 2.0) / d->bin_width) + 1;
-        int hi = jround((d->length - dd / 2.0) / d->bin_width) + 1;
-        size_t qq = (size_t)j * P + K;
-        if (idx < lo) {
-          Ext[qq] += 1.0e20;
-          tr[qq] = 1.0;
-        } else if (idx == lo) {
-          tr[qq] = 0.5;
-        }
-        if (idx > hi) {
-          Ext[qq] += 1.0e20;
-          tr[qq] = 1.0;
-        } else if (idx == hi) {
-          tr[qq] = 0.5;
-        }
-      }
-    }
-  }
-  std::vector<double> surf(P, 0.0), Csurf(P, 0.0);
-  if (d->charged_walls) {  // charged_walls.jl:7-57
-    double pos[2] = {0.0, d->length};
-    for (int w = 0; w < 2; w++) {
-      int gp = jround(pos[w] / d->bin_width) + 1;
-      if (gp >= 1 && gp <= P) surf[gp - 1] += d->wall_charge[w] * (1.0 / d->bin_width);
-    }
-    for (int k = 0; k < P; k++) {
-      long double acc = 0.0L;
-      for (int K = 0; K < P; K++)
-        if (surf[K] != 0.0) acc += (long double)surf[K] * cosl(3.14159265358979323846264338327950288L * k * (2 * K + 1) / (2.0L * P));
-      Csurf[k] = (double)acc;
-    }
-  }
-  std::vector<double> Wbond((size_t)MB * P + 1, 0.0), Wfmt((size_t)NB * 3 * P), Wmsa((size_t)NB * P), Wcoul(P);
-  for (int u = 0; u < MB; u++) {
-    double sij = (d->diameter[bonds[2 * u]] + d->diameter[bonds[2 * u + 1]]) / 2.0;
-    for (int k = 0; k < P; k++)
-      Wbond[(size_t)u * P + k] = filter_k(k, NPS, d->bin_width) * (w_delta(k, NPS, d->bin_width, sij) / (4.0 * kPi * (sij * sij)));
-  }
-  for (int j = 0; j < NB; j++) {
-    double b = d->diameter[j] / 2.0;
-    for (int k = 0; k < P; k++) {
-      Wfmt[((size_t)j * 3 + 0) * P + k] = w_delta(k, NPS, d->bin_width, b);
-      Wfmt[((size_t)j * 3 + 1) * P + k] = w_step(k, NPS, d->bin_width, b);
-      Wfmt[((size_t)j * 3 + 2) * P + k] = w_vec(k, NPS, d->bin_width, b);
-      Wmsa[(size_t)j * P + k] = w_delta(k, NPS, d->bin_width, b) / (4.0 * kPi * (b * b));
-    }
-  }
-  for (int k = 0; k < P; k++) Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
-  const long double PI_L = 3.14159265358979323846264338327950288L;
-  std::vector<double2> tw(M / 2 + 1), twP(M + 1), twD(M + 1);
-  for (int k = 0; k <= M / 2; k++) tw[k] = cis(-2.0L * PI_L * k / M);
-  for (int k = 0; k <= M; k++) twP[k] = cis(-2.0L * PI_L * k / P);
-  for (int k = 0; k <= M; k++) twD[k] = cis(-PI_L * k / (2.0L * P));
-  std::vector<double> x0(q->n, 0.0);
-  for (int j = 0; j < NB; j++)
-    for (int K = 0; K < P; K++) x0[(size_t)j * P + K] = d->mu_ex_bulk[j];
-  for (int u = 0; u < MB; u++)
-    for (int e2 = 0; e2 < 2; e2++)
-      for (int K = 0; K < P; K++) x0[(size_t)P * NB + (size_t)(u * 2 + e2) * P + K] = d->lng_bulk[u];
-  // ---- device descriptor
-  std::vector<DSpecies> dsp(NS);
-  for (int u = 0; u < NS; u++) {
-    const SpeciesHost& h = q->sp[u];
-    DSpecies& s = dsp[u];
-    s.n_seg = h.n_seg;
-    s.S = h.S;
-    s.fixed = h.fixed;
-    s.states = (const int*)P_(o_states[u]);
-    s.nst = (const int*)P_(o_nst[u]);
-    s.md = (const double*)P_(o_md[u]);
-    s.fixed_density = h.fixed_density;
-    s.mu_species = h.mu_species;
-    s.normative = h.normative;
-    s.norm_free = h.norm_free;
-    s.lambda_fixed = 1.0;
-    s.gC = h.n_seg > 1 ? (double*)P_(o_gC[u]) : nullptr;
-    s.gP = h.n_seg > 1 ? (double*)P_(o_gP[u]) : nullptr;
-    s.rho_seg = (double*)P_(o_rho[u]);
-    s.expo = (int*)P_(o_expo[u]);
-  }
-  DReq& r = q->h;
-  r.NP = P;
-  r.M = M;
-  r.L = q->L;
-  r.NB = NB;
-  r.MB = MB;
-  r.NS = NS;
-  r.funcs = (int)d->functionals;
-  r.dz = d->bin_width;
-  r.lB = d->bjerrum_length;
-  r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
-  r.n = q->n;
-  r.sig = (const double*)P_(o_sig);
-  r.z = (const double*)P_(o_z);
-  r.dmu = (const double*)P_(o_dmu);
-  r.bonds = (const int*)P_(o_bonds);
-  r.sp = (const DSpecies*)P_(o_sp);
-  r.Ext = (const double*)P_(o_Ext);
-  r.trapez = (const double*)P_(o_tr);
-  r.Csurf = (const double*)P_(o_Csurf);
-  r.Wbond = (const double*)P_(o_Wbond);
-  r.Wfmt = (const double*)P_(o_Wfmt);
-  r.Wmsa = (const double*)P_(o_Wmsa);
-  r.Wcoul = (const double*)P_(o_Wcoul);
-  r.tw = (const double2*)P_(o_tw);
-  r.twP = (const double2*)P_(o_twP);
-  r.twD = (const double2*)P_(o_twD);
-  r.x = (double*)P_(o_x);
-  r.g = (double*)P_(o_g);
-  r.lambda = (double*)P_(o_lam);
-  r.rho_beads = (double*)P_(o_rb);
-  r.rho_bonds = (double*)P_(o_rbo);
-  r.Cb = (double*)P_(o_Cb);
-  r.Cbond = (double*)P_(o_Cbond);
-  r.Cmu = (double*)P_(o_Cmu);
-  r.Clng = (double*)P_(o_Clng);
-  r.wa = (double*)P_(o_wa);
-  r.wb = (double*)P_(o_wb);
-  r.wc = (double*)P_(o_wc);
-  r.wd = (double*)P_(o_wd);
-  r.TB = tb_for(M);
-  r.hx = (double*)P_(o_hx);
-  r.hg = (double*)P_(o_hg);
-  r.lsq_u = (double*)P_(o_u);
-  r.status = (int*)P_(o_status);
-  r.iters = (int*)P_(o_iters);
-  r.err = (double*)P_(o_err);
-  r.scal = (double*)P_(o_scal);
-  q->dreq = (DReq*)P_(o_dreq);
-  q->dslot = (SolveSlot*)P_(o_slot);
-  q->dout = (double*)P_(o_out);
-  auto up = [&](size_t o, const void* src, size_t nbytes) {
-    return cudaMemcpyAsync(base + o, src, nbytes, cudaMemcpyHostToDevice, q->stream);
-  };
-  cudaError_t ce = cudaSuccess;
-  auto chk = [&](cudaError_t x) {
-    if (ce == cudaSuccess) ce = x;
-  };
-  chk(up(o_sig, d->diameter, sizeof(double) * NB));
-  chk(up(o_z, d->valence, sizeof(double) * NB));
-  chk(up(o_dmu, d->delta_muH, sizeof(double) * NB));
-  if (MB) chk(up(o_bonds, bonds.data(), sizeof(int) * 2 * MB));
-  for (int u = 0; u < NS; u++) {
-    const SpeciesHost& h = q->sp[u];
-    chk(up(o_states[u], h.states.data(), sizeof(int) * h.states.size()));
-    chk(up(o_nst[u], h.nst.data(), sizeof(int) * h.nst.size()));
-    chk(up(o_md[u], h.md.data(), sizeof(double) * h.md.size()));
-  }
-  chk(up(o_sp, dsp.data(), sizeof(DSpecies) * NS));
-  chk(up(o_Ext, Ext.data(), sizeof(double) * Ext.size()));
-  chk(up(o_tr, tr.data(), sizeof(double) * tr.size()));
-  chk(up(o_Csurf, Csurf.data(), sizeof(double) * P));
-  chk(up(o_Wbond, Wbond.data(), sizeof(double) * Wbond.size()));
-  chk(up(o_Wfmt, Wfmt.data(), sizeof(double) * Wfmt.size()));
-  chk(up(o_Wmsa, Wmsa.data(), sizeof(double) * Wmsa.size()));
-  chk(up(o_Wcoul, Wcoul.data(), sizeof(double) * P));
-  chk(up(o_tw, tw.data(), sizeof(double2) * tw.size()));
-  chk(up(o_twP, twP.data(), sizeof(double2) * twP.size()));
-  chk(up(o_twD, twD.data(), sizeof(double2) * twD.size()));
-  chk(up(o_x, x0.data(), sizeof(double) * q->n));
-  chk(up(o_dreq, &r, sizeof(DReq)));
-  chk(cudaStreamSynchronize(q->stream));
+  cudaError_t ce = cudaMemsetAsync(q->dmem, 0, q->bytes, q->stream);
+  std::vector<DSpecies> dsp;
+  q->h = plan_bind(d, pl, q->dmem, nullptr, nullptr, dsp);
+  q->dreq = (DReq*)(q->dmem + pl.o_dreq);
+  q->dslot = (SolveSlot*)(q->dmem + pl.o_slot);
+  q->dout = (double*)(q->dmem + pl.o_out);
+  if (ce == cudaSuccess) ce = plan_upload(d, pl, q->dmem, q->h, dsp, q->stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(q->stream);
   if (ce != cudaSuccess) {
     cudaStreamDestroy(q->stream);
     cudaFree(q->dmem);
@@ -859,268 +963,30 @@ int noalloc_scratch_address(void** out) {
 extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x_dev, double* g_dev, void* stream_ptr) {
   if (!d || !x_dev || !g_dev) return set_err(SDFT_ERR_ARG, "null argument");
   if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
-  const int P = d->np;
-  if (P < 16 || (P & (P - 1)) != 0) return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP = 2^k >= 16");
-  if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
-  if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
-  if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
-  if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
-  if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
+  Plan pl;
+  int rc = plan_species(d, pl);
+  if (rc) return rc;
+  // layout inside the scratch array (no Anderson history: G(x) only)
+  plan_layout(pl, false);
+  if (pl.bytes > (size_t)SDFT_NOALLOC_SCRATCH_BYTES)
+    return set_err(SDFT_ERR_ARG, "system needs " + std::to_string(pl.bytes) + " bytes of scratch; sdft_objective_noalloc holds " +
+                                     std::to_string((size_t)SDFT_NOALLOC_SCRATCH_BYTES));
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_ptr);
   void* base_v = nullptr;
-  int rc = noalloc_scratch_address(&base_v);
+  rc = noalloc_scratch_address(&base_v);
   if (rc) return rc;
   char* base = static_cast<char*>(base_v);
-  const int NB = d->nb, MB = d->mb, NS = d->n_species, M = P / 2;
-  int L = 0;
-  while ((1 << L) < M) L++;
-  const int NPS = 2 * P;
-  std::vector<int> bonds(d->bond_types, d->bond_types + 2 * MB);
-  std::vector<SpeciesHost> sp;
-  for (int u = 0; u < NS; u++) {
-    const sdft_species_desc& s = d->species[u];
-    SpeciesHost h;
-    h.n_seg = s.n_seg;
-    h.S = s.max_states;
-    if (h.n_seg < 1 || h.S < 1 || h.S > kMaxStates)
-      return set_err(SDFT_ERR_UNSUPPORTED, "segments >= 1 and 1 <= states <= 4 per segment are required");
-    for (int g = 0; g < h.n_seg; g++) {
-      if (s.parent[g] != g - 1) return set_err(SDFT_ERR_UNSUPPORTED, "linear chains only");
-      if (s.n_states[g] < 1 || s.n_states[g] > h.S) return set_err(SDFT_ERR_ARG, "n_states out of range");
-    }
-    h.nst.assign(s.n_states, s.n_states + h.n_seg);
-    h.states.assign(s.states, s.states + (size_t)h.n_seg * h.S);
-    h.fixed = -1;
-    if (s.fixed_coord) {
-      for (int g = 1; g < h.n_seg; g++)
-        if (s.fixed_coord[g] >= 0) return set_err(SDFT_ERR_UNSUPPORTED, "only segment 0 can be fixed in a 1D slit");
-      h.fixed = s.fixed_coord[0];
-    }
-    if (h.fixed >= 0) {
-      if (h.fixed >= P || h.n_seg < 2 || !s.max_distance)
-        return set_err(SDFT_ERR_ARG, "fixed segment needs a grid point, a free segment and max_distance");
-      if (h.n_seg == 2 && h.nst[1] > 1) return set_err(SDFT_ERR_UNSUPPORTED, "grafted dimer with a multi-state free segment");
-      h.md.resize(h.n_seg);
-      for (int g = 0; g < h.n_seg; g++) h.md[g] = s.max_distance[(size_t)g * h.n_seg];
-    } else {
-      h.md.assign(h.n_seg, 0.0);
-    }
-    for (int g = 0; g < h.n_seg; g++)
-      for (int i = 0; i < h.nst[g]; i++) {
-        int st = h.states[(size_t)g * h.S + i];
-        if (st < 0 || st >= NB) return set_err(SDFT_ERR_ARG, "state bead type out of range");
-        if (g > 0)
-          for (int j = 0; j < h.nst[g - 1]; j++)
-            if (bond_lookup(bonds, st, h.states[(size_t)(g - 1) * h.S + j]) < 0)
-              return set_err(SDFT_ERR_ARG, "bond missing from bond_types");
-      }
-    h.fixed_density = s.fixed_density;
-    h.mu_species = s.mu_species;
-    double nv = 1.0;
-    for (int g = h.n_seg - 1; g >= 0; g--) {
-      double t = 0.0;
-      for (int i = 0; i < h.nst[g]; i++) t += std::exp(-d->delta_muH[h.states[(size_t)g * h.S + i]]);
-      nv *= std::pow(t, 1.0 / (double)h.n_seg);
-    }
-    h.normative = nv;
-    h.norm_free = std::pow(nv, (double)(h.n_seg - 1));
-    sp.push_back(h);
-  }
-  // layout inside the scratch array (no Anderson history: G(x) only)
-  const int nwa = std::max(NB, 6), nwc = std::max(NB + MB, 6 + MB);
-  Layout lay;
-  size_t o_sig = lay.take<double>(NB), o_z = lay.take<double>(NB), o_dmu = lay.take<double>(NB);
-  size_t o_bonds = lay.take<int>(2 * MB + 2);
-  size_t o_sp = lay.take<DSpecies>(NS);
-  std::vector<size_t> o_states(NS), o_nst(NS), o_md(NS), o_gC(NS), o_gP(NS), o_rho(NS), o_expo(NS);
-  for (int u = 0; u < NS; u++) {
-    const SpeciesHost& h = sp[u];
-    o_states[u] = lay.take<int>(h.states.size());
-    o_nst[u] = lay.take<int>(h.nst.size());
-    o_md[u] = lay.take<double>(h.md.size());
-    size_t gsz = h.n_seg > 1 ? (size_t)h.n_seg * h.S * h.S * P : 0;
-    o_gC[u] = lay.take<double>(gsz);
-    o_gP[u] = lay.take<double>(gsz);
-    o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
-    o_expo[u] = lay.take<int>((size_t)2 * h.n_seg);
-  }
-  size_t o_Ext = lay.take<double>((size_t)NB * P), o_tr = lay.take<double>((size_t)NB * P);
-  size_t o_Csurf = lay.take<double>(P);
-  size_t o_Wbond = lay.take<double>((size_t)MB * P + 1), o_Wfmt = lay.take<double>((size_t)NB * 3 * P);
-  size_t o_Wmsa = lay.take<double>((size_t)NB * P), o_Wcoul = lay.take<double>(P);
-  size_t o_tw = lay.take<double2>(M / 2 + 1), o_twP = lay.take<double2>(M + 1), o_twD = lay.take<double2>(M + 1);
-  size_t o_lam = lay.take<double>((size_t)NB * P), o_rb = lay.take<double>((size_t)NB * P);
-  size_t o_rbo = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_Cb = lay.take<double>((size_t)NB * P), o_Cbond = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_Cmu = lay.take<double>((size_t)NB * P), o_Clng = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_wa = lay.take<double>((size_t)nwa * P), o_wb = lay.take<double>((size_t)MB * 2 * P + 1);
-  size_t o_wc = lay.take<double>((size_t)nwc * P);
-  size_t o_wd = lay.take<double>((size_t)2 * NB * P);
-  size_t o_status = lay.take<int>(4), o_iters = lay.take<int>(4), o_err = lay.take<double>(4);
-  size_t o_scal = lay.take<double>(8);
-  size_t o_dreq = lay.take<DReq>(1);
-  if (lay.off > (size_t)SDFT_NOALLOC_SCRATCH_BYTES)
-    return set_err(SDFT_ERR_ARG, "system needs " + std::to_string(lay.off) + " bytes of scratch; sdft_objective_noalloc holds " +
-                                     std::to_string((size_t)SDFT_NOALLOC_SCRATCH_BYTES));
-  // host tables (the same formulas as sdft_request_create)
-  std::vector<double> Ext((size_t)NB * P, 0.0), tr((size_t)NB * P, 1.0);
-  if (d->hard_walls) {
-    for (int K = 0; K < P; K++) {
-      int idx = K + 1;
-      for (int j = 0; j < NB; j++) {
-        double dd = d->diameter[j];
-        int lo = jround((0.0 + dd / 2.0) / d->bin_width) + 1;
-        int hi = jround((d->length - dd / 2.0) / d->bin_width) + 1;
-        size_t qq = (size_t)j * P + K;
-        if (idx < lo) {
-          Ext[qq] += 1.0e20;
-          tr[qq] = 1.0;
-        } else if (idx == lo) {
-          tr[qq] = 0.5;
-        }
-        if (idx > hi) {
-          Ext[qq] += 1.0e20;
-          tr[qq] = 1.0;
-        } else if (idx == hi) {
-          tr[qq] = 0.5;
-        }
-      }
-    }
-  }
-  std::vector<double> surf(P, 0.0), Csurf(P, 0.0);
-  if (d->charged_walls) {
-    double pos[2] = {0.0, d->length};
-    for (int w = 0; w < 2; w++) {
-      int gp = jround(pos[w] / d->bin_width) + 1;
-      if (gp >= 1 && gp <= P) surf[gp - 1] += d->wall_charge[w] * (1.0 / d->bin_width);
-    }
-    for (int k = 0; k < P; k++) {
-      long double acc = 0.0L;
-      for (int K = 0; K < P; K++)
-        if (surf[K] != 0.0) acc += (long double)surf[K] * cosl(3.14159265358979323846264338327950288L * k * (2 * K + 1) / (2.0L * P));
-      Csurf[k] = (double)acc;
-    }
-  }
-  std::vector<double> Wbond((size_t)MB * P + 1, 0.0), Wfmt((size_t)NB * 3 * P), Wmsa((size_t)NB * P), Wcoul(P);
-  for (int u = 0; u < MB; u++) {
-    double sij = (d->diameter[bonds[2 * u]] + d->diameter[bonds[2 * u + 1]]) / 2.0;
-    for (int k = 0; k < P; k++)
-      Wbond[(size_t)u * P + k] = filter_k(k, NPS, d->bin_width) * (w_delta(k, NPS, d->bin_width, sij) / (4.0 * kPi * (sij * sij)));
-  }
-  for (int j = 0; j < NB; j++) {
-    double b = d->diameter[j] / 2.0;
-    for (int k = 0; k < P; k++) {
-      Wfmt[((size_t)j * 3 + 0) * P + k] = w_delta(k, NPS, d->bin_width, b);
-      Wfmt[((size_t)j * 3 + 1) * P + k] = w_step(k, NPS, d->bin_width, b);
-      Wfmt[((size_t)j * 3 + 2) * P + k] = w_vec(k, NPS, d->bin_width, b);
-      Wmsa[(size_t)j * P + k] = w_delta(k, NPS, d->bin_width, b) / (4.0 * kPi * (b * b));
-    }
-  }
-  for (int k = 0; k < P; k++) Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
-  const long double PI_L = 3.14159265358979323846264338327950288L;
-  std::vector<double2> tw(M / 2 + 1), twP(M + 1), twD(M + 1);
-  for (int k = 0; k <= M / 2; k++) tw[k] = cis(-2.0L * PI_L * k / M);
-  for (int k = 0; k <= M; k++) twP[k] = cis(-2.0L * PI_L * k / P);
-  for (int k = 0; k <= M; k++) twD[k] = cis(-PI_L * k / (2.0L * P));
-  auto at = [&](size_t o) { return (void*)(base + o); };
-  std::vector<DSpecies> dsp(NS);
-  for (int u = 0; u < NS; u++) {
-    const SpeciesHost& h = sp[u];
-    DSpecies& s = dsp[u];
-    s.n_seg = h.n_seg;
-    s.S = h.S;
-    s.fixed = h.fixed;
-    s.states = (const int*)at(o_states[u]);
-    s.nst = (const int*)at(o_nst[u]);
-    s.md = (const double*)at(o_md[u]);
-    s.fixed_density = h.fixed_density;
-    s.mu_species = h.mu_species;
-    s.normative = h.normative;
-    s.norm_free = h.norm_free;
-    s.lambda_fixed = 1.0;
-    s.gC = h.n_seg > 1 ? (double*)at(o_gC[u]) : nullptr;
-    s.gP = h.n_seg > 1 ? (double*)at(o_gP[u]) : nullptr;
-    s.rho_seg = (double*)at(o_rho[u]);
-    s.expo = (int*)at(o_expo[u]);
-  }
-  DReq r{};
-  r.NP = P;
-  r.M = M;
-  r.L = L;
-  r.NB = NB;
-  r.MB = MB;
-  r.NS = NS;
-  r.funcs = (int)d->functionals;
-  r.dz = d->bin_width;
-  r.lB = d->bjerrum_length;
-  r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
-  r.n = (long long)P * (NB + 2 * MB + 1) + 1;
-  r.sig = (const double*)at(o_sig);
-  r.z = (const double*)at(o_z);
-  r.dmu = (const double*)at(o_dmu);
-  r.bonds = (const int*)at(o_bonds);
-  r.sp = (const DSpecies*)at(o_sp);
-  r.Ext = (const double*)at(o_Ext);
-  r.trapez = (const double*)at(o_tr);
-  r.Csurf = (const double*)at(o_Csurf);
-  r.Wbond = (const double*)at(o_Wbond);
-  r.Wfmt = (const double*)at(o_Wfmt);
-  r.Wmsa = (const double*)at(o_Wmsa);
-  r.Wcoul = (const double*)at(o_Wcoul);
-  r.tw = (const double2*)at(o_tw);
-  r.twP = (const double2*)at(o_twP);
-  r.twD = (const double2*)at(o_twD);
-  r.x = const_cast<double*>(x_dev);  // read only in G(x)
-  r.g = g_dev;
-  r.lambda = (double*)at(o_lam);
-  r.rho_beads = (double*)at(o_rb);
-  r.rho_bonds = (double*)at(o_rbo);
-  r.Cb = (double*)at(o_Cb);
-  r.Cbond = (double*)at(o_Cbond);
-  r.Cmu = (double*)at(o_Cmu);
-  r.Clng = (double*)at(o_Clng);
-  r.wa = (double*)at(o_wa);
-  r.wb = (double*)at(o_wb);
-  r.wc = (double*)at(o_wc);
-  r.wd = (double*)at(o_wd);
-  r.TB = tb_for(M);
-  r.hx = nullptr;
-  r.hg = nullptr;
-  r.lsq_u = nullptr;
-  r.status = (int*)at(o_status);
-  r.iters = (int*)at(o_iters);
-  r.err = (double*)at(o_err);
-  r.scal = (double*)at(o_scal);
+  plan_tables(d, pl);
+  const int M = pl.M;
+  std::vector<DSpecies> dsp;
+  DReq r = plan_bind(d, pl, base, const_cast<double*>(x_dev), g_dev, dsp);  // x is read only in G(x)
   // the array keeps the previous call's contents: clear the region this call uses
-  CUDA_TRY(cudaMemsetAsync(base, 0, lay.off, stream));
-  auto up = [&](size_t o, const void* src, size_t nbytes) {
-    return cudaMemcpyAsync(base + o, src, nbytes, cudaMemcpyHostToDevice, stream);
-  };
-  CUDA_TRY(up(o_sig, d->diameter, sizeof(double) * NB));
-  CUDA_TRY(up(o_z, d->valence, sizeof(double) * NB));
-  CUDA_TRY(up(o_dmu, d->delta_muH, sizeof(double) * NB));
-  if (MB) CUDA_TRY(up(o_bonds, bonds.data(), sizeof(int) * 2 * MB));
-  for (int u = 0; u < NS; u++) {
-    CUDA_TRY(up(o_states[u], sp[u].states.data(), sizeof(int) * sp[u].states.size()));
-    CUDA_TRY(up(o_nst[u], sp[u].nst.data(), sizeof(int) * sp[u].nst.size()));
-    CUDA_TRY(up(o_md[u], sp[u].md.data(), sizeof(double) * sp[u].md.size()));
-  }
-  CUDA_TRY(up(o_sp, dsp.data(), sizeof(DSpecies) * NS));
-  CUDA_TRY(up(o_Ext, Ext.data(), sizeof(double) * Ext.size()));
-  CUDA_TRY(up(o_tr, tr.data(), sizeof(double) * tr.size()));
-  CUDA_TRY(up(o_Csurf, Csurf.data(), sizeof(double) * P));
-  CUDA_TRY(up(o_Wbond, Wbond.data(), sizeof(double) * Wbond.size()));
-  CUDA_TRY(up(o_Wfmt, Wfmt.data(), sizeof(double) * Wfmt.size()));
-  CUDA_TRY(up(o_Wmsa, Wmsa.data(), sizeof(double) * Wmsa.size()));
-  CUDA_TRY(up(o_Wcoul, Wcoul.data(), sizeof(double) * P));
-  CUDA_TRY(up(o_tw, tw.data(), sizeof(double2) * tw.size()));
-  CUDA_TRY(up(o_twP, twP.data(), sizeof(double2) * twP.size()));
-  CUDA_TRY(up(o_twD, twD.data(), sizeof(double2) * twD.size()));
-  CUDA_TRY(up(o_dreq, &r, sizeof(DReq)));
+  CUDA_TRY(cudaMemsetAsync(base, 0, pl.bytes, stream));
+  CUDA_TRY(plan_upload(d, pl, base, r, dsp, stream));
   size_t sm = smem_bytes(M);
   rc = prepare_kernel((const void*)sdft_k_objective, sm);
   if (rc) return rc;
-  sdft_k_objective<<<1, kThreads, sm, stream>>>((const DReq*)at(o_dreq));
+  sdft_k_objective<<<1, kThreads, sm, stream>>>((const DReq*)(base + pl.o_dreq));
   CUDA_TRY(cudaGetLastError());
   int st = 0;
   CUDA_TRY(cudaMemcpyAsync(&st, r.status, sizeof(int), cudaMemcpyDeviceToHost, stream));
