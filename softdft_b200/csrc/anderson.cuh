@@ -31,48 +31,68 @@ struct AndersonState {
 // columns j != col of the history, ascending
 __device__ __forceinline__ int hist_col(int c, int col) { return c < col ? c : c + 1; }
 
-__device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* red) {
+// One sweep over the history serves each LSQR iteration: the next vector
+// w = A v - alpha u is stored unnormalised (u_true = uscale * u_stored) while
+// ||w||^2 and A^T w are accumulated in the same pass; A^T u_{i+1} = A^T w / beta
+// follows once beta = ||w|| is known.  The recurrence is LSQR's own; only the
+// order of the divisions by beta differs.  NC bounds the column count at
+// compile time so that the per-thread column values stay in registers.
+template <int NC>
+__device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, double* lam, double* red) {
   const long long n = r.n;
-  const int nc = m - 1;
   const double* gk = r.hg + (size_t)col * n;
+  const double* hc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) hc[c] = c < nc ? r.hg + (size_t)hist_col(c, col) * n : gk;
   double* u = r.lsq_u;
   const double eps = 2.220446049250313e-16;
   const double atol = sqrt(eps), btol = sqrt(eps), conlim = 1.0 / sqrt(eps);
   const long long maxiter = n > nc ? n : nc;
   const double ctol = conlim > 0 ? 1.0 / conlim : 0.0;
-  double v[kMaxAnderson], w[kMaxAnderson], tmp[kMaxAnderson];
-  // u = b - A x, b = -g_k,  A[:, c] = G_hist[j_c] - g_k
-  double ss = 0.0;
+  double v[NC], w[NC], acc[NC + 1], x[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) x[c] = c < nc ? lam[c] : 0.0;
+  // u = b - A x with b = -g_k and A[:, c] = G_hist[j_c] - g_k; ||u||^2 and A^T u
+#pragma unroll
+  for (int c = 0; c <= NC; c++) acc[c] = 0.0;
   for (long long q = threadIdx.x; q < n; q += blockDim.x) {
     const double gq = gk[q];
+    double aq[NC];
     double ax = 0.0;
-    for (int c = 0; c < nc; c++) ax += (r.hg[(size_t)hist_col(c, col) * n + q] - gq) * lam[c];
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) {
+        aq[c] = hc[c][q] - gq;
+        ax += aq[c] * x[c];
+      }
     const double uq = -gq - ax;
     u[q] = uq;
-    ss += uq * uq;
+    acc[NC] += uq * uq;
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) acc[c] += aq[c] * uq;
   }
-  double beta = sqrt(block_sum(ss, red));
+  block_sum_vec<NC + 1>(acc, NC + 1, red);
+  double beta = sqrt(acc[NC]);
+  double uscale = beta > 0 ? 1.0 / beta : 1.0;
   double alpha = 0.0;
-  for (int c = 0; c < nc; c++) v[c] = 0.0;
+#pragma unroll
+  for (int c = 0; c < NC; c++) v[c] = 0.0;
   if (beta > 0) {
-    for (int c = 0; c < nc; c++) tmp[c] = 0.0;
-    for (long long q = threadIdx.x; q < n; q += blockDim.x) {
-      const double uq = u[q] / beta;
-      u[q] = uq;
-      const double gq = gk[q];
-      for (int c = 0; c < nc; c++) tmp[c] += (r.hg[(size_t)hist_col(c, col) * n + q] - gq) * uq;
-    }
-    block_sum_vec<kMaxAnderson>(tmp, nc, red);
     double a2 = 0.0;
-    for (int c = 0; c < nc; c++) {
-      v[c] = tmp[c];
-      a2 += v[c] * v[c];
-    }
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) {
+        v[c] = acc[c] / beta;
+        a2 += v[c] * v[c];
+      }
     alpha = sqrt(a2);
   }
   if (alpha > 0)
-    for (int c = 0; c < nc; c++) v[c] /= alpha;
-  for (int c = 0; c < nc; c++) w[c] = v[c];
+#pragma unroll
+    for (int c = 0; c < NC; c++) v[c] /= alpha;
+#pragma unroll
+  for (int c = 0; c < NC; c++) w[c] = v[c];
   double arnorm = alpha * beta;
   if (arnorm == 0) return;
   double anorm = 0, ddnorm = 0, res2 = 0, xxnorm = 0, zz = 0, sn2 = 0, cs2 = -1.0;
@@ -82,35 +102,43 @@ __device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* 
   int istop = 0;
   while (itn < maxiter && istop == 0) {
     itn++;
-    // u = A v - alpha u
-    ss = 0.0;
+    // w = A v - alpha u (unnormalised), its norm and A^T w in one sweep
+    const double coef = alpha * uscale;
+#pragma unroll
+    for (int c = 0; c <= NC; c++) acc[c] = 0.0;
     for (long long q = threadIdx.x; q < n; q += blockDim.x) {
       const double gq = gk[q];
+      double aq[NC];
       double av = 0.0;
-      for (int c = 0; c < nc; c++) av += (r.hg[(size_t)hist_col(c, col) * n + q] - gq) * v[c];
-      const double uq = -alpha * u[q] + av;
-      u[q] = uq;
-      ss += uq * uq;
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        if (c < nc) {
+          aq[c] = hc[c][q] - gq;
+          av += aq[c] * v[c];
+        }
+      const double wq = -coef * u[q] + av;
+      u[q] = wq;
+      acc[NC] += wq * wq;
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        if (c < nc) acc[c] += aq[c] * wq;
     }
-    beta = sqrt(block_sum(ss, red));
+    block_sum_vec<NC + 1>(acc, NC + 1, red);
+    beta = sqrt(acc[NC]);
     if (beta > 0) {
+      uscale = 1.0 / beta;
       anorm = sqrt(anorm * anorm + alpha * alpha + beta * beta);
-      for (int c = 0; c < nc; c++) tmp[c] = 0.0;
-      for (long long q = threadIdx.x; q < n; q += blockDim.x) {
-        const double uq = u[q] / beta;
-        u[q] = uq;
-        const double gq = gk[q];
-        for (int c = 0; c < nc; c++) tmp[c] += (r.hg[(size_t)hist_col(c, col) * n + q] - gq) * uq;
-      }
-      block_sum_vec<kMaxAnderson>(tmp, nc, red);
       double a2 = 0.0;
-      for (int c = 0; c < nc; c++) {
-        v[c] = -beta * v[c] + tmp[c];
-        a2 += v[c] * v[c];
-      }
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        if (c < nc) {
+          v[c] = -beta * v[c] + acc[c] / beta;
+          a2 += v[c] * v[c];
+        }
       alpha = sqrt(a2);
       if (alpha > 0)
-        for (int c = 0; c < nc; c++) v[c] /= alpha;
+#pragma unroll
+        for (int c = 0; c < NC; c++) v[c] /= alpha;
     }
     const double rhobar1 = rhobar, psi = 0.0;
     const double rho = sqrt(rhobar1 * rhobar1 + beta * beta);
@@ -122,12 +150,14 @@ __device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* 
     const double tau = sn * phi;
     const double t1 = phi / rho, t2 = -theta / rho;
     double dk2 = 0.0;
-    for (int c = 0; c < nc; c++) {
-      const double dk = w[c] / rho;
-      dk2 += dk * dk;
-      lam[c] += t1 * w[c];
-      w[c] = v[c] + t2 * w[c];
-    }
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) {
+        const double dk = w[c] / rho;
+        dk2 += dk * dk;
+        x[c] += t1 * w[c];
+        w[c] = v[c] + t2 * w[c];
+      }
     ddnorm += dk2;
     const double delta = sn2 * rho, gambar = -cs2 * rho, rhs = phi - delta * zz;
     const double zbar = rhs / gambar;
@@ -155,6 +185,16 @@ __device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* 
     if (test2 <= atol) istop = 2;
     if (test1 <= rtol) istop = 1;
   }
+#pragma unroll
+  for (int c = 0; c < NC; c++)
+    if (c < nc) lam[c] = x[c];
+}
+
+__device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* red) {
+  const int nc = m - 1;
+  if (nc <= 4) lsqr_sweep_device<4>(r, nc, col, lam, red);
+  else if (nc <= 9) lsqr_sweep_device<9>(r, nc, col, lam, red);
+  else lsqr_sweep_device<kMaxAnderson - 1>(r, nc, col, lam, red);
 }
 
 // One Anderson update after r.g = G(x).  Returns ST_RUNNING, ST_OK (converged
