@@ -50,6 +50,12 @@ struct DSpecies {
   double* gP;         // [(g * S + i) * S + j] * P + K : child g state i, parent g-1 state j
   double* rho_seg;    // [(g * S + i) * P + K]
   int* expo;          // [2 * n_seg]: power-of-two exponent carried by gC of g, then by gP of g
+  // species-local slots for register accumulation of bond-end and bead densities
+  const int* bslot;       // [(g * S + i) * S + j] slot of bond bnd[...] among the species' bonds
+  const int* bslot_bond;  // [nbslot] bond type of each slot
+  const int* eslot;       // [g * S + i] slot of bead type states[g * S + i] among the species' beads
+  const int* eslot_bead;  // [neslot] bead type of each slot
+  int nbslot, neslot;
 };
 
 struct DReq {
@@ -96,6 +102,7 @@ struct DReq {
   double* wb;             // [MB * 2 * P]  scratch (bond weighted densities)
   double* wc;             // [max(NB, 6 + MB) * P] scratch (derivative fields)
   double* wd;             // [2 * NB * P] scratch (per-bead FMT weighted densities)
+  double* elam;           // [NB * P] e^{-lambda} of the current x
   double* fbe;            // [4 * MB * P] bond-end factors of the current x: e^{-lambda_j + lng/2} trapez_j, then e^{lng/2}
   // Anderson
   double* hx;             // [m * n] history of x

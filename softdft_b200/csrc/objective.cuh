@@ -70,6 +70,7 @@ __device__ void stage_bond_factors(const DReq& r) {
     r.fbe[idx] = exp(-r.lambda[(size_t)j * P + K] + l / 2.0) * r.trapez[(size_t)j * P + K];
     r.fbe[(size_t)nbe * P + idx] = exp(l / 2.0);
   }
+  for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) r.elam[idx] = exp(-r.lambda[idx]);
   __syncthreads();
 }
 
@@ -407,14 +408,137 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, 
   __syncthreads();
 }
 
+// a[idx] += v for a register array (idx < N): unrolled select, no local memory
+template <int N>
+__device__ __forceinline__ void acc_add(double* a, int idx, double v) {
+#pragma unroll
+  for (int q = 0; q < N; q++)
+    if (q == idx) a[q] += v;
+}
+
+// accumulate_densities! of one species with its bond-end and bead densities
+// summed in registers (species-local slots, BR bond slots, ER bead slots) and
+// added to rho_bonds / rho_beads once per grid point, instead of one global
+// read-modify-write per segment.  Each point's sums run over (segment, state,
+// child state) in the reference's order.  The segment prefactor uses
+// e^{-lambda} of the evaluation: norm e^{mu} e^{-lambda_K} (unscaled), or
+// e^{lp} e^{-lambda_K} with lp the log prefactor of the renormalised
+// propagators (e^{lp - lambda_K} directly when |lp| > 600).  Also adds the
+// species to the bead densities (update_spatial_structures.jl:1-34).
+template <int BR, int ER>
+__device__ __noinline__ void accumulate_regs(const DReq& r, const DSpecies& s, double norm, bool scaled,
+                                             const double* __restrict__ gP, const double* __restrict__ gC,
+                                             const double* __restrict__ elam, const double* __restrict__ lam,
+                                             const int* __restrict__ states, const int* __restrict__ nst,
+                                             const int* __restrict__ bslot, const int* __restrict__ eslot,
+                                             double* __restrict__ rho_seg, double* __restrict__ rho_bonds,
+                                             double* __restrict__ rho_beads) {
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  const double pref = norm * exp(s.mu_species);
+  for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    double a0[BR], a1[BR], ab[ER];
+#pragma unroll
+    for (int q = 0; q < BR; q++) a0[q] = a1[q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < ER; q++) ab[q] = 0.0;
+    for (int g = 0; g < N; g++) {
+      double lp = 0.0, elp = pref;
+      bool direct = false;
+      if (scaled) {
+        lp = log_prefactor(s, norm, g);
+        direct = fabs(lp) > 600.0;
+        elp = exp(lp);
+      }
+      const int nn = g < N - 1 ? nst[g + 1] : 0;
+      for (int ii = 0; ii < nst[g]; ii++) {
+        const int si = states[g * S + ii];
+        double sp;
+        if (N > 1) {
+          sp = 0.0;
+          for (int q = 0; q < S; q++) sp += gP[((size_t)(g * S + ii) * S + q) * P + K];
+        } else {
+          sp = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
+        }
+        const double contr = direct ? exp(lp - lam[(size_t)si * P + K]) * sp : elp * elam[(size_t)si * P + K] * sp;
+        double temp;
+        if (nn) {
+          temp = 0.0;
+          for (int jj = 0; jj < nn; jj++) {
+            const double t2 = gC[((size_t)(g * S + ii) * S + jj) * P + K];
+            acc_add<BR>(a0, bslot[(g * S + ii) * S + jj], contr * t2);
+            temp += t2;
+          }
+        } else {
+          temp = 1.0;
+        }
+        const double v = contr * temp;
+        rho_seg[(size_t)(g * S + ii) * P + K] = v;
+        if (g == 0 && s.fixed >= 0) {
+          if (K == s.fixed) acc_add<ER>(ab, eslot[g * S + ii], v / r.dz / r.trapez[(size_t)si * P + K]);
+        } else {
+          acc_add<ER>(ab, eslot[g * S + ii], v);
+        }
+      }
+    }
+    for (int c = 1; c < N; c++) {
+      double lp = 0.0, elp = pref;
+      bool direct = false;
+      if (scaled) {
+        lp = log_prefactor(s, norm, c);
+        direct = fabs(lp) > 600.0;
+        elp = exp(lp);
+      }
+      for (int ii = 0; ii < nst[c]; ii++) {
+        const int si = states[c * S + ii];
+        double contr = direct ? exp(lp - lam[(size_t)si * P + K]) : elp * elam[(size_t)si * P + K];
+        if (c < N - 1) {
+          double t = 0.0;
+          for (int q = 0; q < S; q++) t += gC[((size_t)(c * S + ii) * S + q) * P + K];
+          contr *= t;
+        }
+        for (int jj = 0; jj < nst[c - 1]; jj++)
+          acc_add<BR>(a1, bslot[((c - 1) * S + jj) * S + ii], contr * gP[((size_t)(c * S + ii) * S + jj) * P + K]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < BR; q++)
+      if (q < s.nbslot) {
+        const int b = s.bslot_bond[q];
+        rho_bonds[(size_t)(b * 2 + 0) * P + K] += a0[q];
+        rho_bonds[(size_t)(b * 2 + 1) * P + K] += a1[q];
+      }
+#pragma unroll
+    for (int q = 0; q < ER; q++)
+      if (q < s.neslot) rho_beads[(size_t)s.eslot_bead[q] * P + K] += ab[q];
+  }
+  __syncthreads();
+}
+
+// true when the species went through accumulate_regs (its bead densities are added)
+__device__ __forceinline__ bool accumulate_fast(const DReq& r, const DSpecies& s, double norm, bool scaled) {
+  if (s.nbslot <= 4 && s.neslot <= 4) {
+    accumulate_regs<4, 4>(r, s, norm, scaled, s.gP, s.gC, r.elam, r.lambda, s.states, s.nst, s.bslot, s.eslot, s.rho_seg,
+                          r.rho_bonds, r.rho_beads);
+    return true;
+  }
+  if (s.nbslot <= 16 && s.neslot <= 8) {
+    accumulate_regs<16, 8>(r, s, norm, scaled, s.gP, s.gC, r.elam, r.lambda, s.states, s.nst, s.bslot, s.eslot, s.rho_seg,
+                           r.rho_bonds, r.rho_beads);
+    return true;
+  }
+  return false;
+}
+
 // eval_spatial_density! + update_spatial_structures!; false on a normalisation error
 __device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
   const int P = r.NP;
+  unsigned fast_mask = 0;  // species whose bead densities accumulate_regs added
   for (int u = 0; u < r.NS; u++) {
     const DSpecies& s = r.sp[u];
     for (size_t q = threadIdx.x; q < (size_t)s.n_seg * s.S * P; q += blockDim.x) s.rho_seg[q] = 0.0;
   }
   for (size_t q = threadIdx.x; q < (size_t)r.MB * 2 * P; q += blockDim.x) r.rho_bonds[q] = 0.0;
+  for (size_t q = threadIdx.x; q < (size_t)r.NB * P; q += blockDim.x) r.rho_beads[q] = 0.0;
   __syncthreads();
   for (int u = 0; u < r.NS; u++) {
     DSpecies s = r.sp[u];
@@ -436,23 +560,26 @@ __device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
     }
     // the reference's prefactor norm e^{mu - lambda} overflows beyond e^709
     if (fabs(s.mu_species) + (double)(s.n_seg - 1) * fabs(log(s.normative)) > 600.0) scaled = true;
-    chain_accumulate(r, s, norm, scaled);
+    if (accumulate_fast(r, s, norm, scaled)) fast_mask |= 1u << u;
+    else chain_accumulate(r, s, norm, scaled);
   }
-  // update_spatial_structures!
-  for (int K = threadIdx.x; K < P; K += blockDim.x) {
-    for (int j = 0; j < r.NB; j++) r.rho_beads[(size_t)j * P + K] = 0.0;
-    for (int u = 0; u < r.NS; u++) {
-      const DSpecies& s = r.sp[u];
-      for (int g = 0; g < s.n_seg; g++)
-        for (int ii = 0; ii < s.nst[g]; ii++) {
-          const int st = s.states[g * s.S + ii];
-          const double v = s.rho_seg[(size_t)(g * s.S + ii) * P + K];
-          if (g == 0 && s.fixed >= 0) {
-            if (K == s.fixed) r.rho_beads[(size_t)st * P + K] += v / r.dz / r.trapez[(size_t)st * P + K];
-          } else {
-            r.rho_beads[(size_t)st * P + K] += v;
+  // update_spatial_structures! for the species accumulated without register slots
+  if (fast_mask != (1u << r.NS) - 1u) {
+    for (int K = threadIdx.x; K < P; K += blockDim.x) {
+      for (int u = 0; u < r.NS; u++) {
+        if (fast_mask & (1u << u)) continue;
+        const DSpecies& s = r.sp[u];
+        for (int g = 0; g < s.n_seg; g++)
+          for (int ii = 0; ii < s.nst[g]; ii++) {
+            const int st = s.states[g * s.S + ii];
+            const double v = s.rho_seg[(size_t)(g * s.S + ii) * P + K];
+            if (g == 0 && s.fixed >= 0) {
+              if (K == s.fixed) r.rho_beads[(size_t)st * P + K] += v / r.dz / r.trapez[(size_t)st * P + K];
+            } else {
+              r.rho_beads[(size_t)st * P + K] += v;
+            }
           }
-        }
+      }
     }
   }
   __syncthreads();

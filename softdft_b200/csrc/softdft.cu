@@ -131,7 +131,7 @@ static size_t smem_bytes(int M);
 
 struct SpeciesHost {
   int n_seg, S, fixed;
-  std::vector<int> states, nst, bnd;
+  std::vector<int> states, nst, bnd, bslot, bslot_bond, eslot, eslot_bead;
   std::vector<double> md;
   double fixed_density, mu_species, normative, norm_free;
 };
@@ -204,10 +204,10 @@ struct Plan {
   std::vector<double> grp_sig;   // [ngrp] group diameters
   // layout
   size_t o_sig = 0, o_z = 0, o_dmu = 0, o_bonds = 0, o_grp = 0, o_grp_sig = 0, o_sp = 0;
-  std::vector<size_t> o_states, o_nst, o_bnd, o_md, o_gC, o_gP, o_rho, o_expo;
+  std::vector<size_t> o_states, o_nst, o_bnd, o_md, o_gC, o_gP, o_rho, o_expo, o_bslot, o_bslot_bond, o_eslot, o_eslot_bead;
   size_t o_Ext = 0, o_tr = 0, o_Csurf = 0, o_Wbond = 0, o_Wfmt = 0, o_Wmsa = 0, o_Wcoul = 0, o_tw = 0, o_twP = 0, o_twD = 0;
   size_t o_x = 0, o_g = 0, o_lam = 0, o_rb = 0, o_rbo = 0, o_Cb = 0, o_Cbond = 0, o_Cmu = 0, o_Clng = 0;
-  size_t o_wa = 0, o_wb = 0, o_wc = 0, o_wd = 0, o_fbe = 0;
+  size_t o_wa = 0, o_wb = 0, o_wc = 0, o_wd = 0, o_fbe = 0, o_elam = 0;
   size_t o_hx = 0, o_hg = 0, o_u = 0;
   size_t o_status = 0, o_iters = 0, o_err = 0, o_scal = 0, o_dreq = 0, o_slot = 0, o_out = 0;
   size_t bytes = 0;
@@ -282,6 +282,32 @@ int plan_species(const sdft_system_desc* d, Plan& pl) {
         for (int j = 0; j < h.nst[g + 1]; j++)
           h.bnd[((size_t)g * h.S + i) * h.S + j] =
               bond_lookup(pl.bonds, h.states[(size_t)g * h.S + i], h.states[(size_t)(g + 1) * h.S + j]);
+    // species-local slots of the bond types and bead types the species touches
+    h.bslot.assign(h.bnd.size(), -1);
+    for (size_t q = 0; q < h.bnd.size(); q++) {
+      if (h.bnd[q] < 0) continue;
+      int slot = -1;
+      for (size_t t = 0; t < h.bslot_bond.size(); t++)
+        if (h.bslot_bond[t] == h.bnd[q]) slot = (int)t;
+      if (slot < 0) {
+        slot = (int)h.bslot_bond.size();
+        h.bslot_bond.push_back(h.bnd[q]);
+      }
+      h.bslot[q] = slot;
+    }
+    h.eslot.assign(h.states.size(), -1);
+    for (int g = 0; g < h.n_seg; g++)
+      for (int i = 0; i < h.nst[g]; i++) {
+        const int b = h.states[(size_t)g * h.S + i];
+        int slot = -1;
+        for (size_t t = 0; t < h.eslot_bead.size(); t++)
+          if (h.eslot_bead[t] == b) slot = (int)t;
+        if (slot < 0) {
+          slot = (int)h.eslot_bead.size();
+          h.eslot_bead.push_back(b);
+        }
+        h.eslot[(size_t)g * h.S + i] = slot;
+      }
     h.fixed_density = s.fixed_density;
     h.mu_species = s.mu_species;
     // normative (child_propagators.jl:41-50): levels are visited leaves first
@@ -331,6 +357,10 @@ void plan_layout(Plan& pl, bool history) {
   pl.o_gP.resize(NS);
   pl.o_rho.resize(NS);
   pl.o_expo.resize(NS);
+  pl.o_bslot.resize(NS);
+  pl.o_bslot_bond.resize(NS);
+  pl.o_eslot.resize(NS);
+  pl.o_eslot_bead.resize(NS);
   for (int u = 0; u < NS; u++) {
     const SpeciesHost& h = pl.sp[u];
     pl.o_states[u] = lay.take<int>(h.states.size());
@@ -342,6 +372,10 @@ void plan_layout(Plan& pl, bool history) {
     pl.o_gP[u] = lay.take<double>(gsz);
     pl.o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
     pl.o_expo[u] = lay.take<int>((size_t)2 * h.n_seg);
+    pl.o_bslot[u] = lay.take<int>(h.bslot.size());
+    pl.o_bslot_bond[u] = lay.take<int>(h.bslot_bond.size() + 1);
+    pl.o_eslot[u] = lay.take<int>(h.eslot.size());
+    pl.o_eslot_bead[u] = lay.take<int>(h.eslot_bead.size() + 1);
   }
   pl.o_Ext = lay.take<double>((size_t)NB * P);
   pl.o_tr = lay.take<double>((size_t)NB * P);
@@ -369,6 +403,7 @@ void plan_layout(Plan& pl, bool history) {
   pl.o_wc = lay.take<double>((size_t)nwc * P);
   pl.o_wd = lay.take<double>((size_t)2 * NB * P);
   pl.o_fbe = lay.take<double>((size_t)4 * MB * P + 1);
+  pl.o_elam = lay.take<double>((size_t)NB * P);
   if (history) {
     pl.o_hx = lay.take<double>((size_t)kMaxAnderson * pl.n);
     pl.o_hg = lay.take<double>((size_t)kMaxAnderson * pl.n);
@@ -487,6 +522,12 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
     s.gP = h.n_seg > 1 ? (double*)at(pl.o_gP[u]) : nullptr;
     s.rho_seg = (double*)at(pl.o_rho[u]);
     s.expo = (int*)at(pl.o_expo[u]);
+    s.bslot = (const int*)at(pl.o_bslot[u]);
+    s.bslot_bond = (const int*)at(pl.o_bslot_bond[u]);
+    s.eslot = (const int*)at(pl.o_eslot[u]);
+    s.eslot_bead = (const int*)at(pl.o_eslot_bead[u]);
+    s.nbslot = (int)h.bslot_bond.size();
+    s.neslot = (int)h.eslot_bead.size();
   }
   DReq r{};
   r.NP = pl.P;
@@ -533,6 +574,7 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.wc = (double*)at(pl.o_wc);
   r.wd = (double*)at(pl.o_wd);
   r.fbe = (double*)at(pl.o_fbe);
+  r.elam = (double*)at(pl.o_elam);
   r.hx = pl.history ? (double*)at(pl.o_hx) : nullptr;
   r.hg = pl.history ? (double*)at(pl.o_hg) : nullptr;
   r.lsq_u = pl.history ? (double*)at(pl.o_u) : nullptr;
@@ -563,6 +605,10 @@ cudaError_t plan_upload(const sdft_system_desc* d, const Plan& pl, char* base, c
     up(pl.o_nst[u], h.nst.data(), sizeof(int) * h.nst.size());
     up(pl.o_bnd[u], h.bnd.data(), sizeof(int) * h.bnd.size());
     up(pl.o_md[u], h.md.data(), sizeof(double) * h.md.size());
+    up(pl.o_bslot[u], h.bslot.data(), sizeof(int) * h.bslot.size());
+    up(pl.o_bslot_bond[u], h.bslot_bond.data(), sizeof(int) * h.bslot_bond.size());
+    up(pl.o_eslot[u], h.eslot.data(), sizeof(int) * h.eslot.size());
+    up(pl.o_eslot_bead[u], h.eslot_bead.data(), sizeof(int) * h.eslot_bead.size());
   }
   up(pl.o_sp, dsp.data(), sizeof(DSpecies) * pl.NS);
   up(pl.o_Ext, pl.Ext.data(), sizeof(double) * pl.Ext.size());
