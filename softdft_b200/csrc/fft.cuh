@@ -90,6 +90,67 @@ __device__ __forceinline__ void store_b(const FftCtx& c, int nT, double scale, S
   }
 }
 
+// ---- grid-point pairs: the (K, K+1) samples of a transform moved together ----
+// Pair kp covers K = 2 kp (Makhoul index q = kp) and K + 1 (q = P - 1 - kp);
+// the functors read and write both samples with 16-byte accesses.  Each round
+// of a thread handles two pairs whose global loads are issued first.
+__device__ __forceinline__ double2 ldcg2(const double* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ void stcg2(double* p, double2 v) { __stcg(reinterpret_cast<double2*>(p), v); }
+
+__device__ __forceinline__ void put_pair(const FftCtx& c, int t, int kp, double2 v) {
+  double* zb = reinterpret_cast<double*>(c.z + (size_t)t * c.stride);
+  const int q1 = c.P - 1 - kp;
+  zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)] = v.x;
+  zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)] = v.y;
+}
+__device__ __forceinline__ double2 get_pair(const FftCtx& c, int t, int kp) {
+  const double* zb = reinterpret_cast<const double*>(c.z + (size_t)t * c.stride);
+  const int q1 = c.P - 1 - kp;
+  return make_double2(zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)], zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)]);
+}
+
+// f2(t, K) -> (f(K), f(K+1)) for even K
+template <class F2>
+__device__ __forceinline__ void load_b2(const FftCtx& c, int nT, F2 f2) {
+  const int lm = c.L;
+  const int total = nT << lm;
+  for (int b0 = threadIdx.x; b0 < total; b0 += 2 * blockDim.x) {
+    const int i1 = b0 + blockDim.x;
+    const double2 v0 = f2(b0 >> lm, (b0 & (c.M - 1)) << 1);
+    double2 v1 = make_double2(0.0, 0.0);
+    if (i1 < total) v1 = f2(i1 >> lm, (i1 & (c.M - 1)) << 1);
+    put_pair(c, b0 >> lm, b0 & (c.M - 1), v0);
+    if (i1 < total) put_pair(c, i1 >> lm, i1 & (c.M - 1), v1);
+  }
+}
+
+// put2(t, K, (y_K, y_K+1) * scale, pre2(t, K)) for even K; pre2 holds the loads
+template <class A2, class S2>
+__device__ __forceinline__ void store_b2(const FftCtx& c, int nT, double scale, A2 pre2, S2 put2) {
+  const int lm = c.L;
+  const int total = nT << lm;
+  for (int b0 = threadIdx.x; b0 < total; b0 += 2 * blockDim.x) {
+    const int i1 = b0 + blockDim.x;
+    const int t0 = b0 >> lm, K0 = (b0 & (c.M - 1)) << 1;
+    double2 y0 = get_pair(c, t0, K0 >> 1);
+    const double2 a0 = pre2(t0, K0);
+    double2 y1 = make_double2(0.0, 0.0), a1 = y1;
+    const int t1 = i1 >> lm, K1 = (i1 & (c.M - 1)) << 1;
+    if (i1 < total) {
+      y1 = get_pair(c, t1, K1 >> 1);
+      a1 = pre2(t1, K1);
+    }
+    y0.x *= scale;
+    y0.y *= scale;
+    put2(t0, K0, y0, a0);
+    if (i1 < total) {
+      y1.x *= scale;
+      y1.y *= scale;
+      put2(t1, K1, y1, a1);
+    }
+  }
+}
+
 __device__ __forceinline__ void bfly(double2& a, double2& b, double2 w) {  // DIT: (a + wb, a - wb)
   const double2 wb = cmul(b, w);
   b = sub2(a, wb);
@@ -390,6 +451,41 @@ __device__ __forceinline__ void dct2_convolve_b(const FftCtx& c, int nT, F f, W 
 }
 fft_inv_b(c, nT);
 store_b(c, nT, 1.0 / (double)M, store);
+__syncthreads();
+}
+
+// the same convolution with grid-point pair functors (load_b2 / store_b2)
+template <class F2, class W, class A2, class S2>
+__device__ __forceinline__ void dct2_convolve_b2(const FftCtx& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
+  const int P = c.P, M = c.M, H = c.H;
+  __syncthreads();
+  load_b2(c, nT, f2);
+  fft_fwd_b(c, nT);
+  SDFT_PAIR_LOOP(c, nT)
+  if (k == 0) {
+    const double2 dM = __ldg(&c.twD[M]);
+    double c0, cM;
+    zero_forward(zb[0], dM, &c0, &cM);
+    const double2 dh = __ldg(&c.twD[H]);
+    double ch, cPh;
+    mid_forward(zb[fpad(H)], dh, &ch, &cPh);
+    zb[0] = zero_inverse(c0 * wgt(t, 0), cM * wgt(t, M), dM);
+    zb[fpad(H)] = mid_inverse(ch * wgt(t, H), cPh * wgt(t, P - H), dh);
+  } else {
+    const double2 wk = __ldg(&c.twP[k]), dk = __ldg(&c.twD[k]), dk2 = __ldg(&c.twD[M - k]);
+    Quad q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], wk, dk, dk2);
+    q.c0 *= wgt(t, k);
+    q.c1 *= wgt(t, P - k);
+    q.c2 *= wgt(t, M - k);
+    q.c3 *= wgt(t, M + k);
+    double2 a, b;
+    pair_inverse(q, wk, dk, dk2, &a, &b);
+    zb[fpad(k)] = a;
+    zb[fpad(M - k)] = b;
+  }
+}
+fft_inv_b(c, nT);
+store_b2(c, nT, 1.0 / (double)M, pre2, put2);
 __syncthreads();
 }
 

@@ -167,19 +167,27 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
           gcc_t[t] = (c < N - 1) ? s.gC + ((size_t)(c * S + jj) * S) * P : nullptr;
           wb_t[t] = r.Wbond + (size_t)bond * P;
         }
-        dct2_convolve_b(
+        dct2_convolve_b2(
             fc, nT,
             [&](int t, int K) {
-              double f = in_t[t][K];
+              double2 f = ldcg2(in_t[t] + K);
               if (gcc_t[t]) {
-                double q2 = 0.0;
-                for (int q = 0; q < S; q++) q2 += gcc_t[t][(size_t)q * P + K];
-                f *= q2;
+                double2 q2 = make_double2(0.0, 0.0);
+                for (int q = 0; q < S; q++) {
+                  const double2 v = ldcg2(gcc_t[t] + (size_t)q * P + K);
+                  q2.x += v.x;
+                  q2.y += v.y;
+                }
+                f.x *= q2.x;
+                f.y *= q2.y;
               }
               return f;
             },
             [&](int t, int q) { return __ldg(&wb_t[t][q]); },
-            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * out_f[t][K] * inv_norm; });
+            [&](int t, int K) { return ldcg2(out_f[t] + K); },
+            [&](int t, int K, double2 y, double2 fo) {
+              stcg2(out_t[t] + K, make_double2(fabs(y.x) * fo.x * inv_norm, fabs(y.y) * fo.y * inv_norm));
+            });
       }
     }
     if (s.fixed >= 0) {  // max-distance mask (child_propagators.jl:147-157)
@@ -277,15 +285,23 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
           gpp_t[t] = s.gP + ((size_t)(p * S + jj) * S) * P;
           wb_t[t] = r.Wbond + (size_t)bond * P;
         }
-        dct2_convolve_b(
+        dct2_convolve_b2(
             fc, nT,
             [&](int t, int K) {
-              double q2 = 0.0;
-              for (int q = 0; q < S; q++) q2 += gpp_t[t][(size_t)q * P + K];
-              return in_t[t][K] * q2;
+              double2 q2 = make_double2(0.0, 0.0);
+              for (int q = 0; q < S; q++) {
+                const double2 v = ldcg2(gpp_t[t] + (size_t)q * P + K);
+                q2.x += v.x;
+                q2.y += v.y;
+              }
+              const double2 in = ldcg2(in_t[t] + K);
+              return make_double2(in.x * q2.x, in.y * q2.y);
             },
             [&](int t, int q) { return __ldg(&wb_t[t][q]); },
-            [&](int t, int K, double y) { out_t[t][K] = fabs(y) * out_f[t][K] * inv_norm; });
+            [&](int t, int K) { return ldcg2(out_f[t] + K); },
+            [&](int t, int K, double2 y, double2 fo) {
+              stcg2(out_t[t] + K, make_double2(fabs(y.x) * fo.x * inv_norm, fabs(y.y) * fo.y * inv_norm));
+            });
       }
     }
     if (s.fixed >= 0) {
