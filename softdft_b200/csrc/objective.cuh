@@ -530,8 +530,238 @@ __device__ __noinline__ void accumulate_regs(const DReq& r, const DSpecies& s, d
   __syncthreads();
 }
 
+// accumulate_regs for chains with at most two states per segment, on grid-point
+// pairs (K, K+1) with 16-byte loads, software-pipelined over the segment
+// states: the loads of the next (segment, state) are issued before the
+// current one is combined, so two steps' memory latencies overlap.  Same sums
+// in the same order as accumulate_regs.
+struct AccStep {
+  double2 el, p0, p1, c0, c1;
+};
+
+template <int BR, int ER>
+__device__ __noinline__ void accumulate_pairs(const DReq& r, const DSpecies& s, double norm, bool scaled) {
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  const double pref = norm * exp(s.mu_species);
+  const double* __restrict__ gP = s.gP;
+  const double* __restrict__ gC = s.gC;
+  const double* __restrict__ elam = r.elam;
+  const int* __restrict__ states = s.states;
+  const int* __restrict__ nst = s.nst;
+  const int* __restrict__ bslot = s.bslot;
+  const int* __restrict__ eslot = s.eslot;
+  auto seg_pref = [&](int g, double* lp, bool* direct) {
+    if (!scaled) {
+      *lp = 0.0;
+      *direct = false;
+      return pref;
+    }
+    *lp = log_prefactor(s, norm, g);
+    *direct = fabs(*lp) > 600.0;
+    return exp(*lp);
+  };
+  for (int kp = threadIdx.x; kp < P / 2; kp += blockDim.x) {
+    const int K = 2 * kp;
+    double2 a0[BR], a1[BR], ab[ER];
+#pragma unroll
+    for (int q = 0; q < BR; q++) a0[q] = a1[q] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < ER; q++) ab[q] = make_double2(0.0, 0.0);
+    // segment densities and bond end 0: steps (g, ii) in order
+    auto load1 = [&](int g, int ii, AccStep& d) {
+      const int si = states[g * S + ii];
+      d.el = ldcg2(elam + (size_t)si * P + K);
+      if (N > 1) {
+        d.p0 = ldcg2(gP + ((size_t)(g * S + ii) * S) * P + K);
+        if (S > 1) d.p1 = ldcg2(gP + ((size_t)(g * S + ii) * S + 1) * P + K);
+      }
+      const int nn = g < N - 1 ? nst[g + 1] : 0;
+      if (nn > 0) d.c0 = ldcg2(gC + ((size_t)(g * S + ii) * S) * P + K);
+      if (nn > 1) d.c1 = ldcg2(gC + ((size_t)(g * S + ii) * S + 1) * P + K);
+    };
+    {
+      int g = 0, ii = 0;
+      AccStep cur, nxt;
+      load1(0, 0, cur);
+      while (g < N) {
+        int g2 = g, ii2 = ii + 1;
+        if (ii2 == nst[g2]) {
+          g2++;
+          ii2 = 0;
+        }
+        if (g2 < N) load1(g2, ii2, nxt);
+        // combine (g, ii)
+        double lp;
+        bool direct;
+        const double elp = seg_pref(g, &lp, &direct);
+        const int si = states[g * S + ii];
+        double2 sp;
+        if (N > 1) {
+          sp.x = 0.0 + cur.p0.x;
+          sp.y = 0.0 + cur.p0.y;
+          if (S > 1) {
+            sp.x += cur.p1.x;
+            sp.y += cur.p1.y;
+          }
+        } else {
+          sp.x = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
+          sp.y = (s.fixed < 0 || K + 1 == s.fixed) ? 1.0 : 0.0;
+        }
+        double2 contr;
+        if (direct) {
+          contr.x = exp(lp - r.lambda[(size_t)si * P + K]) * sp.x;
+          contr.y = exp(lp - r.lambda[(size_t)si * P + K + 1]) * sp.y;
+        } else {
+          contr.x = elp * cur.el.x * sp.x;
+          contr.y = elp * cur.el.y * sp.y;
+        }
+        const int nn = g < N - 1 ? nst[g + 1] : 0;
+        double2 temp;
+        if (nn) {
+          temp = make_double2(0.0, 0.0);
+          const int b0 = bslot[(g * S + ii) * S];
+#pragma unroll
+          for (int q = 0; q < BR; q++)
+            if (q == b0) {
+              a0[q].x += contr.x * cur.c0.x;
+              a0[q].y += contr.y * cur.c0.y;
+            }
+          temp.x += cur.c0.x;
+          temp.y += cur.c0.y;
+          if (nn > 1) {
+            const int b1 = bslot[(g * S + ii) * S + 1];
+#pragma unroll
+            for (int q = 0; q < BR; q++)
+              if (q == b1) {
+                a0[q].x += contr.x * cur.c1.x;
+                a0[q].y += contr.y * cur.c1.y;
+              }
+            temp.x += cur.c1.x;
+            temp.y += cur.c1.y;
+          }
+        } else {
+          temp = make_double2(1.0, 1.0);
+        }
+        const double2 v = make_double2(contr.x * temp.x, contr.y * temp.y);
+        stcg2(s.rho_seg + (size_t)(g * S + ii) * P + K, v);
+        const int e = eslot[g * S + ii];
+        if (g == 0 && s.fixed >= 0) {
+#pragma unroll
+          for (int q = 0; q < ER; q++)
+            if (q == e) {
+              if (K == s.fixed) ab[q].x += v.x / r.dz / r.trapez[(size_t)si * P + K];
+              if (K + 1 == s.fixed) ab[q].y += v.y / r.dz / r.trapez[(size_t)si * P + K + 1];
+            }
+        } else {
+#pragma unroll
+          for (int q = 0; q < ER; q++)
+            if (q == e) {
+              ab[q].x += v.x;
+              ab[q].y += v.y;
+            }
+        }
+        cur = nxt;
+        g = g2;
+        ii = ii2;
+      }
+    }
+    // bond end 1: steps (c, ii), c >= 1
+    auto load2 = [&](int c, int ii, AccStep& d) {
+      const int si = states[c * S + ii];
+      d.el = ldcg2(elam + (size_t)si * P + K);
+      if (c < N - 1) {
+        d.c0 = ldcg2(gC + ((size_t)(c * S + ii) * S) * P + K);
+        if (S > 1) d.c1 = ldcg2(gC + ((size_t)(c * S + ii) * S + 1) * P + K);
+      }
+      const int np_ = nst[c - 1];
+      d.p0 = ldcg2(gP + ((size_t)(c * S + ii) * S) * P + K);
+      if (np_ > 1) d.p1 = ldcg2(gP + ((size_t)(c * S + ii) * S + 1) * P + K);
+    };
+    if (N > 1) {
+      int c = 1, ii = 0;
+      AccStep cur, nxt;
+      load2(1, 0, cur);
+      while (c < N) {
+        int c2 = c, ii2 = ii + 1;
+        if (ii2 == nst[c2]) {
+          c2++;
+          ii2 = 0;
+        }
+        if (c2 < N) load2(c2, ii2, nxt);
+        double lp;
+        bool direct;
+        const double elp = seg_pref(c, &lp, &direct);
+        const int si = states[c * S + ii];
+        double2 contr;
+        if (direct) {
+          contr.x = exp(lp - r.lambda[(size_t)si * P + K]);
+          contr.y = exp(lp - r.lambda[(size_t)si * P + K + 1]);
+        } else {
+          contr.x = elp * cur.el.x;
+          contr.y = elp * cur.el.y;
+        }
+        if (c < N - 1) {
+          double2 t = make_double2(0.0 + cur.c0.x, 0.0 + cur.c0.y);
+          if (S > 1) {
+            t.x += cur.c1.x;
+            t.y += cur.c1.y;
+          }
+          contr.x *= t.x;
+          contr.y *= t.y;
+        }
+        const int np_ = nst[c - 1];
+        const int b0 = bslot[((c - 1) * S) * S + ii];
+#pragma unroll
+        for (int q = 0; q < BR; q++)
+          if (q == b0) {
+            a1[q].x += contr.x * cur.p0.x;
+            a1[q].y += contr.y * cur.p0.y;
+          }
+        if (np_ > 1) {
+          const int b1 = bslot[((c - 1) * S + 1) * S + ii];
+#pragma unroll
+          for (int q = 0; q < BR; q++)
+            if (q == b1) {
+              a1[q].x += contr.x * cur.p1.x;
+              a1[q].y += contr.y * cur.p1.y;
+            }
+        }
+        cur = nxt;
+        c = c2;
+        ii = ii2;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < BR; q++)
+      if (q < s.nbslot) {
+        const int b = s.bslot_bond[q];
+        double* r0 = r.rho_bonds + (size_t)(b * 2 + 0) * P + K;
+        double* r1 = r.rho_bonds + (size_t)(b * 2 + 1) * P + K;
+        const double2 o0 = ldcg2(r0), o1 = ldcg2(r1);
+        stcg2(r0, make_double2(o0.x + a0[q].x, o0.y + a0[q].y));
+        stcg2(r1, make_double2(o1.x + a1[q].x, o1.y + a1[q].y));
+      }
+#pragma unroll
+    for (int q = 0; q < ER; q++)
+      if (q < s.neslot) {
+        double* rb = r.rho_beads + (size_t)s.eslot_bead[q] * P + K;
+        const double2 o = ldcg2(rb);
+        stcg2(rb, make_double2(o.x + ab[q].x, o.y + ab[q].y));
+      }
+  }
+  __syncthreads();
+}
+
 // true when the species went through accumulate_regs (its bead densities are added)
 __device__ __forceinline__ bool accumulate_fast(const DReq& r, const DSpecies& s, double norm, bool scaled) {
+  if (s.S <= 2 && s.nbslot <= 4 && s.neslot <= 2) {
+    accumulate_pairs<4, 2>(r, s, norm, scaled);
+    return true;
+  }
+  if (s.S <= 2 && s.nbslot <= 4 && s.neslot <= 4) {
+    accumulate_pairs<4, 4>(r, s, norm, scaled);
+    return true;
+  }
   if (s.nbslot <= 4 && s.neslot <= 4) {
     accumulate_regs<4, 4>(r, s, norm, scaled, s.gP, s.gC, r.elam, r.lambda, s.states, s.nst, s.bslot, s.eslot, s.rho_seg,
                           r.rho_bonds, r.rho_beads);
