@@ -752,8 +752,180 @@ __device__ __noinline__ void accumulate_pairs(const DReq& r, const DSpecies& s, 
   __syncthreads();
 }
 
+// accumulate_densities! for long grids, segment-outer: each (segment, state)
+// step streams its slices over the grid on point pairs, two pairs per round
+// with every load of the round issued first, and adds into rho_bonds /
+// rho_beads in place.  Per grid point the sums run over the steps in the
+// reference's order; two updates of one address are a whole grid sweep apart.
+// Chains with at most two states per segment.
+__device__ __noinline__ void accumulate_stream(const DReq& r, const DSpecies& s, double norm, bool scaled) {
+  const int P = r.NP, S = s.S, N = s.n_seg, P2 = P / 2;
+  const double pref = norm * exp(s.mu_species);
+  const int bd = blockDim.x;
+  for (int g = 0; g < N; g++) {
+    double lp = 0.0, elp = pref;
+    bool direct = false;
+    if (scaled) {
+      lp = log_prefactor(s, norm, g);
+      direct = fabs(lp) > 600.0;
+      elp = exp(lp);
+    }
+    const int nn = g < N - 1 ? s.nst[g + 1] : 0;
+    for (int ii = 0; ii < s.nst[g]; ii++) {
+      const int si = s.states[g * S + ii];
+      const double* el = r.elam + (size_t)si * P;
+      const double* gp = N > 1 ? s.gP + (size_t)(g * S + ii) * S * P : nullptr;
+      const double* gc = s.gC + (size_t)(g * S + ii) * S * P;
+      double* rb0 = nn > 0 ? r.rho_bonds + (size_t)(s.bnd[(g * S + ii) * S] * 2) * P : nullptr;
+      double* rb1 = nn > 1 ? r.rho_bonds + (size_t)(s.bnd[(g * S + ii) * S + 1] * 2) * P : nullptr;
+      double* rs = s.rho_seg + (size_t)(g * S + ii) * P;
+      double* rbd = r.rho_beads + (size_t)si * P;
+      const bool graft = g == 0 && s.fixed >= 0;
+      for (int k0 = threadIdx.x; k0 < P2; k0 += 2 * bd) {
+        AccStep d[2];
+        double2 o0[2], o1[2], ob[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int K = 2 * (k0 + u * bd);
+          if (K < P) {
+            d[u].el = ldcg2(el + K);
+            if (gp) {
+              d[u].p0 = ldcg2(gp + K);
+              if (S > 1) d[u].p1 = ldcg2(gp + P + K);
+            }
+            if (nn > 0) {
+              d[u].c0 = ldcg2(gc + K);
+              o0[u] = ldcg2(rb0 + K);
+            }
+            if (nn > 1) {
+              d[u].c1 = ldcg2(gc + P + K);
+              o1[u] = ldcg2(rb1 + K);
+            }
+            ob[u] = ldcg2(rbd + K);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int K = 2 * (k0 + u * bd);
+          if (K >= P) continue;
+          double2 sp;
+          if (gp) {
+            sp.x = 0.0 + d[u].p0.x;
+            sp.y = 0.0 + d[u].p0.y;
+            if (S > 1) {
+              sp.x += d[u].p1.x;
+              sp.y += d[u].p1.y;
+            }
+          } else {
+            sp.x = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
+            sp.y = (s.fixed < 0 || K + 1 == s.fixed) ? 1.0 : 0.0;
+          }
+          double2 contr;
+          if (direct) {
+            contr.x = exp(lp - r.lambda[(size_t)si * P + K]) * sp.x;
+            contr.y = exp(lp - r.lambda[(size_t)si * P + K + 1]) * sp.y;
+          } else {
+            contr.x = elp * d[u].el.x * sp.x;
+            contr.y = elp * d[u].el.y * sp.y;
+          }
+          double2 temp = make_double2(1.0, 1.0);
+          if (nn > 0) {
+            temp = make_double2(0.0 + d[u].c0.x, 0.0 + d[u].c0.y);
+            stcg2(rb0 + K, make_double2(o0[u].x + contr.x * d[u].c0.x, o0[u].y + contr.y * d[u].c0.y));
+          }
+          if (nn > 1) {
+            temp.x += d[u].c1.x;
+            temp.y += d[u].c1.y;
+            stcg2(rb1 + K, make_double2(o1[u].x + contr.x * d[u].c1.x, o1[u].y + contr.y * d[u].c1.y));
+          }
+          const double2 v = make_double2(contr.x * temp.x, contr.y * temp.y);
+          stcg2(rs + K, v);
+          if (graft) {
+            double2 b = ob[u];
+            if (K == s.fixed) b.x += v.x / r.dz / r.trapez[(size_t)si * P + K];
+            if (K + 1 == s.fixed) b.y += v.y / r.dz / r.trapez[(size_t)si * P + K + 1];
+            stcg2(rbd + K, b);
+          } else {
+            stcg2(rbd + K, make_double2(ob[u].x + v.x, ob[u].y + v.y));
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int c = 1; c < N; c++) {
+    double lp = 0.0, elp = pref;
+    bool direct = false;
+    if (scaled) {
+      lp = log_prefactor(s, norm, c);
+      direct = fabs(lp) > 600.0;
+      elp = exp(lp);
+    }
+    const int np_ = s.nst[c - 1];
+    for (int ii = 0; ii < s.nst[c]; ii++) {
+      const int si = s.states[c * S + ii];
+      const double* el = r.elam + (size_t)si * P;
+      const double* gc = c < N - 1 ? s.gC + (size_t)(c * S + ii) * S * P : nullptr;
+      const double* gp = s.gP + (size_t)(c * S + ii) * S * P;
+      double* rb0 = r.rho_bonds + (size_t)(s.bnd[((c - 1) * S) * S + ii] * 2 + 1) * P;
+      double* rb1 = np_ > 1 ? r.rho_bonds + (size_t)(s.bnd[((c - 1) * S + 1) * S + ii] * 2 + 1) * P : nullptr;
+      for (int k0 = threadIdx.x; k0 < P2; k0 += 2 * bd) {
+        AccStep d[2];
+        double2 o0[2], o1[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int K = 2 * (k0 + u * bd);
+          if (K < P) {
+            d[u].el = ldcg2(el + K);
+            if (gc) {
+              d[u].c0 = ldcg2(gc + K);
+              if (S > 1) d[u].c1 = ldcg2(gc + P + K);
+            }
+            d[u].p0 = ldcg2(gp + K);
+            o0[u] = ldcg2(rb0 + K);
+            if (np_ > 1) {
+              d[u].p1 = ldcg2(gp + P + K);
+              o1[u] = ldcg2(rb1 + K);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int K = 2 * (k0 + u * bd);
+          if (K >= P) continue;
+          double2 contr;
+          if (direct) {
+            contr.x = exp(lp - r.lambda[(size_t)si * P + K]);
+            contr.y = exp(lp - r.lambda[(size_t)si * P + K + 1]);
+          } else {
+            contr.x = elp * d[u].el.x;
+            contr.y = elp * d[u].el.y;
+          }
+          if (gc) {
+            double2 t = make_double2(0.0 + d[u].c0.x, 0.0 + d[u].c0.y);
+            if (S > 1) {
+              t.x += d[u].c1.x;
+              t.y += d[u].c1.y;
+            }
+            contr.x *= t.x;
+            contr.y *= t.y;
+          }
+          stcg2(rb0 + K, make_double2(o0[u].x + contr.x * d[u].p0.x, o0[u].y + contr.y * d[u].p0.y));
+          if (np_ > 1) stcg2(rb1 + K, make_double2(o1[u].x + contr.x * d[u].p1.x, o1[u].y + contr.y * d[u].p1.y));
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+}
+
 // true when the species went through accumulate_regs (its bead densities are added)
 __device__ __forceinline__ bool accumulate_fast(const DReq& r, const DSpecies& s, double norm, bool scaled) {
+  if (s.S <= 2 && s.n_seg > 1 && (r.NP >= 4096 || s.nbslot > 4 || s.neslot > 4)) {
+    accumulate_stream(r, s, norm, scaled);
+    return true;
+  }
   if (s.S <= 2 && s.nbslot <= 4 && s.neslot <= 2) {
     accumulate_pairs<4, 2>(r, s, norm, scaled);
     return true;
