@@ -1400,11 +1400,104 @@ __device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
   }
 }
 
+// Gamma, eta, H of every grid point into out[0..3P) from the MSA weighted
+// densities wa.  With a single diameter group (all beads of one size) each
+// thread iterates four points in lock-step, so that their dependent
+// divide/square-root chains overlap; the per-point arithmetic is exactly that
+// of gamma_msa_grouped, and a point's value is frozen once its own stopping
+// test fires.
+constexpr int kGammaLanes = 4;
+
+__device__ __noinline__ void msa_gamma_pass(const DReq& r, double* out) {
+  const int P = r.NP, nb = r.NB;
+  if (r.ngrp != 1) {
+    for (int K = threadIdx.x; K < P; K += blockDim.x) {
+      double rho[kMaxBeads];
+      for (int j = 0; j < nb; j++) rho[j] = r.wa[(size_t)j * P + K];
+      const MsaGamma gm = gamma_msa_point(r, rho);
+      out[K] = gm.G;
+      out[(size_t)P + K] = gm.eta;
+      out[(size_t)2 * P + K] = gm.H;
+    }
+    __syncthreads();
+    return;
+  }
+  const double lB = r.lB, tol = 1e-10, sg = r.grp_sig[0];
+  const int bd = blockDim.x;
+  for (int K0 = threadIdx.x; K0 < P; K0 += kGammaLanes * bd) {
+    double G[kGammaLanes], eta[kGammaLanes], H[kGammaLanes], cg[kGammaLanes], bg[kGammaLanes], ag[kGammaLanes],
+        term2[kGammaLanes];
+    bool live[kGammaLanes];
+#pragma unroll
+    for (int u = 0; u < kGammaLanes; u++) {
+      const int K = K0 + u * bd;
+      live[u] = false;
+      G[u] = eta[u] = H[u] = 0.0;
+      cg[u] = bg[u] = ag[u] = term2[u] = 0.0;
+      if (K >= P) continue;
+      double s = 0.0, sr = 0.0, srs = 0.0, s3 = 0.0;
+      for (int j = 0; j < nb; j++) {
+        const double rj = r.wa[(size_t)j * P + K], zj = r.z[j], sj = r.sig[j];
+        s += rj * zj * zj;
+        sr += rj * sj;
+        srs += rj;
+        s3 += rj * sj * sj * sj;
+        cg[u] += rj;
+        bg[u] += rj * zj;
+        ag[u] += rj * zj * zj;
+      }
+      const double kappa = sqrt(4.0 * kPi * lB * s);
+      if (kappa < tol) {
+        G[u] = kappa / 2.0;
+        eta[u] = 0.0;
+        H[u] = 2.0 / kPi;
+        continue;
+      }
+      const double sig_eff = sr / srs;
+      const double xx = sig_eff * sqrt(4.0 * kPi * lB * s);
+      G[u] = (sqrt(1.0 + 2.0 * xx) - 1.0) / (2.0 * sig_eff);
+      term2[u] = 2.0 / kPi * (1.0 - kPi / 6.0 * s3);
+      live[u] = true;
+    }
+    for (int it = 1;; it++) {
+      bool any = false;
+#pragma unroll
+      for (int u = 0; u < kGammaLanes; u++) {
+        if (!live[u]) continue;
+        const double inv = 1.0 / (1.0 + G[u] * sg);
+        const double hs = 0.0 + cg[u] * sg * sg * sg * inv;
+        const double es = 0.0 + bg[u] * sg * inv;
+        H[u] = hs + term2[u];
+        eta[u] = es / H[u];
+        const double s2 = sg * sg;
+        const double gs = 0.0 + (ag[u] - 2.0 * eta[u] * s2 * bg[u] + eta[u] * eta[u] * s2 * s2 * cg[u]) * (inv * inv);
+        const double G1 = sqrt(kPi * lB * gs);
+        const double Gn = 0.9 * G[u] + 0.1 * G1;
+        if (fabs(G1 - G[u]) < tol || it >= 1000) live[u] = false;
+        G[u] = Gn;
+        any |= live[u];
+      }
+      if (!any) break;
+    }
+#pragma unroll
+    for (int u = 0; u < kGammaLanes; u++) {
+      const int K = K0 + u * bd;
+      if (K < P) {
+        out[K] = G[u];
+        out[(size_t)P + K] = eta[u];
+        out[(size_t)2 * P + K] = H[u];
+      }
+    }
+  }
+  __syncthreads();
+}
+
 __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
   const int P = r.NP, NB = r.NB, MB = r.MB;
   const FftCtx fc = make_fft(sh.z, r);
   msa_weighted(r, sh, tpt1);
   __syncthreads();
+  msa_gamma_pass(r, r.wd);  // wd is free between the FMT stage and the next evaluation
   // point-wise derivative (TPT1msa.jl:129-156 -> iLST TPT1msa.jl:200-282)
   const double* sig = r.sig;
   const double* Z = r.z;
@@ -1412,8 +1505,7 @@ __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
   for (int K = threadIdx.x; K < P; K += blockDim.x) {
     double rho[kMaxBeads], dphi[kMaxBeads];
     for (int j = 0; j < NB; j++) rho[j] = r.wa[(size_t)j * P + K];
-    const MsaGamma gm = gamma_msa_point(r, rho);
-    const double G = gm.G, eta = gm.eta, H = gm.H;
+    const double G = r.wd[K], eta = r.wd[(size_t)P + K], H = r.wd[(size_t)2 * P + K];
     double us = 0.0;
     for (int j = 0; j < NB; j++)
       us += rho[j] * sig[j] * sig[j] * ((Z[j] - eta * sig[j] * sig[j]) / (1.0 + G * sig[j]) + Z[j]);
