@@ -162,6 +162,28 @@ int sdft_solve_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num,
  * No reference counterpart: measurement support for the batched solve. */
 int sdft_last_batch_stats(double* device_ms, int32_t* launches, double* latency_ms, int32_t n);
 
+/* Serving loop with continuous batching.  No reference counterpart: the
+ * reference solves one request per process (iDFT.jl); these entry points keep
+ * many requests resident on the GPU and admit new ones as slots free up.
+ *
+ * sdft_server_create: all requests of the server share `num`; at most
+ *   max_slots requests are active at a time and, when max_bytes > 0, the sum of
+ *   their device footprints (sdft_request_sizes) stays within max_bytes.
+ * sdft_server_submit: queue a request (it starts from its current state); the
+ *   handle must stay alive until its completion has been polled.
+ * sdft_server_step: admit queued requests (first in, first out), run every
+ *   active request for at most `iters` Anderson iterations in one launch, retire
+ *   the finished ones; returns the counts still active and still queued.
+ * sdft_server_poll: completions since the last poll (tag, sdft_status,
+ *   iterations, final residual, device ms from first to last iteration). */
+typedef struct sdft_server* sdft_server_t;
+int sdft_server_create(const sdft_numerics* num, int32_t max_slots, int64_t max_bytes, sdft_server_t* out);
+int sdft_server_destroy(sdft_server_t server);
+int sdft_server_submit(sdft_server_t server, sdft_handle h, int64_t tag);
+int sdft_server_step(sdft_server_t server, int32_t iters, int32_t* active, int32_t* queued);
+int sdft_server_poll(sdft_server_t server, int64_t* tags, int32_t* status, int32_t* iters, double* errs,
+                     double* device_ms, int32_t max, int32_t* n);
+
 /* Bytes of the static device array behind sdft_objective_noalloc (16 MiB). */
 #define SDFT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 

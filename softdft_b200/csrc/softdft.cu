@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <string>
 #include <vector>
 
@@ -915,6 +916,173 @@ extern "C" int sdft_last_batch_stats(double* device_ms, int32_t* launches, doubl
   if (launches) *launches = g_batch_launches;
   if (latency_ms)
     for (int i = 0; i < n && i < (int)g_batch_latency.size(); i++) latency_ms[i] = g_batch_latency[i];
+  return SDFT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// serving loop: continuous batching over persistent solver slots
+//
+// Requests are queued with sdft_server_submit and admitted, first in first
+// out, into free slots while the slot count and the device-byte budget allow.
+// Each sdft_server_step runs one launch of sdft_k_solve over the slots, at
+// most `iters` Anderson iterations per request, then retires the requests that
+// converged or failed; requests submitted meanwhile join at the next step.  A
+// request's fields, history and solver scalars stay on the device between
+// launches, so its result does not depend on the other requests in the mix.
+// ---------------------------------------------------------------------------
+struct sdft_server {
+  sdft_numerics num{};
+  int max_slots = 0;
+  long long max_bytes = 0;
+  cudaStream_t stream = nullptr;
+  DReq* dreqs = nullptr;
+  SolveSlot* dslots = nullptr;
+  std::vector<DReq> hreq;
+  std::vector<SolveSlot> hslot;
+  std::vector<sdft_handle> owner;   // per slot, null when free
+  std::vector<long long> tag;
+  std::deque<std::pair<sdft_handle, long long>> queue;
+  long long bytes_active = 0;
+  int active = 0;
+  struct Done {
+    long long tag;
+    int status, iters;
+    double err, device_ms;
+  };
+  std::deque<Done> done;
+};
+
+static int slot_status_to_rc(int st) {
+  return st == ST_OK ? SDFT_OK : st == ST_MAX_ITERS ? SDFT_MAX_ITERS : st == ST_NORM ? SDFT_ERR_NORM : SDFT_ERR_NONFINITE;
+}
+
+extern "C" int sdft_server_create(const sdft_numerics* num, int32_t max_slots, int64_t max_bytes, sdft_server_t* out) {
+  if (!out) return set_err(SDFT_ERR_ARG, "null argument");
+  *out = nullptr;
+  int rc = validate_numerics(num);
+  if (rc) return rc;
+  if (max_slots < 1 || max_slots > 65535) return set_err(SDFT_ERR_ARG, "max_slots must be in [1, 65535]");
+  auto* sv = new sdft_server();
+  sv->num = *num;
+  sv->max_slots = max_slots;
+  sv->max_bytes = max_bytes;
+  cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&sv->dreqs, sizeof(DReq) * max_slots);
+  if (e == cudaSuccess) e = cudaMalloc(&sv->dslots, sizeof(SolveSlot) * max_slots);
+  if (e != cudaSuccess) {
+    if (sv->dreqs) cudaFree(sv->dreqs);
+    if (sv->stream) cudaStreamDestroy(sv->stream);
+    delete sv;
+    return set_err(SDFT_ERR_OOM, std::string("server allocation: ") + cudaGetErrorString(e));
+  }
+  sv->hreq.assign(max_slots, DReq{});
+  SolveSlot idle{};
+  idle.status = -1;  // not ST_RUNNING: the kernel skips the slot
+  sv->hslot.assign(max_slots, idle);
+  sv->owner.assign(max_slots, nullptr);
+  sv->tag.assign(max_slots, 0);
+  *out = sv;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_server_destroy(sdft_server_t sv) {
+  if (!sv) return SDFT_OK;
+  cudaStreamSynchronize(sv->stream);
+  cudaFree(sv->dreqs);
+  cudaFree(sv->dslots);
+  cudaStreamDestroy(sv->stream);
+  delete sv;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_server_submit(sdft_server_t sv, sdft_handle h, int64_t tag) {
+  if (!sv || !h) return set_err(SDFT_ERR_ARG, "null argument");
+  if (sv->max_bytes > 0 && (long long)h->bytes > sv->max_bytes)
+    return set_err(SDFT_ERR_ARG, "request needs more device memory than the server budget");
+  sv->queue.emplace_back(h, tag);
+  return SDFT_OK;
+}
+
+extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active, int32_t* queued) {
+  if (!sv) return set_err(SDFT_ERR_ARG, "null server");
+  if (iters < 1) return set_err(SDFT_ERR_ARG, "iters must be >= 1");
+  // admission: FIFO into free slots within the byte budget
+  for (int i = 0; i < sv->max_slots && !sv->queue.empty(); i++) {
+    if (sv->owner[i]) continue;
+    sdft_handle h = sv->queue.front().first;
+    if (sv->max_bytes > 0 && sv->bytes_active + (long long)h->bytes > sv->max_bytes) break;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));  // the request's own uploads are complete
+    sv->owner[i] = h;
+    sv->tag[i] = sv->queue.front().second;
+    sv->queue.pop_front();
+    sv->hreq[i] = h->h;
+    SolveSlot s{};
+    s.iter = 0;
+    s.status = ST_RUNNING;
+    s.use_picard = 1;
+    s.err = 1.0;
+    sv->hslot[i] = s;
+    sv->bytes_active += (long long)h->bytes;
+    sv->active++;
+  }
+  int hi = 0;
+  size_t sm = 0;
+  for (int i = 0; i < sv->max_slots; i++)
+    if (sv->owner[i]) {
+      hi = i + 1;
+      sm = std::max(sm, smem_bytes(sv->owner[i]->M));
+    }
+  if (hi > 0) {
+    int rc = prepare_kernel((const void*)sdft_k_solve, sm);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(sv->dreqs, sv->hreq.data(), sizeof(DReq) * hi, cudaMemcpyHostToDevice, sv->stream));
+    CUDA_TRY(cudaMemcpyAsync(sv->dslots, sv->hslot.data(), sizeof(SolveSlot) * hi, cudaMemcpyHostToDevice, sv->stream));
+    SolveCfg cfg;
+    cfg.max_iters = sv->num.max_iters;
+    cfg.anderm = sv->num.anderm;
+    cfg.damping = sv->num.damping;
+    cfg.mixing_max = sv->num.mixing_max;
+    cfg.switch_tole = sv->num.switch_tole;
+    cfg.tole = sv->num.tole;
+    sdft_k_solve<<<hi, kThreads, sm, sv->stream>>>(sv->dreqs, sv->dslots, cfg, iters);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(sv->hslot.data(), sv->dslots, sizeof(SolveSlot) * hi, cudaMemcpyDeviceToHost, sv->stream));
+    CUDA_TRY(cudaStreamSynchronize(sv->stream));
+    for (int i = 0; i < hi; i++) {
+      if (!sv->owner[i] || sv->hslot[i].status == ST_RUNNING) continue;
+      sdft_server::Done d;
+      d.tag = sv->tag[i];
+      d.status = slot_status_to_rc(sv->hslot[i].status);
+      d.iters = sv->hslot[i].iter;
+      d.err = sv->hslot[i].err;
+      d.device_ms = (double)(sv->hslot[i].t1 - sv->hslot[i].t0) * 1e-6;
+      sv->done.push_back(d);
+      sv->bytes_active -= (long long)sv->owner[i]->bytes;
+      sv->owner[i] = nullptr;
+      sv->hslot[i].status = -1;
+      sv->active--;
+    }
+  }
+  if (active) *active = sv->active;
+  if (queued) *queued = (int32_t)sv->queue.size();
+  return SDFT_OK;
+}
+
+extern "C" int sdft_server_poll(sdft_server_t sv, int64_t* tags, int32_t* status, int32_t* iters, double* errs,
+                                double* device_ms, int32_t max, int32_t* n) {
+  if (!sv || !n) return set_err(SDFT_ERR_ARG, "null argument");
+  int k = 0;
+  while (k < max && !sv->done.empty()) {
+    const auto& d = sv->done.front();
+    if (tags) tags[k] = d.tag;
+    if (status) status[k] = d.status;
+    if (iters) iters[k] = d.iters;
+    if (errs) errs[k] = d.err;
+    if (device_ms) device_ms[k] = d.device_ms;
+    sv->done.pop_front();
+    k++;
+  }
+  *n = k;
   return SDFT_OK;
 }
 

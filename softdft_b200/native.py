@@ -24,7 +24,8 @@ STATUS_NAMES = {0: "OK", 1: "MAX_ITERS", 2: "ERR_ARG", 3: "ERR_UNSUPPORTED", 4: 
 EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_numerics_default",
            "sdft_request_create", "sdft_request_destroy", "sdft_request_sizes", "sdft_set_state",
            "sdft_get_state", "sdft_objective", "sdft_solve", "sdft_get_densities", "sdft_grand_potential",
-           "sdft_num_species", "sdft_solve_batch", "sdft_last_batch_stats"]
+           "sdft_num_species", "sdft_solve_batch", "sdft_last_batch_stats", "sdft_server_create",
+           "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll"]
 
 
 class SdftError(RuntimeError):
@@ -57,6 +58,11 @@ def lib():
         L.sdft_num_species.argtypes = [vp, vp]
         L.sdft_solve_batch.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
         L.sdft_last_batch_stats.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int32), vp, C.c_int32]
+        L.sdft_server_create.argtypes = [vp, C.c_int32, C.c_int64, C.POINTER(vp)]
+        L.sdft_server_destroy.argtypes = [vp]
+        L.sdft_server_submit.argtypes = [vp, vp, C.c_int64]
+        L.sdft_server_step.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.sdft_server_poll.argtypes = [vp, vp, vp, vp, vp, vp, C.c_int32, C.POINTER(C.c_int32)]
         _LIB = L
     return _LIB
 
@@ -178,3 +184,47 @@ def objective_noalloc(d: Descriptor, x_dev_ptr: int, g_dev_ptr: int, stream_ptr:
     f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     f.restype = C.c_int
     _check(f(C.byref(d.desc), C.c_void_p(x_dev_ptr), C.c_void_p(g_dev_ptr), C.c_void_p(stream_ptr or None)))
+
+
+class Server:
+    """Continuous-batching solve server (sdft_server_*): requests are admitted
+    into free slots as earlier ones finish; each step is one launch."""
+
+    def __init__(self, num: Numerics, max_slots: int, max_bytes: int = 0):
+        self.h = C.c_void_p()
+        _check(lib().sdft_server_create(C.byref(num), int(max_slots), int(max_bytes), C.byref(self.h)))
+        self._held = {}
+
+    def close(self):
+        if self.h:
+            lib().sdft_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, system: "DeviceSystem", tag: int) -> None:
+        _check(lib().sdft_server_submit(self.h, system.h, int(tag)))
+        self._held[int(tag)] = system
+
+    def step(self, iters: int):
+        a, q = C.c_int32(), C.c_int32()
+        _check(lib().sdft_server_step(self.h, int(iters), C.byref(a), C.byref(q)))
+        return int(a.value), int(q.value)
+
+    def poll(self, max_n: int = 4096):
+        tags = np.zeros(max_n, dtype=np.int64)
+        st = np.zeros(max_n, dtype=np.int32)
+        it = np.zeros(max_n, dtype=np.int32)
+        err = np.zeros(max_n)
+        dms = np.zeros(max_n)
+        n = C.c_int32()
+        _check(lib().sdft_server_poll(self.h, _p(tags), _p(st), _p(it), _p(err), _p(dms), max_n, C.byref(n)))
+        out = []
+        for i in range(n.value):
+            self._held.pop(int(tags[i]), None)
+            out.append((int(tags[i]), int(st[i]), int(it[i]), float(err[i]), float(dms[i])))
+        return out

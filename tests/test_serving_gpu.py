@@ -1,0 +1,76 @@
+"""Continuous batching on the device: requests submitted while others run are
+admitted as slots free up, and each result is the same alone and in the mix
+(bit for bit: a request's state never depends on the other slots)."""
+import copy
+
+import numpy as np
+import pytest
+
+from softdft_b200 import native
+from softdft_b200.host.descriptor import numerics_from_dict
+from tests.helpers import descriptor, small_slit
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    # parameter points that converge under these numerics (the CPU oracle takes
+    # 683-2579 iterations); their different iteration counts make requests
+    # finish, and slots free up, at different steps
+    pts = [(7.0, 0.1, 6), (8.0, 0.1, 7), (9.0, 0.2, 8), (4.0, 0.1, 9), (8.5, 0.3, 6)]
+    return [small_slit(pH=pH, salt=salt, n_chain=n) for pH, salt, n in pts]
+
+
+def test_results_alone_equal_results_in_the_mix():
+    cases = _cases()
+    numd = dict(cases[0]["numerical"], tole=1e-8, max_iters=5000)
+    num = numerics_from_dict(numd)
+    dfts = [descriptor(c) for c in cases]
+    alone = []
+    for d in dfts:
+        s = native.DeviceSystem(d.descriptor)
+        it, err, rc = s.solve(num)
+        assert rc == 0
+        alone.append((s.get_x(), it))
+    srv = native.Server(num, max_slots=3)
+    systems = [native.DeviceSystem(d.descriptor) for d in dfts]
+    # staggered submission: two now, the rest while those run
+    srv.submit(systems[0], 0)
+    srv.submit(systems[1], 1)
+    done = {}
+    pending = 2
+    nxt = 2
+    steps = 0
+    while len(done) < len(systems):
+        active, queued = srv.step(7)
+        steps += 1
+        for tag, st, it, err, dms in srv.poll():
+            done[tag] = (st, it, err)
+        if nxt < len(systems) and steps % 2 == 1:
+            srv.submit(systems[nxt], nxt)
+            nxt += 1
+        assert active <= 3
+        assert steps < 5000
+    for i, s in enumerate(systems):
+        st, it, err = done[i]
+        assert st == 0 and err < 1e-8
+        assert it == alone[i][1]
+        assert np.array_equal(s.get_x(), alone[i][0])
+    srv.close()
+
+
+def test_byte_budget_limits_admission():
+    cases = _cases()[:3]
+    num = numerics_from_dict(dict(cases[0]["numerical"], tole=1e-8, max_iters=5000))
+    systems = [native.DeviceSystem(descriptor(c).descriptor) for c in cases]
+    one = max(s.device_bytes for s in systems)
+    srv = native.Server(num, max_slots=8, max_bytes=one)  # room for one request at a time
+    for i, s in enumerate(systems):
+        srv.submit(s, i)
+    done = []
+    while len(done) < 3:
+        active, queued = srv.step(50)
+        assert active <= 1
+        done += srv.poll()
+    assert sorted(t for t, *_ in done) == [0, 1, 2]
+    srv.close()
