@@ -125,15 +125,20 @@ def solver_dft(dft: IsingDFT) -> int:
     return it
 
 
-def eval_inhomogeneous(dft: IsingDFT) -> IsingDFT:
+def eval_inhomogeneous(dft: IsingDFT, directory: Optional[str] = ".") -> IsingDFT:
+    """solver_dft, then the analysis files of call_analysis written into
+    `directory` (eval_inhomogeneous.jl:4-11); directory=None only solves."""
     solver_dft(dft)
+    if directory is not None:
+        from .output import call_analysis
+        call_analysis(dft, directory)
     return dft
 
 
-def iDFT(input_file: str, precision: int = desc_mod.PREC_FP64) -> IsingDFT:
+def iDFT(input_file: str, precision: int = desc_mod.PREC_FP64, directory: Optional[str] = ".") -> IsingDFT:
     dataset = yamlio.load_file(input_file)
     dft = setup_request(dataset, precision)
-    return eval_inhomogeneous(dft)
+    return eval_inhomogeneous(dft, directory)
 
 
 def densities(dft: IsingDFT):

@@ -1,0 +1,299 @@
+"""Natural-parameter continuation over wall separation and pH.
+
+Restates the sweep routines of the reference:
+
+* `adjust_distancesZ` (`routines/adjust_distanceZ.jl:15-155`): the wall
+  separation grows by `stepZ` per step; each step rebuilds the system, starts
+  from the previous solution, solves, records the grand potential, the energy
+  Omega + P_bulk H and the contact-value pressure, and the sweep stops after 20
+  consecutive steps with |dE| < errP or past `stopZ`;
+* `adjust_pH` (`routines/adjust_pH.jl:16-125`): pH (the pSpecies of the `Y`
+  species) runs over start:step:stop; each step writes the analysis files and
+  reads back the brush height and the average degree of ionisation, and the
+  sweep stops once alpha reaches 0.99 (rising pH) or 0.01 (falling pH);
+* `batched_distance_sweep`: the wall-separation sweep of many independent
+  branches at once, every step of all branches solved in one batched device
+  launch.
+
+Warm start.  The routines copy the near-wall halves of the previous segment and
+bond densities and PsiC into the new system, but the solver's unknowns are
+(mu_ex_K, lng_K, Psi, PsiC) (`solver_dft.jl:13`) and `eval_spatial_density!`
+recomputes the densities from them, so in the reference only PsiC carries over.
+Here the unknowns themselves carry over: the point at distance d from the
+nearer wall of the new slit takes the previous solution's value at distance d
+from the same wall (linear interpolation; the previous slit's midpoint value
+beyond its half width).  With an unchanged grid spacing and a change of H by
+whole grid spacings this is the routines' index copy of the near-wall halves.
+
+Grid.  The device transform needs NP = 2^k.  When `pow2` is set (the default)
+a step with wall separation H keeps the requested spacing as an upper bound:
+NP is the smallest power of two with NP >= cld(H, dz) + 1 and the spacing is
+H / (NP - 1) (nudged so that the reference's rule NP = cld(H, dz) + 1 gives
+exactly NP).
+"""
+from __future__ import annotations
+
+import copy
+import math
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import native
+from .api import IsingDFT, densities, eval_inhomogeneous, geometry_system, grand_potential, iLST, setup_iDFT
+from .host.descriptor import numerics_from_dict
+from .host.geometry import cld
+from .output import contact_value_theorem_arrays, jl
+
+
+# ---- grid and warm start ------------------------------------------------------
+
+def pow2_bin_width(H: float, dz: float) -> float:
+    """Spacing <= dz for which NP = cld(H, spacing) + 1 is a power of two."""
+    need = cld(H, dz) + 1
+    NP = 1 << max(4, math.ceil(math.log2(need)))
+    w = H / (NP - 1)
+    while cld(H, w) + 1 > NP:
+        w = math.nextafter(w, math.inf)
+    while cld(H, w) + 1 < NP:
+        w = math.nextafter(w, 0.0)
+    return w
+
+
+def set_distance(data: dict, H: float, dz: Optional[float] = None, pow2: bool = True) -> None:
+    """Wall separation H in place (data["geometry"]["dimensions"] = [H])."""
+    g = data["geometry"]
+    g["dimensions"] = [H]
+    if pow2:
+        base = float(dz if dz is not None else g["bin_width"][0])
+        g["bin_width"] = [pow2_bin_width(H, base)]
+    elif dz is not None:
+        g["bin_width"] = [dz]
+
+
+def _resample(f: np.ndarray, np_old: int, dz_old: float, np_new: int, dz_new: float) -> np.ndarray:
+    """Columns of f (grid index first) onto the new grid by distance to the
+    nearer wall, in units of the old grid (exact index copies when the
+    spacings are equal)."""
+    r = dz_new / dz_old
+    K = np.arange(np_new, dtype=np.float64)
+    mid_old = (np_old - 1) / 2.0
+    left = K <= (np_new - 1) / 2.0
+    pos = np.where(left, np.minimum(K * r, mid_old), np.maximum((np_old - 1) - (np_new - 1 - K) * r, mid_old))
+    i0 = np.clip(np.floor(pos).astype(np.int64), 0, np_old - 1)
+    i1 = np.minimum(i0 + 1, np_old - 1)
+    w = pos - i0
+    flat = f.reshape(f.shape[0], -1)
+    out = np.where(w[:, None] == 0.0, flat[i0], flat[i0] * (1.0 - w[:, None]) + flat[i1] * w[:, None])
+    return out.reshape((np_new,) + f.shape[1:])
+
+
+def resample_state(state, old_geometry, new_geometry):
+    """(mu_ex_K, lng_K, Psi, PsiC) of a solved slit onto another slit's grid."""
+    mu, lng, psi, psic = state
+    a = (old_geometry.NP, old_geometry.bin_width, new_geometry.NP, new_geometry.bin_width)
+    return (np.asfortranarray(_resample(np.asarray(mu), *a)), np.asfortranarray(_resample(np.asarray(lng), *a)),
+            _resample(np.asarray(psi), *a), np.array(psic, dtype=np.float64))
+
+
+# ---- measurements -------------------------------------------------------------
+
+def slit_measurements(dft: IsingDFT) -> dict:
+    """Omega, energy Omega + P_bulk H and the contact-value pressure of a solved slit."""
+    H = dft.geometry.dimensions
+    omega = grand_potential(dft)
+    p_bulk = dft.bulk_system.bulk.pressure
+    _, beads, _ = densities(dft)
+    cvt = contact_value_theorem_arrays(beads, dft.bulk_system.molsys, dft.geometry)
+    return {"distance": H, "NP": dft.NP, "omega": omega, "energy": omega + p_bulk * H, "Pressure": float(cvt[0]),
+            "deltaP": float(cvt[0]) - p_bulk}
+
+
+# ---- adjust_distancesZ --------------------------------------------------------
+
+def _fmt_dir(prefix: str, v: float, digits: int = 2) -> str:
+    return prefix + f"{v:0.{digits}f}"
+
+
+def adjust_distancesZ(data: dict, startZ: float = 1.6, stopZ: float = 20.0, stepZ: float = 0.02, errP: float = 1e-6,
+                      out_root: Optional[str] = "dist_sweep", dz: Optional[float] = None, pow2: bool = True,
+                      max_count: int = 20) -> List[dict]:
+    """routines/adjust_distanceZ.jl:15-155 (files under out_root when given)."""
+    data = copy.deepcopy(data)
+    bulk = iLST(data)  # the bulk state does not depend on the wall separation
+    results: List[dict] = []
+    distance, count, i = startZ, 0, 0
+    prev = None
+    if out_root is not None:
+        os.makedirs(out_root, exist_ok=True)
+    while count < max_count:
+        distance += stepZ
+        i += 1
+        set_distance(data, distance, dz, pow2)
+        geom = geometry_system(data)
+        dft = setup_iDFT(data, bulk, geom)
+        step_dir = None
+        if out_root is not None:
+            step_dir = os.path.join(out_root, _fmt_dir("dist_", distance))
+            os.makedirs(step_dir, exist_ok=True)
+        if prev is not None:
+            dft.state = resample_state(prev[0], prev[1], geom)
+        eval_inhomogeneous(dft, step_dir)
+        m = slit_measurements(dft)
+        delta_E = m["energy"] - results[-1]["energy"] if results else 10.0
+        r = {"step": i, **m, "iterations": dft.iterations, "status": dft.status, "residual": dft.residual}
+        results.append(r)
+        if step_dir is not None:
+            with open(os.path.join(step_dir, "run_info.csv"), "w") as fh:
+                fh.write("step,distance,Pressure,deltaP,energy\n")
+                fh.write(f"{i},{jl(r['distance'])},{jl(r['Pressure'])},{jl(r['deltaP'])},{jl(r['energy'])}\n")
+        count = count + 1 if abs(delta_E) < errP else 0
+        if distance > stopZ:
+            count = max_count + 1
+        prev = (dft.state, geom)
+        dft.handle().close()
+    if out_root is not None:
+        final_E, final_dP = results[-1]["energy"], results[-1]["deltaP"]
+        with open(os.path.join(out_root, "adjust_distancesZ_results.csv"), "w") as fh:
+            fh.write("step,distance,Pressure,deltaP,energy,deltaE\n")
+            for r in results:
+                fh.write(f"{r['step']},{jl(r['distance'])},{jl(r['Pressure'])},{jl(r['deltaP'] - final_dP)},"
+                         f"{jl(r['energy'])},{jl(r['energy'] - final_E)}\n")
+    return results
+
+
+# ---- adjust_pH ----------------------------------------------------------------
+
+def julia_range(start: float, step: float, stop: float) -> List[float]:
+    """start:step:stop for floats: the values that do not pass stop."""
+    n = math.floor((stop - start) / step * (1 + 1e-12) + 1e-9) + 1
+    return [start + k * step for k in range(max(n, 0))]
+
+
+def read_brush_height(path: str) -> dict:
+    """routines/adjust_pH.jl:246-276."""
+    vals = {}
+    if not os.path.isfile(path):
+        return vals
+    for ln in open(path):
+        s = ln.strip()
+        if not s or s.startswith("#"):
+            continue
+        parts = s.split()
+        if len(parts) < 2:
+            continue
+        try:
+            vals[parts[0]] = float(parts[1])
+        except ValueError:
+            continue
+    return vals
+
+
+def read_avg_state_fraction(path: str, state_index: int = 2) -> Optional[float]:
+    """routines/adjust_pH.jl:278-295: the `avg` line's state_index-th entry."""
+    alpha = None
+    for ln in open(path):
+        s = ln.strip()
+        if not s.startswith("avg "):
+            continue
+        parts = s.split()
+        if len(parts) >= 1 + state_index and parts[state_index]:
+            alpha = float(parts[state_index])
+    return alpha
+
+
+def _set_pH(data: dict, pH: float) -> None:
+    for sp in data["species"]:
+        if sp.get("sequence") == "Y":
+            sp["pSpecies"] = pH
+            return
+
+
+def adjust_pH(data: dict, startZ: float = 3.0, stopZ: float = 10.0, stepZ: float = 0.05,
+              out_root: str = "pH_sweep") -> List[dict]:
+    """routines/adjust_pH.jl:16-125.  The analysis files of every step are written
+    under out_root/pH_<pH> and the brush height and alpha are read back from
+    them, as the routine does; alpha is taken from the total_state_fractions
+    file of the first species with dissociating segments."""
+    data = copy.deepcopy(data)
+    root = os.path.abspath(out_root)
+    os.makedirs(root, exist_ok=True)
+    results: List[dict] = []
+    prev = None
+    for i, pH in enumerate(julia_range(startZ, stepZ, stopZ), start=1):
+        step_dir = os.path.join(out_root, _fmt_dir("pH_", pH))
+        os.makedirs(step_dir, exist_ok=True)
+        _set_pH(data, pH)
+        bulk = iLST(data)
+        geom = geometry_system(data)
+        dft = setup_iDFT(data, bulk, geom)
+        if prev is not None:
+            dft.state = prev
+        eval_inhomogeneous(dft, step_dir)
+        ms = dft.bulk_system.molsys
+        hb = read_brush_height(os.path.join(step_dir, "brush_height.txt"))
+        if len(hb) > 1:
+            raise ValueError("more than one grafted species in brush_height.txt")
+        h = next(iter(hb.values())) if hb else float("nan")
+        alpha = float("nan")
+        for u, cfg in enumerate(ms.configurations):
+            if any(len(f) > 1 for f in cfg.state_family):
+                a = read_avg_state_fraction(os.path.join(step_dir, f"total_state_fractions_{ms.species[u]}.txt"), 2)
+                alpha = float("nan") if a is None else a
+                break
+        r = {"step": i, "pH": pH, "brush_height": h, "alpha": alpha, "iterations": dft.iterations,
+             "status": dft.status, "residual": dft.residual}
+        results.append(r)
+        summary = os.path.join(root, "summary_brush_alpha.csv")
+        header = not os.path.isfile(summary) or os.path.getsize(summary) == 0
+        with open(summary, "w" if header else "a") as fh:
+            if header:
+                fh.write("step,pH,brush_height,alpha\n")
+            fh.write("%d,%.12g,%.12g,%.12g\n" % (i, pH, h, alpha))
+        with open(os.path.join(step_dir, "run_info.csv"), "w" if i == 1 else "a") as fh:
+            if i == 1:
+                fh.write("step,pH,brush_height,alpha\n")
+            fh.write(f"{i},{jl(pH)},{jl(h)},{jl(alpha)}\n")
+        prev = dft.state
+        dft.handle().close()
+        if alpha >= 0.99 and stepZ > 0:
+            break
+        if alpha <= 0.01 and stepZ < 0:
+            break
+    return results
+
+
+# ---- batched branches -----------------------------------------------------------
+
+def batched_distance_sweep(branches: Sequence[dict], distances: Sequence[float], dz: Optional[float] = None,
+                           pow2: bool = True, num=None) -> List[List[dict]]:
+    """Wall-separation sweep of independent branches (input datasets, one per
+    branch, sharing the numerics): at every distance all branches are solved in
+    one batched launch, each starting from its own previous solution.  Returns
+    per branch the list of per-step measurements."""
+    datas = [copy.deepcopy(b) for b in branches]
+    bulks = [iLST(d) for d in datas]
+    if num is None:
+        num = numerics_from_dict(datas[0].get("numerical") or {})
+    prev = [None] * len(datas)
+    out: List[List[dict]] = [[] for _ in datas]
+    for step, H in enumerate(distances, start=1):
+        dfts = []
+        for b, d in enumerate(datas):
+            set_distance(d, H, dz, pow2)
+            geom = geometry_system(d)
+            dft = setup_iDFT(d, bulks[b], geom)
+            if prev[b] is not None:
+                dft.state = resample_state(prev[b][0], prev[b][1], geom)
+            dfts.append(dft)
+        iters, errs, status = native.solve_batch([t.handle() for t in dfts], num)
+        device_ms, launches, _ = native.last_batch_stats(len(dfts))
+        for b, dft in enumerate(dfts):
+            dft.iterations, dft.residual, dft.status = int(iters[b]), float(errs[b]), int(status[b])
+            m = slit_measurements(dft)
+            out[b].append({"step": step, **m, "iterations": int(iters[b]), "status": int(status[b]),
+                           "residual": float(errs[b]), "batch_device_ms": device_ms})
+            prev[b] = (dft.state, dft.geometry)
+            dft.handle().close()
+    return out

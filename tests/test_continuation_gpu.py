@@ -1,0 +1,78 @@
+"""Batched wall-separation continuation on the device: every step of all
+branches in one launch gives the same numbers as each branch swept alone, and
+each step's grand potential matches the CPU oracle solving the same
+warm-started state (converged-state tolerance)."""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleSystem
+from softdft_b200 import continuation as ct
+from softdft_b200 import native, workloads
+from softdft_b200.api import geometry_system, iLST, setup_iDFT
+from softdft_b200.host.descriptor import numerics_from_dict
+
+pytestmark = pytest.mark.gpu
+
+
+def _branches():
+    out = []
+    for pH in (6.0, 8.0):
+        ds = workloads.grafted_brush(128, 0.05, 8, 0.05, 4.5, pH, 0.01)
+        ds["numerical"] = dict(ds["numerical"], tole=1e-10, max_iters=8000)
+        out.append(ds)
+    return out
+
+
+DIST = [6.0, 5.4, 4.8]
+
+
+def test_batched_sweep_equals_branches_alone():
+    br = _branches()
+    together = ct.batched_distance_sweep(br, DIST, dz=0.05)
+    for b, ds in enumerate(br):
+        alone = ct.batched_distance_sweep([ds], DIST, dz=0.05)[0]
+        for s_t, s_a in zip(together[b], alone):
+            assert s_t["status"] == 0 and s_t["iterations"] == s_a["iterations"]
+            assert s_t["omega"] == s_a["omega"] and s_t["Pressure"] == s_a["Pressure"]
+    # warm starts: later steps need fewer iterations than the cold first step
+    for b in range(len(br)):
+        assert together[b][-1]["iterations"] < together[b][0]["iterations"]
+
+
+def test_sweep_grand_potential_matches_oracle():
+    ds = _branches()[0]
+    num = numerics_from_dict(ds["numerical"])
+    data = copy.deepcopy(ds)
+    bulk = iLST(data)
+    prev = None
+    for H in DIST:
+        ct.set_distance(data, H, 0.05)
+        geom = geometry_system(data)
+        dft = setup_iDFT(data, bulk, geom)
+        o = OracleSystem(dft.descriptor)
+        if prev is not None:
+            dft.state = ct.resample_state(prev[0], prev[1], geom)
+            o.set_x(dft.handle().get_x())
+        it_o, _, rc_o, _ = o.solve(num, 0)
+        it_d, err_d, rc_d = dft.handle().solve(num)
+        assert rc_o == 0 and rc_d == 0
+        om_d, om_o = dft.handle().grand_potential(), o.grand_potential()
+        assert abs(om_d - om_o) <= 1e-8 * abs(om_o)
+        prev = (dft.state, geom)
+        dft.handle().close()
+
+
+def test_adjust_pH_sweep_writes_the_routine_files(tmp_path):
+    ds = workloads.grafted_brush(128, 0.05, 8, 0.05, 4.5, 5.0, 0.01)
+    ds["numerical"] = dict(ds["numerical"], max_iters=8000)
+    res = ct.adjust_pH(ds, startZ=5.0, stopZ=6.0, stepZ=0.5, out_root=str(tmp_path / "pH_sweep"))
+    assert [r["step"] for r in res] == [1, 2, 3] and all(r["status"] == 0 for r in res)
+    alphas = [r["alpha"] for r in res]
+    assert alphas[0] < alphas[1] < alphas[2]          # ionisation grows with pH
+    assert all(r["brush_height"] > 0 for r in res)
+    lines = open(tmp_path / "pH_sweep" / "summary_brush_alpha.csv").read().splitlines()
+    assert lines[0] == "step,pH,brush_height,alpha" and len(lines) == 4
+    for name in ("cvt.txt", "grand_potential.txt", "brush_height.txt", "MEP.txt", "rho_beads_K.txt"):
+        assert (tmp_path / "pH_sweep" / "pH_5.50" / name).is_file(), name
