@@ -5,7 +5,8 @@ One step = solving one batch of B independent requests to convergence in one
 device launch sequence (one persistent CTA per request).  The default
 workload is the plain slit request (NP=1024, dz=0.02, N=20 weak-polyacid
 chain pKa 4.5 at pH 7, 1:1 salt 0.1 M, hard-sphere solvent, packing 0.3, hard
-walls, Anderson m=5) in FP64; B defaults to two requests per SM.
+walls, Anderson m=5) in FP64; B defaults to three requests per SM (the solve
+kernel's occupancy).
 
   value      device-timed solves/s over all ranks (CUDA events on the launch
              stream, inputs resident, max time over ranks)
@@ -49,7 +50,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=0, help="requests per GPU (0: two per SM)")
+    ap.add_argument("--batch", type=int, default=0, help="requests per GPU (0: three per SM)")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -306,7 +307,7 @@ def run_ours(args, ws, rank, local):
     num = numerics_from_dict(ds["numerical"])
     import torch
     sms = torch.cuda.get_device_properties(local if ws > 1 else 0).multi_processor_count
-    B = args.batch if args.batch > 0 else 2 * sms
+    B = args.batch if args.batch > 0 else 3 * sms  # the solve kernel keeps three CTAs per SM
     systems = [native.DeviceSystem(dft.descriptor) for _ in range(B)]
     x0 = systems[0].get_x()
     n = x0.size

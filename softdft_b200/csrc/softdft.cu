@@ -60,7 +60,7 @@ extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_objective(const DR
   if (threadIdx.x == 0) *r.status = ok ? ST_OK : ST_NORM;
 }
 
-extern "C" __global__ void __launch_bounds__(kThreads, 2) sdft_k_solve(const DReq* reqs, SolveSlot* slots, SolveCfg cfg,
+extern "C" __global__ void __launch_bounds__(kThreads, 3) sdft_k_solve(const DReq* reqs, SolveSlot* slots, SolveCfg cfg,
                                                                     int max_chunk) {
   extern __shared__ double smem[];
   const DReq& r = reqs[blockIdx.x];
