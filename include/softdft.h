@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define SDFT_ABI_VERSION 1
+#define SDFT_ABI_VERSION 2
 
 typedef enum sdft_status {
   SDFT_OK = 0,
@@ -110,6 +110,9 @@ typedef struct sdft_numerics {
   double mixing_max;             /* default 1.0 */
   double switch_tole;            /* default 1e-3 */
   double tole;                   /* default 1e-6 */
+  double mixed_switch;           /* SDFT_PREC_MIXED requests evaluate with FP32 propagators while
+                                    the residual is above this, then in FP64 (0: the default 1e-2;
+                                    never below 10 * tole).  No reference counterpart. */
 } sdft_numerics;
 
 typedef struct sdft_request* sdft_handle;

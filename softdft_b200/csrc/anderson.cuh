@@ -21,6 +21,7 @@ struct SolveCfg {
   int max_iters;
   int anderm;
   double damping, mixing_max, switch_tole, tole;
+  double mixed_switch;  // residual below which a mixed-precision request evaluates in FP64
 };
 
 struct AndersonState {

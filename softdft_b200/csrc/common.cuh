@@ -65,6 +65,7 @@ struct DReq {
   int funcs;          // SDFT_FUNC_* bits
   int TB;             // transform buffers in shared memory for this launch (1..kMaxTB)
   int ngrp;           // distinct bead diameters
+  int prec;           // 0: FP64; 1: FP32 propagators while the residual is above the switch
   double dz, lB, total_charge;
   long long n;        // Anderson unknowns
   // per-bead / per-bond constants
@@ -88,6 +89,9 @@ struct DReq {
   const double2* tw;      // [M/2] e^{-2 pi i k / M}
   const double2* twP;     // [M+1] e^{-2 pi i k / P}
   const double2* twD;     // [M+1] e^{-i pi k / (2P)}
+  const float2* tw32;     // FP32 copies of tw, twP, twD (mixed precision)
+  const float2* twP32;
+  const float2* twD32;
   // state
   double* x;              // [n] unknowns
   double* g;              // [n] G(x) of the last evaluation
@@ -103,6 +107,7 @@ struct DReq {
   double* wc;             // [max(NB, 6 + MB) * P] scratch (derivative fields)
   double* wd;             // [2 * NB * P] scratch (per-bead FMT weighted densities)
   double* elam;           // [NB * P] e^{-lambda} of the current x
+  float* fbe32;           // [4 * MB * P] FP32 copy of fbe (mixed precision)
   double* fbe;            // [4 * MB * P] bond-end factors of the current x: e^{-lambda_j + lng/2} trapez_j, then e^{lng/2}
   // Anderson
   double* hx;             // [m * n] history of x
@@ -125,6 +130,29 @@ __device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -
 __device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 scl2(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// the same for FP32 complex values (mixed-precision propagators)
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 conj2(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 scl2(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// real type and constructor of a complex type
+template <class C>
+struct Cx;
+template <>
+struct Cx<double2> {
+  using R = double;
+  static __device__ __forceinline__ double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <>
+struct Cx<float2> {
+  using R = float;
+  static __device__ __forceinline__ float2 make(float x, float y) { return make_float2(x, y); }
+};
 
 // ---------------------------------------------------------------------------
 // CTA reductions (warp shuffles + one shared slot per warp)

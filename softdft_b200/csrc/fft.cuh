@@ -38,14 +38,17 @@ __device__ __forceinline__ int brev_bits(int m, int L) {
   return L == 0 ? 0 : (int)(__brev((unsigned)m) >> (32 - L));
 }
 
-struct FftCtx {
-  double2* z;        // TB buffers of `stride` slots
+// C = double2 (FP64) or float2 (the mixed-precision propagator convolutions)
+template <class C>
+struct FftCtxT {
+  C* z;              // TB buffers of `stride` slots
   int stride;        // M + M/8
   int P, M, L, H;    // H = M/2
-  const double2* __restrict__ tw;   // [M/2] e^{-2 pi i k / M}
-  const double2* __restrict__ twP;  // [M+1] e^{-2 pi i k / P}
-  const double2* __restrict__ twD;  // [M+1] e^{-i pi k / 2P}
+  const C* __restrict__ tw;   // [M/2] e^{-2 pi i k / M}
+  const C* __restrict__ twP;  // [M+1] e^{-2 pi i k / P}
+  const C* __restrict__ twD;  // [M+1] e^{-i pi k / 2P}
 };
+using FftCtx = FftCtxT<double2>;
 
 __device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
   FftCtx c;
@@ -58,6 +61,21 @@ __device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
   c.tw = r.tw;
   c.twP = r.twP;
   c.twD = r.twD;
+  return c;
+}
+
+// FP32 transform buffers over the same shared memory
+__device__ __forceinline__ FftCtxT<float2> make_fft32(double2* z, const DReq& r) {
+  FftCtxT<float2> c;
+  c.z = reinterpret_cast<float2*>(z);
+  c.M = r.M;
+  c.L = r.L;
+  c.P = r.NP;
+  c.H = r.M >> 1;
+  c.stride = r.M + (r.M >> 3);
+  c.tw = r.tw32;
+  c.twP = r.twP32;
+  c.twD = r.twD32;
   return c;
 }
 
@@ -96,28 +114,34 @@ __device__ __forceinline__ void store_b(const FftCtx& c, int nT, double scale, S
 // of a thread handles two pairs whose global loads are issued first.
 __device__ __forceinline__ double2 ldcg2(const double* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
 __device__ __forceinline__ void stcg2(double* p, double2 v) { __stcg(reinterpret_cast<double2*>(p), v); }
+__device__ __forceinline__ float2 ldcg2(const float* p) { return __ldcg(reinterpret_cast<const float2*>(p)); }
+__device__ __forceinline__ void stcg2(float* p, float2 v) { __stcg(reinterpret_cast<float2*>(p), v); }
 
-__device__ __forceinline__ void put_pair(const FftCtx& c, int t, int kp, double2 v) {
-  double* zb = reinterpret_cast<double*>(c.z + (size_t)t * c.stride);
+template <class C, class V>
+__device__ __forceinline__ void put_pair(const FftCtxT<C>& c, int t, int kp, V v) {
+  using R = typename Cx<C>::R;
+  R* zb = reinterpret_cast<R*>(c.z + (size_t)t * c.stride);
   const int q1 = c.P - 1 - kp;
-  zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)] = v.x;
-  zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)] = v.y;
+  zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)] = (R)v.x;
+  zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)] = (R)v.y;
 }
-__device__ __forceinline__ double2 get_pair(const FftCtx& c, int t, int kp) {
-  const double* zb = reinterpret_cast<const double*>(c.z + (size_t)t * c.stride);
+template <class C>
+__device__ __forceinline__ C get_pair(const FftCtxT<C>& c, int t, int kp) {
+  using R = typename Cx<C>::R;
+  const R* zb = reinterpret_cast<const R*>(c.z + (size_t)t * c.stride);
   const int q1 = c.P - 1 - kp;
-  return make_double2(zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)], zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)]);
+  return Cx<C>::make(zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)], zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)]);
 }
 
 // f2(t, K) -> (f(K), f(K+1)) for even K
-template <class F2>
-__device__ __forceinline__ void load_b2(const FftCtx& c, int nT, F2 f2) {
+template <class C, class F2>
+__device__ __forceinline__ void load_b2(const FftCtxT<C>& c, int nT, F2 f2) {
   const int lm = c.L;
   const int total = nT << lm;
   for (int b0 = threadIdx.x; b0 < total; b0 += 2 * blockDim.x) {
     const int i1 = b0 + blockDim.x;
-    const double2 v0 = f2(b0 >> lm, (b0 & (c.M - 1)) << 1);
-    double2 v1 = make_double2(0.0, 0.0);
+    const auto v0 = f2(b0 >> lm, (b0 & (c.M - 1)) << 1);
+    auto v1 = v0;
     if (i1 < total) v1 = f2(i1 >> lm, (i1 & (c.M - 1)) << 1);
     put_pair(c, b0 >> lm, b0 & (c.M - 1), v0);
     if (i1 < total) put_pair(c, i1 >> lm, i1 & (c.M - 1), v1);
@@ -125,16 +149,17 @@ __device__ __forceinline__ void load_b2(const FftCtx& c, int nT, F2 f2) {
 }
 
 // put2(t, K, (y_K, y_K+1) * scale, pre2(t, K)) for even K; pre2 holds the loads
-template <class A2, class S2>
-__device__ __forceinline__ void store_b2(const FftCtx& c, int nT, double scale, A2 pre2, S2 put2) {
+template <class C, class A2, class S2>
+__device__ __forceinline__ void store_b2(const FftCtxT<C>& c, int nT, typename Cx<C>::R scale, A2 pre2, S2 put2) {
   const int lm = c.L;
   const int total = nT << lm;
   for (int b0 = threadIdx.x; b0 < total; b0 += 2 * blockDim.x) {
     const int i1 = b0 + blockDim.x;
     const int t0 = b0 >> lm, K0 = (b0 & (c.M - 1)) << 1;
-    double2 y0 = get_pair(c, t0, K0 >> 1);
-    const double2 a0 = pre2(t0, K0);
-    double2 y1 = make_double2(0.0, 0.0), a1 = y1;
+    C y0 = get_pair(c, t0, K0 >> 1);
+    const auto a0 = pre2(t0, K0);
+    C y1 = y0;
+    auto a1 = a0;
     const int t1 = i1 >> lm, K1 = (i1 & (c.M - 1)) << 1;
     if (i1 < total) {
       y1 = get_pair(c, t1, K1 >> 1);
@@ -151,19 +176,22 @@ __device__ __forceinline__ void store_b2(const FftCtx& c, int nT, double scale, 
   }
 }
 
-__device__ __forceinline__ void bfly(double2& a, double2& b, double2 w) {  // DIT: (a + wb, a - wb)
-  const double2 wb = cmul(b, w);
+template <class C>
+__device__ __forceinline__ void bfly(C& a, C& b, C w) {  // DIT: (a + wb, a - wb)
+  const C wb = cmul(b, w);
   b = sub2(a, wb);
   a = add2(a, wb);
 }
-__device__ __forceinline__ void bfly_dif(double2& a, double2& b, double2 w) {  // DIF: (a + b, (a - b) w)
-  const double2 d = sub2(a, b);
+template <class C>
+__device__ __forceinline__ void bfly_dif(C& a, C& b, C w) {  // DIF: (a + b, (a - b) w)
+  const C d = sub2(a, b);
   a = add2(a, b);
   b = cmul(d, w);
 }
 
 // forward FFT of nT buffers: bit-reversed input -> natural output
-__device__ __forceinline__ void fft_fwd_b(const FftCtx& c, int nT) {
+template <class C>
+__device__ __forceinline__ void fft_fwd_b(const FftCtxT<C>& c, int nT) {
   const int M = c.M, L = c.L;
   for (int s = 0; s < L;) {
     const int rr = min(3, L - s);
@@ -173,17 +201,17 @@ __device__ __forceinline__ void fft_fwd_b(const FftCtx& c, int nT) {
       const int per = M >> 3, lper = L - 3;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        double2* zb = c.z + (size_t)t * c.stride;
+        C* zb = c.z + (size_t)t * c.stride;
         const int p = u & (h - 1);
         const int base = ((u >> s) << (s + 3)) + p;
-        double2 x[8];
+        C x[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) x[j] = zb[fpad(base + j * h)];
-        const double2 w1 = __ldg(&c.tw[p << (L - 1 - s)]);
+        const C w1 = __ldg(&c.tw[p << (L - 1 - s)]);
 #pragma unroll
         for (int m = 0; m < 4; m++) bfly(x[2 * m], x[2 * m + 1], w1);
-        const double2 w2a = __ldg(&c.tw[p << (L - 2 - s)]);
-        const double2 w2b = __ldg(&c.tw[(p + h) << (L - 2 - s)]);
+        const C w2a = __ldg(&c.tw[p << (L - 2 - s)]);
+        const C w2b = __ldg(&c.tw[(p + h) << (L - 2 - s)]);
         bfly(x[0], x[2], w2a);
         bfly(x[1], x[3], w2b);
         bfly(x[4], x[6], w2a);
@@ -197,13 +225,13 @@ __device__ __forceinline__ void fft_fwd_b(const FftCtx& c, int nT) {
       const int per = M >> 2, lper = L - 2;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        double2* zb = c.z + (size_t)t * c.stride;
+        C* zb = c.z + (size_t)t * c.stride;
         const int p = u & (h - 1);
         const int base = ((u >> s) << (s + 2)) + p;
-        double2 x[4];
+        C x[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) x[j] = zb[fpad(base + j * h)];
-        const double2 w1 = __ldg(&c.tw[p << (L - 1 - s)]);
+        const C w1 = __ldg(&c.tw[p << (L - 1 - s)]);
         bfly(x[0], x[1], w1);
         bfly(x[2], x[3], w1);
         bfly(x[0], x[2], __ldg(&c.tw[p << (L - 2 - s)]));
@@ -215,10 +243,10 @@ __device__ __forceinline__ void fft_fwd_b(const FftCtx& c, int nT) {
       const int per = M >> 1, lper = L - 1;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        double2* zb = c.z + (size_t)t * c.stride;
+        C* zb = c.z + (size_t)t * c.stride;
         const int p = u & (h - 1);
         const int base = ((u >> s) << (s + 1)) + p;
-        double2 a = zb[fpad(base)], b = zb[fpad(base + h)];
+        C a = zb[fpad(base)], b = zb[fpad(base + h)];
         bfly(a, b, __ldg(&c.tw[p << (L - 1 - s)]));
         zb[fpad(base)] = a;
         zb[fpad(base + h)] = b;
@@ -230,7 +258,8 @@ __device__ __forceinline__ void fft_fwd_b(const FftCtx& c, int nT) {
 }
 
 // inverse FFT of nT buffers (unscaled): natural input -> bit-reversed output
-__device__ __forceinline__ void fft_inv_b(const FftCtx& c, int nT) {
+template <class C>
+__device__ __forceinline__ void fft_inv_b(const FftCtxT<C>& c, int nT) {
   const int M = c.M, L = c.L;
   for (int top = L; top > 0;) {
     const int rr = min(3, top);
@@ -241,21 +270,21 @@ __device__ __forceinline__ void fft_inv_b(const FftCtx& c, int nT) {
       const int per = M >> 3, lper = L - 3;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        double2* zb = c.z + (size_t)t * c.stride;
+        C* zb = c.z + (size_t)t * c.stride;
         const int p = u & (h - 1);
         const int base = ((u >> s0) << (s0 + 3)) + p;
-        double2 x[8];
+        C x[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) x[j] = zb[fpad(base + j * h)];
 #pragma unroll
         for (int j = 0; j < 4; j++) bfly_dif(x[j], x[j + 4], conj2(__ldg(&c.tw[(p + j * h) << (L - 3 - s0)])));
-        const double2 w2a = conj2(__ldg(&c.tw[p << (L - 2 - s0)]));
-        const double2 w2b = conj2(__ldg(&c.tw[(p + h) << (L - 2 - s0)]));
+        const C w2a = conj2(__ldg(&c.tw[p << (L - 2 - s0)]));
+        const C w2b = conj2(__ldg(&c.tw[(p + h) << (L - 2 - s0)]));
         bfly_dif(x[0], x[2], w2a);
         bfly_dif(x[1], x[3], w2b);
         bfly_dif(x[4], x[6], w2a);
         bfly_dif(x[5], x[7], w2b);
-        const double2 w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
+        const C w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
 #pragma unroll
         for (int m = 0; m < 4; m++) bfly_dif(x[2 * m], x[2 * m + 1], w1);
 #pragma unroll
@@ -265,15 +294,15 @@ __device__ __forceinline__ void fft_inv_b(const FftCtx& c, int nT) {
       const int per = M >> 2, lper = L - 2;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        double2* zb = c.z + (size_t)t * c.stride;
+        C* zb = c.z + (size_t)t * c.stride;
         const int p = u & (h - 1);
         const int base = ((u >> s0) << (s0 + 2)) + p;
-        double2 x[4];
+        C x[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) x[j] = zb[fpad(base + j * h)];
         bfly_dif(x[0], x[2], conj2(__ldg(&c.tw[p << (L - 2 - s0)])));
         bfly_dif(x[1], x[3], conj2(__ldg(&c.tw[(p + h) << (L - 2 - s0)])));
-        const double2 w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
+        const C w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
         bfly_dif(x[0], x[1], w1);
         bfly_dif(x[2], x[3], w1);
 #pragma unroll
@@ -283,10 +312,10 @@ __device__ __forceinline__ void fft_inv_b(const FftCtx& c, int nT) {
       const int per = M >> 1, lper = L - 1;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        double2* zb = c.z + (size_t)t * c.stride;
+        C* zb = c.z + (size_t)t * c.stride;
         const int p = u & (h - 1);
         const int base = ((u >> s0) << (s0 + 1)) + p;
-        double2 a = zb[fpad(base)], b = zb[fpad(base + h)];
+        C a = zb[fpad(base)], b = zb[fpad(base + h)];
         bfly_dif(a, b, conj2(__ldg(&c.tw[p << (L - 1 - s0)])));
         zb[fpad(base)] = a;
         zb[fpad(base + h)] = b;
@@ -300,20 +329,25 @@ __device__ __forceinline__ void fft_inv_b(const FftCtx& c, int nT) {
 // ---- pair step ------------------------------------------------------------
 // From Z[k], Z[M-k] (natural order, after the forward FFT) to the four DCT-II
 // coefficients C[k], C[P-k], C[M-k], C[M+k] (0 < k < M/2).
-struct Quad {
-  double c0, c1, c2, c3;  // indices k, P-k, M-k, M+k
+template <class R>
+struct QuadT {
+  R c0, c1, c2, c3;  // indices k, P-k, M-k, M+k
 };
+using Quad = QuadT<double>;
 
-__device__ __forceinline__ Quad pair_forward(double2 A, double2 B, double2 wk, double2 dk, double2 dk2) {
-  double2 Ze = scl2(add2(A, conj2(B)), 0.5);
-  double2 D = sub2(A, conj2(B));
-  double2 Zo = make_double2(0.5 * D.y, -0.5 * D.x);  // -i D / 2
-  double2 wZo = cmul(wk, Zo);
-  double2 Vk = add2(Ze, wZo);
-  double2 Vk2 = conj2(sub2(Ze, wZo));
-  double2 tk = cmul(dk, Vk);
-  double2 tk2 = cmul(dk2, Vk2);
-  Quad q;
+template <class C>
+__device__ __forceinline__ QuadT<typename Cx<C>::R> pair_forward(C A, C B, C wk, C dk, C dk2) {
+  using R = typename Cx<C>::R;
+  const R half = (R)0.5;
+  C Ze = scl2(add2(A, conj2(B)), half);
+  C D = sub2(A, conj2(B));
+  C Zo = Cx<C>::make(half * D.y, -half * D.x);  // -i D / 2
+  C wZo = cmul(wk, Zo);
+  C Vk = add2(Ze, wZo);
+  C Vk2 = conj2(sub2(Ze, wZo));
+  C tk = cmul(dk, Vk);
+  C tk2 = cmul(dk2, Vk2);
+  QuadT<R> q;
   q.c0 = tk.x;
   q.c1 = -tk.y;
   q.c2 = tk2.x;
@@ -322,37 +356,45 @@ __device__ __forceinline__ Quad pair_forward(double2 A, double2 B, double2 wk, d
 }
 
 // inverse of pair_forward: coefficients E[k], E[P-k], E[M-k], E[M+k] -> Z'[k], Z'[M-k]
-__device__ __forceinline__ void pair_inverse(const Quad& e, double2 wk, double2 dk, double2 dk2, double2* Zk,
-                                             double2* Zk2) {
-  double2 Vk = cmul(conj2(dk), make_double2(e.c0, -e.c1));
-  double2 Vk2 = cmul(conj2(dk2), make_double2(e.c2, -e.c3));
-  double2 Ze = scl2(add2(Vk, conj2(Vk2)), 0.5);
-  double2 Zo = scl2(cmul(sub2(Vk, conj2(Vk2)), conj2(wk)), 0.5);
-  *Zk = make_double2(Ze.x - Zo.y, Ze.y + Zo.x);
-  *Zk2 = make_double2(Ze.x + Zo.y, -Ze.y + Zo.x);
+template <class C>
+__device__ __forceinline__ void pair_inverse(const QuadT<typename Cx<C>::R>& e, C wk, C dk, C dk2, C* Zk, C* Zk2) {
+  using R = typename Cx<C>::R;
+  const R half = (R)0.5;
+  C Vk = cmul(conj2(dk), Cx<C>::make(e.c0, -e.c1));
+  C Vk2 = cmul(conj2(dk2), Cx<C>::make(e.c2, -e.c3));
+  C Ze = scl2(add2(Vk, conj2(Vk2)), half);
+  C Zo = scl2(cmul(sub2(Vk, conj2(Vk2)), conj2(wk)), half);
+  *Zk = Cx<C>::make(Ze.x - Zo.y, Ze.y + Zo.x);
+  *Zk2 = Cx<C>::make(Ze.x + Zo.y, -Ze.y + Zo.x);
 }
 
 // k = 0: C[0] and C[M] (C[P] does not exist)
-__device__ __forceinline__ void zero_forward(double2 A, double2 dM, double* c0, double* cM) {
-  double V0 = A.x + A.y;
-  double VM = A.x - A.y;
+template <class C, class R>
+__device__ __forceinline__ void zero_forward(C A, C dM, R* c0, R* cM) {
+  R V0 = A.x + A.y;
+  R VM = A.x - A.y;
   *c0 = V0;
   *cM = VM * dM.x;
 }
-__device__ __forceinline__ double2 zero_inverse(double e0, double eM, double2 dM) {
-  double2 VM = cmul(conj2(dM), make_double2(eM, -eM));
-  double2 Ze = scl2(add2(make_double2(e0, 0.0), conj2(VM)), 0.5);
-  double2 Zo = scl2(sub2(make_double2(e0, 0.0), conj2(VM)), 0.5);
-  return make_double2(Ze.x - Zo.y, Ze.y + Zo.x);
+template <class C>
+__device__ __forceinline__ C zero_inverse(typename Cx<C>::R e0, typename Cx<C>::R eM, C dM) {
+  using R = typename Cx<C>::R;
+  const R half = (R)0.5;
+  C VM = cmul(conj2(dM), Cx<C>::make(eM, -eM));
+  C Ze = scl2(add2(Cx<C>::make(e0, (R)0), conj2(VM)), half);
+  C Zo = scl2(sub2(Cx<C>::make(e0, (R)0), conj2(VM)), half);
+  return Cx<C>::make(Ze.x - Zo.y, Ze.y + Zo.x);
 }
 // k = M/2: C[M/2], C[P-M/2]
-__device__ __forceinline__ void mid_forward(double2 A, double2 dh, double* ch, double* cPh) {
-  double2 t = cmul(dh, conj2(A));
+template <class C, class R>
+__device__ __forceinline__ void mid_forward(C A, C dh, R* ch, R* cPh) {
+  C t = cmul(dh, conj2(A));
   *ch = t.x;
   *cPh = -t.y;
 }
-__device__ __forceinline__ double2 mid_inverse(double eh, double ePh, double2 dh) {
-  double2 V = cmul(conj2(dh), make_double2(eh, -ePh));
+template <class C>
+__device__ __forceinline__ C mid_inverse(typename Cx<C>::R eh, typename Cx<C>::R ePh, C dh) {
+  C V = cmul(conj2(dh), Cx<C>::make(eh, -ePh));
   return conj2(V);
 }
 
@@ -361,7 +403,7 @@ __device__ __forceinline__ double2 mid_inverse(double eh, double ePh, double2 dh
   const int lH_ = (c).L - 1;                                            \
   for (int it = threadIdx.x; it < ((nT) << lH_); it += blockDim.x) {   \
     const int t = it >> lH_, k = it & ((c).H - 1);                      \
-    double2* zb = (c).z + (size_t)t * (c).stride;
+    auto* zb = (c).z + (size_t)t * (c).stride;
 
 // ---- whole transforms ------------------------------------------------------
 
@@ -454,38 +496,40 @@ store_b(c, nT, 1.0 / (double)M, store);
 __syncthreads();
 }
 
-// the same convolution with grid-point pair functors (load_b2 / store_b2)
-template <class F2, class W, class A2, class S2>
-__device__ __forceinline__ void dct2_convolve_b2(const FftCtx& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
+// the same convolution with grid-point pair functors (load_b2 / store_b2), in
+// the precision of the context (FP64, or FP32 for mixed-precision propagators)
+template <class C, class F2, class W, class A2, class S2>
+__device__ __forceinline__ void dct2_convolve_b2(const FftCtxT<C>& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
+  using R = typename Cx<C>::R;
   const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
   load_b2(c, nT, f2);
   fft_fwd_b(c, nT);
   SDFT_PAIR_LOOP(c, nT)
   if (k == 0) {
-    const double2 dM = __ldg(&c.twD[M]);
-    double c0, cM;
+    const C dM = __ldg(&c.twD[M]);
+    R c0, cM;
     zero_forward(zb[0], dM, &c0, &cM);
-    const double2 dh = __ldg(&c.twD[H]);
-    double ch, cPh;
+    const C dh = __ldg(&c.twD[H]);
+    R ch, cPh;
     mid_forward(zb[fpad(H)], dh, &ch, &cPh);
-    zb[0] = zero_inverse(c0 * wgt(t, 0), cM * wgt(t, M), dM);
-    zb[fpad(H)] = mid_inverse(ch * wgt(t, H), cPh * wgt(t, P - H), dh);
+    zb[0] = zero_inverse(c0 * (R)wgt(t, 0), cM * (R)wgt(t, M), dM);
+    zb[fpad(H)] = mid_inverse(ch * (R)wgt(t, H), cPh * (R)wgt(t, P - H), dh);
   } else {
-    const double2 wk = __ldg(&c.twP[k]), dk = __ldg(&c.twD[k]), dk2 = __ldg(&c.twD[M - k]);
-    Quad q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], wk, dk, dk2);
-    q.c0 *= wgt(t, k);
-    q.c1 *= wgt(t, P - k);
-    q.c2 *= wgt(t, M - k);
-    q.c3 *= wgt(t, M + k);
-    double2 a, b;
+    const C wk = __ldg(&c.twP[k]), dk = __ldg(&c.twD[k]), dk2 = __ldg(&c.twD[M - k]);
+    QuadT<R> q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], wk, dk, dk2);
+    q.c0 *= (R)wgt(t, k);
+    q.c1 *= (R)wgt(t, P - k);
+    q.c2 *= (R)wgt(t, M - k);
+    q.c3 *= (R)wgt(t, M + k);
+    C a, b;
     pair_inverse(q, wk, dk, dk2, &a, &b);
     zb[fpad(k)] = a;
     zb[fpad(M - k)] = b;
   }
 }
 fft_inv_b(c, nT);
-store_b2(c, nT, 1.0 / (double)M, pre2, put2);
+store_b2(c, nT, (R)1 / (R)M, pre2, put2);
 __syncthreads();
 }
 

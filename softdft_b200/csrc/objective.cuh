@@ -60,17 +60,34 @@ __device__ void stage_lambda(const DReq& r) {
 //          convolution towards the bead at this end, child_propagators.jl:118-133)
 //   Fout = e^{lng_{b,e}/2}                          (the output factor at this end)
 // computed once per evaluation instead of once per (segment, state pair).
-__device__ void stage_bond_factors(const DReq& r) {
+// In an FP32 evaluation the input factors are also written as floats, all
+// divided by one power of two 2^sc that brings their maximum below 1 (e^{-lambda}
+// can exceed the float range far from the solution); sc goes to scal[1] and
+// every convolution step adds it to the carried propagator exponent.
+__device__ void stage_bond_factors(const DReq& r, Shared sh, bool fp32) {
   const int P = r.NP, nbe = 2 * r.MB;
   const double* lng = xs_lng(r, r.x);
+  double mx = 0.0;
   for (int idx = threadIdx.x; idx < nbe * P; idx += blockDim.x) {
     const int be = idx / P, K = idx - be * P;
     const int j = r.bonds[be];
     const double l = lng[idx];
-    r.fbe[idx] = exp(-r.lambda[(size_t)j * P + K] + l / 2.0) * r.trapez[(size_t)j * P + K];
+    const double fin = exp(-r.lambda[(size_t)j * P + K] + l / 2.0) * r.trapez[(size_t)j * P + K];
+    r.fbe[idx] = fin;
     r.fbe[(size_t)nbe * P + idx] = exp(l / 2.0);
+    if (isfinite(fin)) mx = fmax(mx, fin);
   }
   for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) r.elam[idx] = exp(-r.lambda[idx]);
+  if (fp32 && r.fbe32) {
+    mx = block_max(mx, sh.red);
+    int sc = 0;
+    if (mx > 0.0) frexp(mx, &sc);
+    for (int idx = threadIdx.x; idx < nbe * P; idx += blockDim.x) {
+      r.fbe32[idx] = (float)ldexp(r.fbe[idx], -sc);
+      r.fbe32[(size_t)nbe * P + idx] = (float)r.fbe[(size_t)nbe * P + idx];
+    }
+    if (threadIdx.x == 0) r.scal[1] = (double)sc;
+  }
   __syncthreads();
 }
 
@@ -84,13 +101,35 @@ __device__ void stage_bond_factors(const DReq& r) {
 // 2^e that brings the maximum into [0.5, 1) -- an exact scaling -- and e is
 // carried (expo); otherwise e = 0 and the arithmetic is the reference's.
 // ---------------------------------------------------------------------------
-__device__ int renormalise_block(double* a, int count_per_K, int P, double* red) {
+// precision of the propagator stage: R = double (FP64) or float (mixed)
+template <class R>
+__device__ __forceinline__ FftCtxT<double2> fft_ctx_sel(double2* z, const DReq& r, double*) {
+  return make_fft(z, r);
+}
+template <class R>
+__device__ __forceinline__ FftCtxT<float2> fft_ctx_sel(double2* z, const DReq& r, float*) {
+  return make_fft32(z, r);
+}
+template <class R>
+__device__ __forceinline__ auto fft_ctx(double2* z, const DReq& r) {
+  return fft_ctx_sel<R>(z, r, (R*)nullptr);
+}
+__device__ __forceinline__ const double* bond_factors(const DReq& r, double*) { return r.fbe; }
+__device__ __forceinline__ const float* bond_factors(const DReq& r, float*) { return r.fbe32; }
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2((double)v.x, (double)v.y); }
+
+// fp32_bounds: the propagators feed FP32 convolutions (mixed precision) and
+// are kept in [2^-30, 2^30], so that the FP32 inputs (factors <= 1 times
+// propagator sums) stay far from the float range; FP64 keeps [2^-400, 2^400]
+__device__ int renormalise_block(double* a, int count_per_K, int P, double* red, bool fp32_bounds) {
+  const double lo = fp32_bounds ? 0x1p-30 : 0x1p-400, hi = fp32_bounds ? 0x1p30 : 0x1p400;
   double mx = 0.0;
   for (int K = threadIdx.x; K < P; K += blockDim.x)
     for (int q = 0; q < count_per_K; q++) mx = fmax(mx, fabs(a[(size_t)q * P + K]));
   mx = block_max(mx, red);
   if (!(mx > 0.0) || !isfinite(mx)) return 0;
-  if (mx >= 0x1p-400 && mx <= 0x1p400) return 0;
+  if (mx >= lo && mx <= hi) return 0;
   int e;
   frexp(mx, &e);
   for (int K = threadIdx.x; K < P; K += blockDim.x)
@@ -99,13 +138,17 @@ __device__ int renormalise_block(double* a, int count_per_K, int P, double* red)
   return e;
 }
 
+template <class R>
 __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
   const int P = r.NP, S = s.S, N = s.n_seg;
+  double* const gC = s.gC;
+  // FP32: the input factors are stored divided by 2^sc (stage_bond_factors)
+  const int sc = sizeof(R) == 4 ? (int)r.scal[1] : 0;
   bool scaled = false;
   int e_child = 0;  // exponent carried by gC of segment p + 1 (the leaf carries none)
   const double* lng = xs_lng(r, r.x);
   const double inv_norm = 1.0 / s.normative;
-  const FftCtx fc = make_fft(sh.z, r);
+  const auto fc = fft_ctx<R>(sh.z, r);
   for (int p = N - 2; p >= 0; p--) {
     const int c = p + 1;
     const int nc = s.nst[c];
@@ -116,12 +159,12 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
         const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
         const int bond = s.bnd[(p * S + ii) * S + jj];
         const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
-        double* out = s.gC + ((size_t)(p * S + ii) * S + jj) * P;
+        double* out = gC + ((size_t)(p * S + ii) * S + jj) * P;
         const double* lam_j = r.lambda + (size_t)sj * P;
         const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
         const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
         const double* tr_j = r.trapez + (size_t)sj * P;
-        const double* gcc = (c < N - 1) ? s.gC + ((size_t)(c * S + jj) * S) * P : nullptr;
+        const double* gcc = (c < N - 1) ? gC + ((size_t)(c * S + jj) * S) * P : nullptr;
         // parent grafted, child free: local sum within sigma_ij (child_propagators.jl:91-116)
         const int Kp = s.fixed;
         const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
@@ -144,15 +187,16 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
           }
         }
         acc = block_sum(acc, sh.red);
+        if (sc) acc = ldexp(acc, -sc);
         for (int K = threadIdx.x; K < P; K += blockDim.x) out[K] = (K == Kp) ? acc : 0.0;
       }
     } else {
-      const double* fin = r.fbe;
-      const double* fout = r.fbe + (size_t)2 * r.MB * P;
+      const R* fin = bond_factors(r, (R*)nullptr);
+      const R* fout = fin + (size_t)2 * r.MB * P;
       for (int g0 = 0; g0 < npair; g0 += r.TB) {
         const int nT = min(r.TB, npair - g0);
-        const double* in_t[kMaxTB];
-        const double* out_f[kMaxTB];
+        const R* in_t[kMaxTB];
+        const R* out_f[kMaxTB];
         const double* gcc_t[kMaxTB];
         const double* wb_t[kMaxTB];
         double* out_t[kMaxTB];
@@ -161,16 +205,17 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
           const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
           const int bond = s.bnd[(p * S + ii) * S + jj];
           const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
-          out_t[t] = s.gC + ((size_t)(p * S + ii) * S + jj) * P;
+          out_t[t] = gC + ((size_t)(p * S + ii) * S + jj) * P;
           in_t[t] = fin + (size_t)(bond * 2 + pair_j) * P;
           out_f[t] = fout + (size_t)(bond * 2 + pair_i) * P;
-          gcc_t[t] = (c < N - 1) ? s.gC + ((size_t)(c * S + jj) * S) * P : nullptr;
+          gcc_t[t] = (c < N - 1) ? gC + ((size_t)(c * S + jj) * S) * P : nullptr;
           wb_t[t] = r.Wbond + (size_t)bond * P;
         }
         dct2_convolve_b2(
             fc, nT,
             [&](int t, int K) {
-              double2 f = ldcg2(in_t[t] + K);
+              const auto fin = ldcg2(in_t[t] + K);
+              double2 f = make_double2(fin.x, fin.y);
               if (gcc_t[t]) {
                 double2 q2 = make_double2(0.0, 0.0);
                 for (int q = 0; q < S; q++) {
@@ -185,8 +230,9 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
             },
             [&](int t, int q) { return __ldg(&wb_t[t][q]); },
             [&](int t, int K) { return ldcg2(out_f[t] + K); },
-            [&](int t, int K, double2 y, double2 fo) {
-              stcg2(out_t[t] + K, make_double2(fabs(y.x) * fo.x * inv_norm, fabs(y.y) * fo.y * inv_norm));
+            [&](int t, int K, auto y, auto fo) {
+              stcg2(out_t[t] + K, make_double2(fabs((double)y.x) * (double)fo.x * inv_norm,
+                                               fabs((double)y.y) * (double)fo.y * inv_norm));
             });
       }
     }
@@ -195,12 +241,12 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
       __syncthreads();
       for (int K = threadIdx.x; K < P; K += blockDim.x)
         if (dist2_grid(K, s.fixed, r.dz) > md2)
-          for (int q = 0; q < S * S; q++) s.gC[((size_t)p * S * S + q) * P + K] = 0.0;
+          for (int q = 0; q < S * S; q++) gC[((size_t)p * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
-    const int e = renormalise_block(s.gC + (size_t)p * S * S * P, S * S, P, sh.red);
-    e_child += e;
-    scaled |= e != 0;
+    const int e = renormalise_block(gC + (size_t)p * S * S * P, S * S, P, sh.red, sizeof(R) == 4);
+    e_child += e + sc;
+    scaled |= (e + sc) != 0;
     if (threadIdx.x == 0) s.expo[p] = e_child;
   }
   if (threadIdx.x == 0) s.expo[N - 1] = 0;
@@ -208,8 +254,12 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
   return scaled;
 }
 
+template <class R>
 __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
   const int P = r.NP, S = s.S, N = s.n_seg;
+  double* const gP = s.gP;
+  // FP32: the input factors are stored divided by 2^sc (stage_bond_factors)
+  const int sc = sizeof(R) == 4 ? (int)r.scal[1] : 0;
   bool scaled = false;
   int e_parent = 0;  // exponent carried by gP of segment c - 1 (the root carries none)
   if (threadIdx.x == 0) s.expo[N] = 0;
@@ -221,18 +271,18 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
       for (int jj = 0; jj < S; jj++) {
         double v = 0.0;
         if (jj == 0 && ii < s.nst[0]) v = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
-        s.gP[((size_t)ii * S + jj) * P + K] = v;
+        gP[((size_t)ii * S + jj) * P + K] = v;
       }
   }
   __syncthreads();
-  const FftCtx fc = make_fft(sh.z, r);
+  const auto fc = fft_ctx<R>(sh.z, r);
   for (int c = 1; c < N; c++) {
     const int p = c - 1;
     // base case then the parent loop overwrites slot jj < nst[p]
     for (int K = threadIdx.x; K < P; K += blockDim.x)
       for (int ii = 0; ii < S; ii++)
         for (int jj = 0; jj < S; jj++)
-          s.gP[((size_t)(c * S + ii) * S + jj) * P + K] = (jj == 0 && ii < s.nst[c]) ? 1.0 : 0.0;
+          gP[((size_t)(c * S + ii) * S + jj) * P + K] = (jj == 0 && ii < s.nst[c]) ? 1.0 : 0.0;
     __syncthreads();
     const int np_ = s.nst[p];
     const int npair = s.nst[c] * np_;
@@ -242,10 +292,10 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
         const int si = s.states[c * S + ii], sj = s.states[p * S + jj];
         const int bond = s.bnd[(p * S + jj) * S + ii];
         const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
-        double* out = s.gP + ((size_t)(c * S + ii) * S + jj) * P;
+        double* out = gP + ((size_t)(c * S + ii) * S + jj) * P;
         const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
         const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
-        const double* gpp = s.gP + ((size_t)(p * S + jj) * S) * P;
+        const double* gpp = gP + ((size_t)(p * S + jj) * S) * P;
         // parent grafted (parent_propagators.jl:72-94)
         const int Kp = s.fixed;
         const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
@@ -259,18 +309,18 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
           if (d2 <= Dij2) {
             double v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm / s.normative;
             if (fabs(d2 - Dij2) <= 1e-6) v /= 2.0;
-            out[K1] = v;
+            out[K1] = sc ? ldexp(v, -sc) : v;
           }
         }
         __syncthreads();
       }
     } else {
-      const double* fin = r.fbe;
-      const double* fout = r.fbe + (size_t)2 * r.MB * P;
+      const R* fin = bond_factors(r, (R*)nullptr);
+      const R* fout = fin + (size_t)2 * r.MB * P;
       for (int g0 = 0; g0 < npair; g0 += r.TB) {
         const int nT = min(r.TB, npair - g0);
-        const double* in_t[kMaxTB];
-        const double* out_f[kMaxTB];
+        const R* in_t[kMaxTB];
+        const R* out_f[kMaxTB];
         const double* gpp_t[kMaxTB];
         const double* wb_t[kMaxTB];
         double* out_t[kMaxTB];
@@ -279,10 +329,10 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
           const int si = s.states[c * S + ii], sj = s.states[p * S + jj];
           const int bond = s.bnd[(p * S + jj) * S + ii];
           const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
-          out_t[t] = s.gP + ((size_t)(c * S + ii) * S + jj) * P;
+          out_t[t] = gP + ((size_t)(c * S + ii) * S + jj) * P;
           in_t[t] = fin + (size_t)(bond * 2 + pair_j) * P;
           out_f[t] = fout + (size_t)(bond * 2 + pair_i) * P;
-          gpp_t[t] = s.gP + ((size_t)(p * S + jj) * S) * P;
+          gpp_t[t] = gP + ((size_t)(p * S + jj) * S) * P;
           wb_t[t] = r.Wbond + (size_t)bond * P;
         }
         dct2_convolve_b2(
@@ -294,13 +344,14 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
                 q2.x += v.x;
                 q2.y += v.y;
               }
-              const double2 in = ldcg2(in_t[t] + K);
-              return make_double2(in.x * q2.x, in.y * q2.y);
+              const auto in = ldcg2(in_t[t] + K);
+              return make_double2((double)in.x * q2.x, (double)in.y * q2.y);
             },
             [&](int t, int q) { return __ldg(&wb_t[t][q]); },
             [&](int t, int K) { return ldcg2(out_f[t] + K); },
-            [&](int t, int K, double2 y, double2 fo) {
-              stcg2(out_t[t] + K, make_double2(fabs(y.x) * fo.x * inv_norm, fabs(y.y) * fo.y * inv_norm));
+            [&](int t, int K, auto y, auto fo) {
+              stcg2(out_t[t] + K, make_double2(fabs((double)y.x) * (double)fo.x * inv_norm,
+                                               fabs((double)y.y) * (double)fo.y * inv_norm));
             });
       }
     }
@@ -309,12 +360,12 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
       __syncthreads();
       for (int K = threadIdx.x; K < P; K += blockDim.x)
         if (dist2_grid(K, s.fixed, r.dz) > md2)
-          for (int q = 0; q < S * S; q++) s.gP[((size_t)c * S * S + q) * P + K] = 0.0;
+          for (int q = 0; q < S * S; q++) gP[((size_t)c * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
-    const int e = renormalise_block(s.gP + (size_t)c * S * S * P, S * S, P, sh.red);
-    e_parent += e;
-    scaled |= e != 0;
+    const int e = renormalise_block(gP + (size_t)c * S * S * P, S * S, P, sh.red, sizeof(R) == 4);
+    e_parent += e + sc;
+    scaled |= (e + sc) != 0;
     if (threadIdx.x == 0) s.expo[N + c] = e_parent;
   }
   __syncthreads();
@@ -322,8 +373,11 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
 }
 
 // handle_fixed (handle_fixed.jl:1-120): chain normalisation; false on lambda <= 0
+template <class R>
 __device__ bool chain_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_out) {
   const int P = r.NP, S = s.S, N = s.n_seg;
+  const R* gP = reinterpret_cast<const R*>(s.gP);
+  const R* gC = reinterpret_cast<const R*>(s.gC);
   double lam, norm;
   if (s.fixed >= 0) {
     norm = s.fixed_density;
@@ -334,12 +388,12 @@ __device__ bool chain_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_o
       for (int ii = 0; ii < s.nst[parent]; ii++) {
         const int si = s.states[parent * S + ii];
         double sp = 0.0;
-        for (int q = 0; q < S; q++) sp += s.gP[((size_t)(parent * S + ii) * S + q) * P + K];
+        for (int q = 0; q < S; q++) sp += gP[((size_t)(parent * S + ii) * S + q) * P + K];
         double contr = exp(-r.lambda[(size_t)si * P + K]) * sp;
         double temp;
         if (parent < N - 1) {
           temp = 0.0;
-          for (int jj = 0; jj < s.nst[parent + 1]; jj++) temp += s.gC[((size_t)(parent * S + ii) * S + jj) * P + K];
+          for (int jj = 0; jj < s.nst[parent + 1]; jj++) temp += gC[((size_t)(parent * S + ii) * S + jj) * P + K];
         } else {
           temp = (ii == 0) ? 1.0 : 0.0;  // leaf base case read as gC[K, :, idx_i, 1, parent]
         }
@@ -372,8 +426,11 @@ __device__ __forceinline__ double log_prefactor(const DSpecies& s, double norm, 
 }
 
 // accumulate_densities! for one species: rho_seg and both bond ends
+template <class R>
 __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, bool scaled) {
   const int P = r.NP, S = s.S, N = s.n_seg;
+  const R* gP = reinterpret_cast<const R*>(s.gP);
+  const R* gC = reinterpret_cast<const R*>(s.gC);
   const double mu = s.mu_species;
   for (int K = threadIdx.x; K < P; K += blockDim.x) {
     for (int g = 0; g < N; g++) {
@@ -383,7 +440,7 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, 
         double sp;
         if (N > 1) {
           sp = 0.0;
-          for (int q = 0; q < S; q++) sp += s.gP[((size_t)(g * S + ii) * S + q) * P + K];
+          for (int q = 0; q < S; q++) sp += gP[((size_t)(g * S + ii) * S + q) * P + K];
         } else {
           sp = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
         }
@@ -394,7 +451,7 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, 
           temp = 0.0;
           for (int jj = 0; jj < s.nst[g + 1]; jj++) {
             const int bond = s.bnd[(g * S + ii) * S + jj];
-            const double t2 = s.gC[((size_t)(g * S + ii) * S + jj) * P + K];
+            const double t2 = gC[((size_t)(g * S + ii) * S + jj) * P + K];
             r.rho_bonds[(size_t)(bond * 2 + 0) * P + K] += contr * t2;
             temp += t2;
           }
@@ -411,12 +468,12 @@ __device__ void chain_accumulate(const DReq& r, const DSpecies& s, double norm, 
         double contr = scaled ? exp(lp - r.lambda[(size_t)si * P + K]) : norm * exp(mu - r.lambda[(size_t)si * P + K]);
         if (c < N - 1) {
           double t = 0.0;
-          for (int q = 0; q < S; q++) t += s.gC[((size_t)(c * S + ii) * S + q) * P + K];
+          for (int q = 0; q < S; q++) t += gC[((size_t)(c * S + ii) * S + q) * P + K];
           contr *= t;
         }
         for (int jj = 0; jj < s.nst[c - 1]; jj++) {
           const int bond = s.bnd[((c - 1) * S + jj) * S + ii];
-          r.rho_bonds[(size_t)(bond * 2 + 1) * P + K] += contr * s.gP[((size_t)(c * S + ii) * S + jj) * P + K];
+          r.rho_bonds[(size_t)(bond * 2 + 1) * P + K] += contr * gP[((size_t)(c * S + ii) * S + jj) * P + K];
         }
       }
     }
@@ -441,9 +498,9 @@ __device__ __forceinline__ void acc_add(double* a, int idx, double v) {
 // e^{lp} e^{-lambda_K} with lp the log prefactor of the renormalised
 // propagators (e^{lp - lambda_K} directly when |lp| > 600).  Also adds the
 // species to the bead densities (update_spatial_structures.jl:1-34).
-template <int BR, int ER>
+template <int BR, int ER, class R>
 __device__ __noinline__ void accumulate_regs(const DReq& r, const DSpecies& s, double norm, bool scaled,
-                                             const double* __restrict__ gP, const double* __restrict__ gC,
+                                             const R* __restrict__ gP, const R* __restrict__ gC,
                                              const double* __restrict__ elam, const double* __restrict__ lam,
                                              const int* __restrict__ states, const int* __restrict__ nst,
                                              const int* __restrict__ bslot, const int* __restrict__ eslot,
@@ -539,12 +596,12 @@ struct AccStep {
   double2 el, p0, p1, c0, c1;
 };
 
-template <int BR, int ER>
+template <int BR, int ER, class R>
 __device__ __noinline__ void accumulate_pairs(const DReq& r, const DSpecies& s, double norm, bool scaled) {
   const int P = r.NP, S = s.S, N = s.n_seg;
   const double pref = norm * exp(s.mu_species);
-  const double* __restrict__ gP = s.gP;
-  const double* __restrict__ gC = s.gC;
+  const R* __restrict__ gP = reinterpret_cast<const R*>(s.gP);
+  const R* __restrict__ gC = reinterpret_cast<const R*>(s.gC);
   const double* __restrict__ elam = r.elam;
   const int* __restrict__ states = s.states;
   const int* __restrict__ nst = s.nst;
@@ -572,12 +629,12 @@ __device__ __noinline__ void accumulate_pairs(const DReq& r, const DSpecies& s, 
       const int si = states[g * S + ii];
       d.el = ldcg2(elam + (size_t)si * P + K);
       if (N > 1) {
-        d.p0 = ldcg2(gP + ((size_t)(g * S + ii) * S) * P + K);
-        if (S > 1) d.p1 = ldcg2(gP + ((size_t)(g * S + ii) * S + 1) * P + K);
+        d.p0 = to_d2(ldcg2(gP + ((size_t)(g * S + ii) * S) * P + K));
+        if (S > 1) d.p1 = to_d2(ldcg2(gP + ((size_t)(g * S + ii) * S + 1) * P + K));
       }
       const int nn = g < N - 1 ? nst[g + 1] : 0;
-      if (nn > 0) d.c0 = ldcg2(gC + ((size_t)(g * S + ii) * S) * P + K);
-      if (nn > 1) d.c1 = ldcg2(gC + ((size_t)(g * S + ii) * S + 1) * P + K);
+      if (nn > 0) d.c0 = to_d2(ldcg2(gC + ((size_t)(g * S + ii) * S) * P + K));
+      if (nn > 1) d.c1 = to_d2(ldcg2(gC + ((size_t)(g * S + ii) * S + 1) * P + K));
     };
     {
       int g = 0, ii = 0;
@@ -670,12 +727,12 @@ __device__ __noinline__ void accumulate_pairs(const DReq& r, const DSpecies& s, 
       const int si = states[c * S + ii];
       d.el = ldcg2(elam + (size_t)si * P + K);
       if (c < N - 1) {
-        d.c0 = ldcg2(gC + ((size_t)(c * S + ii) * S) * P + K);
-        if (S > 1) d.c1 = ldcg2(gC + ((size_t)(c * S + ii) * S + 1) * P + K);
+        d.c0 = to_d2(ldcg2(gC + ((size_t)(c * S + ii) * S) * P + K));
+        if (S > 1) d.c1 = to_d2(ldcg2(gC + ((size_t)(c * S + ii) * S + 1) * P + K));
       }
       const int np_ = nst[c - 1];
-      d.p0 = ldcg2(gP + ((size_t)(c * S + ii) * S) * P + K);
-      if (np_ > 1) d.p1 = ldcg2(gP + ((size_t)(c * S + ii) * S + 1) * P + K);
+      d.p0 = to_d2(ldcg2(gP + ((size_t)(c * S + ii) * S) * P + K));
+      if (np_ > 1) d.p1 = to_d2(ldcg2(gP + ((size_t)(c * S + ii) * S + 1) * P + K));
     };
     if (N > 1) {
       int c = 1, ii = 0;
@@ -758,6 +815,7 @@ __device__ __noinline__ void accumulate_pairs(const DReq& r, const DSpecies& s, 
 // rho_beads in place.  Per grid point the sums run over the steps in the
 // reference's order; two updates of one address are a whole grid sweep apart.
 // Chains with at most two states per segment.
+template <class R>
 __device__ __noinline__ void accumulate_stream(const DReq& r, const DSpecies& s, double norm, bool scaled) {
   const int P = r.NP, S = s.S, N = s.n_seg, P2 = P / 2;
   const double pref = norm * exp(s.mu_species);
@@ -774,8 +832,8 @@ __device__ __noinline__ void accumulate_stream(const DReq& r, const DSpecies& s,
     for (int ii = 0; ii < s.nst[g]; ii++) {
       const int si = s.states[g * S + ii];
       const double* el = r.elam + (size_t)si * P;
-      const double* gp = N > 1 ? s.gP + (size_t)(g * S + ii) * S * P : nullptr;
-      const double* gc = s.gC + (size_t)(g * S + ii) * S * P;
+      const R* gp = N > 1 ? reinterpret_cast<const R*>(s.gP) + (size_t)(g * S + ii) * S * P : nullptr;
+      const R* gc = reinterpret_cast<const R*>(s.gC) + (size_t)(g * S + ii) * S * P;
       double* rb0 = nn > 0 ? r.rho_bonds + (size_t)(s.bnd[(g * S + ii) * S] * 2) * P : nullptr;
       double* rb1 = nn > 1 ? r.rho_bonds + (size_t)(s.bnd[(g * S + ii) * S + 1] * 2) * P : nullptr;
       double* rs = s.rho_seg + (size_t)(g * S + ii) * P;
@@ -790,15 +848,15 @@ __device__ __noinline__ void accumulate_stream(const DReq& r, const DSpecies& s,
           if (K < P) {
             d[u].el = ldcg2(el + K);
             if (gp) {
-              d[u].p0 = ldcg2(gp + K);
-              if (S > 1) d[u].p1 = ldcg2(gp + P + K);
+              d[u].p0 = to_d2(ldcg2(gp + K));
+              if (S > 1) d[u].p1 = to_d2(ldcg2(gp + P + K));
             }
             if (nn > 0) {
-              d[u].c0 = ldcg2(gc + K);
+              d[u].c0 = to_d2(ldcg2(gc + K));
               o0[u] = ldcg2(rb0 + K);
             }
             if (nn > 1) {
-              d[u].c1 = ldcg2(gc + P + K);
+              d[u].c1 = to_d2(ldcg2(gc + P + K));
               o1[u] = ldcg2(rb1 + K);
             }
             ob[u] = ldcg2(rbd + K);
@@ -865,8 +923,8 @@ __device__ __noinline__ void accumulate_stream(const DReq& r, const DSpecies& s,
     for (int ii = 0; ii < s.nst[c]; ii++) {
       const int si = s.states[c * S + ii];
       const double* el = r.elam + (size_t)si * P;
-      const double* gc = c < N - 1 ? s.gC + (size_t)(c * S + ii) * S * P : nullptr;
-      const double* gp = s.gP + (size_t)(c * S + ii) * S * P;
+      const R* gc = c < N - 1 ? reinterpret_cast<const R*>(s.gC) + (size_t)(c * S + ii) * S * P : nullptr;
+      const R* gp = reinterpret_cast<const R*>(s.gP) + (size_t)(c * S + ii) * S * P;
       double* rb0 = r.rho_bonds + (size_t)(s.bnd[((c - 1) * S) * S + ii] * 2 + 1) * P;
       double* rb1 = np_ > 1 ? r.rho_bonds + (size_t)(s.bnd[((c - 1) * S + 1) * S + ii] * 2 + 1) * P : nullptr;
       for (int k0 = threadIdx.x; k0 < P2; k0 += 2 * bd) {
@@ -878,13 +936,13 @@ __device__ __noinline__ void accumulate_stream(const DReq& r, const DSpecies& s,
           if (K < P) {
             d[u].el = ldcg2(el + K);
             if (gc) {
-              d[u].c0 = ldcg2(gc + K);
-              if (S > 1) d[u].c1 = ldcg2(gc + P + K);
+              d[u].c0 = to_d2(ldcg2(gc + K));
+              if (S > 1) d[u].c1 = to_d2(ldcg2(gc + P + K));
             }
-            d[u].p0 = ldcg2(gp + K);
+            d[u].p0 = to_d2(ldcg2(gp + K));
             o0[u] = ldcg2(rb0 + K);
             if (np_ > 1) {
-              d[u].p1 = ldcg2(gp + P + K);
+              d[u].p1 = to_d2(ldcg2(gp + P + K));
               o1[u] = ldcg2(rb1 + K);
             }
           }
@@ -921,26 +979,27 @@ __device__ __noinline__ void accumulate_stream(const DReq& r, const DSpecies& s,
 }
 
 // true when the species went through accumulate_regs (its bead densities are added)
+template <class R>
 __device__ __forceinline__ bool accumulate_fast(const DReq& r, const DSpecies& s, double norm, bool scaled) {
   if (s.S <= 2 && s.n_seg > 1 && (r.NP >= 4096 || s.nbslot > 4 || s.neslot > 4)) {
-    accumulate_stream(r, s, norm, scaled);
+    accumulate_stream<R>(r, s, norm, scaled);
     return true;
   }
   if (s.S <= 2 && s.nbslot <= 4 && s.neslot <= 2) {
-    accumulate_pairs<4, 2>(r, s, norm, scaled);
+    accumulate_pairs<4, 2, R>(r, s, norm, scaled);
     return true;
   }
   if (s.S <= 2 && s.nbslot <= 4 && s.neslot <= 4) {
-    accumulate_pairs<4, 4>(r, s, norm, scaled);
+    accumulate_pairs<4, 4, R>(r, s, norm, scaled);
     return true;
   }
   if (s.nbslot <= 4 && s.neslot <= 4) {
-    accumulate_regs<4, 4>(r, s, norm, scaled, s.gP, s.gC, r.elam, r.lambda, s.states, s.nst, s.bslot, s.eslot, s.rho_seg,
+    accumulate_regs<4, 4, R>(r, s, norm, scaled, reinterpret_cast<const R*>(s.gP), reinterpret_cast<const R*>(s.gC), r.elam, r.lambda, s.states, s.nst, s.bslot, s.eslot, s.rho_seg,
                           r.rho_bonds, r.rho_beads);
     return true;
   }
   if (s.nbslot <= 16 && s.neslot <= 8) {
-    accumulate_regs<16, 8>(r, s, norm, scaled, s.gP, s.gC, r.elam, r.lambda, s.states, s.nst, s.bslot, s.eslot, s.rho_seg,
+    accumulate_regs<16, 8, R>(r, s, norm, scaled, reinterpret_cast<const R*>(s.gP), reinterpret_cast<const R*>(s.gC), r.elam, r.lambda, s.states, s.nst, s.bslot, s.eslot, s.rho_seg,
                            r.rho_bonds, r.rho_beads);
     return true;
   }
@@ -948,7 +1007,8 @@ __device__ __forceinline__ bool accumulate_fast(const DReq& r, const DSpecies& s
 }
 
 // eval_spatial_density! + update_spatial_structures!; false on a normalisation error
-__device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
+template <class R>
+__device__ __noinline__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
   const int P = r.NP;
   unsigned fast_mask = 0;  // species whose bead densities accumulate_regs added
   for (int u = 0; u < r.NS; u++) {
@@ -962,11 +1022,11 @@ __device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
     DSpecies s = r.sp[u];
     bool scaled = false;
     if (s.n_seg > 1) {
-      scaled |= chain_child(r, s, sh);
-      scaled |= chain_parent(r, s, sh);
+      scaled |= chain_child<R>(r, s, sh);
+      scaled |= chain_parent<R>(r, s, sh);
     }
     double norm;
-    bool ok = chain_norm(r, s, sh, &norm);
+    bool ok = chain_norm<double>(r, s, sh, &norm);
     if (!ok) {
       *bad_species = u;
       return false;
@@ -978,8 +1038,8 @@ __device__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
     }
     // the reference's prefactor norm e^{mu - lambda} overflows beyond e^709
     if (fabs(s.mu_species) + (double)(s.n_seg - 1) * fabs(log(s.normative)) > 600.0) scaled = true;
-    if (accumulate_fast(r, s, norm, scaled)) fast_mask |= 1u << u;
-    else chain_accumulate(r, s, norm, scaled);
+    if (accumulate_fast<double>(r, s, norm, scaled)) fast_mask |= 1u << u;
+    else chain_accumulate<double>(r, s, norm, scaled);
   }
   // update_spatial_structures! for the species accumulated without register slots
   if (fast_mask != (1u << r.NS) - 1u) {
@@ -1660,12 +1720,13 @@ __device__ double stage_neutrality(const DReq& r, Shared sh) {
 // ---------------------------------------------------------------------------
 // full G(x): writes r.g; returns false on a normalisation error
 // ---------------------------------------------------------------------------
-__device__ bool objective(const DReq& r, Shared sh) {
+// fp32: the propagator stage in FP32 (mixed precision), everything else FP64
+__device__ bool objective(const DReq& r, Shared sh, bool fp32 = false) {
   const int P = r.NP;
   stage_lambda(r);
-  stage_bond_factors(r);
+  stage_bond_factors(r, sh, fp32);
   int bad = -1;
-  if (!stage_densities(r, sh, &bad)) return false;
+  if (!(fp32 ? stage_densities<float>(r, sh, &bad) : stage_densities<double>(r, sh, &bad))) return false;
   stage_rho_hat(r, sh);
   for (size_t q = threadIdx.x; q < (size_t)r.NB * P; q += blockDim.x) r.Cmu[q] = 0.0;
   for (size_t q = threadIdx.x; q < (size_t)r.MB * 2 * P; q += blockDim.x) r.Clng[q] = 0.0;

@@ -56,7 +56,7 @@ extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_objective(const DR
   extern __shared__ double smem[];
   const DReq& r = reqs[blockIdx.x];
   Shared sh = make_shared(smem);
-  bool ok = objective(r, sh);
+  bool ok = objective(r, sh, r.prec == 1);
   if (threadIdx.x == 0) *r.status = ok ? ST_OK : ST_NORM;
 }
 
@@ -76,7 +76,8 @@ extern "C" __global__ void __launch_bounds__(kThreads, 3) sdft_k_solve(const DRe
   double err = sl->err;
   for (int step = 0; step < max_chunk && iter < cfg.max_iters; step++) {
     iter++;
-    if (!objective(r, sh)) {
+    // mixed precision: FP32 propagators while the residual is above the switch
+    if (!objective(r, sh, r.prec == 1 && err > cfg.mixed_switch)) {
       status = ST_NORM;
       break;
     }
@@ -207,6 +208,8 @@ struct Plan {
   size_t o_sig = 0, o_z = 0, o_dmu = 0, o_bonds = 0, o_grp = 0, o_grp_sig = 0, o_sp = 0;
   std::vector<size_t> o_states, o_nst, o_bnd, o_md, o_gC, o_gP, o_rho, o_expo, o_bslot, o_bslot_bond, o_eslot, o_eslot_bead;
   size_t o_Ext = 0, o_tr = 0, o_Csurf = 0, o_Wbond = 0, o_Wfmt = 0, o_Wmsa = 0, o_Wcoul = 0, o_tw = 0, o_twP = 0, o_twD = 0;
+  size_t o_tw32 = 0, o_twP32 = 0, o_twD32 = 0, o_fbe32 = 0;
+  int prec = SDFT_PREC_FP64;
   size_t o_x = 0, o_g = 0, o_lam = 0, o_rb = 0, o_rbo = 0, o_Cb = 0, o_Cbond = 0, o_Cmu = 0, o_Clng = 0;
   size_t o_wa = 0, o_wb = 0, o_wc = 0, o_wd = 0, o_fbe = 0, o_elam = 0;
   size_t o_hx = 0, o_hg = 0, o_u = 0;
@@ -215,6 +218,7 @@ struct Plan {
   // host tables
   std::vector<double> Ext, tr, Csurf, Wbond, Wfmt, Wmsa, Wcoul, x0;
   std::vector<double2> tw, twP, twD;
+  std::vector<float2> tw32, twP32, twD32;
 };
 
 // validation of the descriptor (the device solve's supported subset) and the
@@ -388,6 +392,12 @@ void plan_layout(Plan& pl, bool history) {
   pl.o_tw = lay.take<double2>(M / 2 + 1);
   pl.o_twP = lay.take<double2>(M + 1);
   pl.o_twD = lay.take<double2>(M + 1);
+  if (pl.prec == SDFT_PREC_MIXED) {
+    pl.o_tw32 = lay.take<float2>(M / 2 + 1);
+    pl.o_twP32 = lay.take<float2>(M + 1);
+    pl.o_twD32 = lay.take<float2>(M + 1);
+    pl.o_fbe32 = lay.take<float>((size_t)4 * MB * P + 1);
+  }
   if (history) {
     pl.o_x = lay.take<double>(pl.n);
     pl.o_g = lay.take<double>(pl.n);
@@ -490,6 +500,15 @@ void plan_tables(const sdft_system_desc* d, Plan& pl) {
   for (int k = 0; k <= M / 2; k++) pl.tw[k] = cis(-2.0L * PI_L * k / M);
   for (int k = 0; k <= M; k++) pl.twP[k] = cis(-2.0L * PI_L * k / P);
   for (int k = 0; k <= M; k++) pl.twD[k] = cis(-PI_L * k / (2.0L * P));
+  if (pl.prec == SDFT_PREC_MIXED) {
+    auto f2 = [](double2 v) { return make_float2((float)v.x, (float)v.y); };
+    pl.tw32.resize(pl.tw.size());
+    pl.twP32.resize(pl.twP.size());
+    pl.twD32.resize(pl.twD.size());
+    for (size_t k = 0; k < pl.tw.size(); k++) pl.tw32[k] = f2(pl.tw[k]);
+    for (size_t k = 0; k < pl.twP.size(); k++) pl.twP32[k] = f2(pl.twP[k]);
+    for (size_t k = 0; k < pl.twD.size(); k++) pl.twD32[k] = f2(pl.twD[k]);
+  }
   if (pl.history) {
     pl.x0.assign(pl.n, 0.0);
     for (int j = 0; j < NB; j++)
@@ -540,6 +559,7 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.funcs = (int)d->functionals;
   r.TB = tb_for(pl.M);
   r.ngrp = (int)pl.grp_sig.size();
+  r.prec = pl.prec;
   r.dz = d->bin_width;
   r.lB = d->bjerrum_length;
   r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
@@ -561,6 +581,11 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.tw = (const double2*)at(pl.o_tw);
   r.twP = (const double2*)at(pl.o_twP);
   r.twD = (const double2*)at(pl.o_twD);
+  const bool mixed = pl.prec == SDFT_PREC_MIXED;
+  r.tw32 = mixed ? (const float2*)at(pl.o_tw32) : nullptr;
+  r.twP32 = mixed ? (const float2*)at(pl.o_twP32) : nullptr;
+  r.twD32 = mixed ? (const float2*)at(pl.o_twD32) : nullptr;
+  r.fbe32 = mixed ? (float*)at(pl.o_fbe32) : nullptr;
   r.x = pl.history ? (double*)at(pl.o_x) : x;
   r.g = pl.history ? (double*)at(pl.o_g) : g;
   r.lambda = (double*)at(pl.o_lam);
@@ -622,6 +647,11 @@ cudaError_t plan_upload(const sdft_system_desc* d, const Plan& pl, char* base, c
   up(pl.o_tw, pl.tw.data(), sizeof(double2) * pl.tw.size());
   up(pl.o_twP, pl.twP.data(), sizeof(double2) * pl.twP.size());
   up(pl.o_twD, pl.twD.data(), sizeof(double2) * pl.twD.size());
+  if (pl.prec == SDFT_PREC_MIXED) {
+    up(pl.o_tw32, pl.tw32.data(), sizeof(float2) * pl.tw32.size());
+    up(pl.o_twP32, pl.twP32.data(), sizeof(float2) * pl.twP32.size());
+    up(pl.o_twD32, pl.twD32.data(), sizeof(float2) * pl.twD32.size());
+  }
   if (pl.history) up(pl.o_x, pl.x0.data(), sizeof(double) * pl.n);
   up(pl.o_dreq, &r, sizeof(DReq));
   return ce;
@@ -665,15 +695,16 @@ extern "C" void sdft_numerics_default(sdft_numerics* o) {
   o->mixing_max = 1.0;
   o->switch_tole = 1e-3;
   o->tole = 1e-6;
+  o->mixed_switch = 0.0;
 }
 
 extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
   if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
   *out = nullptr;
   if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
-  if (precision != SDFT_PREC_FP64)
-    return set_err(SDFT_ERR_UNSUPPORTED, "only the FP64 precision is available in this build");
+  if (precision != SDFT_PREC_FP64 && precision != SDFT_PREC_MIXED) return set_err(SDFT_ERR_ARG, "unknown precision");
   Plan pl;
+  pl.prec = precision;
   int rc = plan_species(d, pl);
   if (rc) return rc;
   int ndev = 0;
@@ -801,6 +832,17 @@ extern "C" int sdft_objective(sdft_handle h, double* mu_ex_K, double* lng_K, dou
   return copy_vec_out(h, h->h.g, mu_ex_K, lng_K, Psi, PsiC);
 }
 
+// Mixed precision: a request evaluates G(x) with FP32 convolutions and
+// propagators while the max-norm residual of the previous iteration is above
+// the switch, then in FP64 to the tolerance, so the converged state is the FP64
+// fixed point.  One FP32 evaluation differs from the FP64 one by 4e-8..1.4e-6
+// (max-norm relative to max|G| on the test systems); the Anderson history must
+// not be dominated by that noise, hence a switch well above it.
+static double mixed_switch(const sdft_numerics* num) {
+  const double s = num->mixed_switch > 0.0 ? num->mixed_switch : 1e-2;
+  return std::max(s, 10.0 * num->tole);
+}
+
 static int validate_numerics(const sdft_numerics* num) {
   if (!num) return set_err(SDFT_ERR_ARG, "null numerics");
   if (num->anderm < 2 || num->anderm > kMaxAnderson) return set_err(SDFT_ERR_UNSUPPORTED, "anderm must be in [2, 16]");
@@ -844,6 +886,7 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
   cfg.mixing_max = num->mixing_max;
   cfg.switch_tole = num->switch_tole;
   cfg.tole = num->tole;
+  cfg.mixed_switch = mixed_switch(num);
   // bounded launches: each runs at most `chunk` iterations per request, the
   // host re-launches until every request has converged, failed or hit max_iters
   const int chunk = 1024;
@@ -1044,6 +1087,7 @@ extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active
     cfg.mixing_max = sv->num.mixing_max;
     cfg.switch_tole = sv->num.switch_tole;
     cfg.tole = sv->num.tole;
+    cfg.mixed_switch = mixed_switch(&sv->num);
     sdft_k_solve<<<hi, kThreads, sm, sv->stream>>>(sv->dreqs, sv->dslots, cfg, iters);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(sv->hslot.data(), sv->dslots, sizeof(SolveSlot) * hi, cudaMemcpyDeviceToHost, sv->stream));

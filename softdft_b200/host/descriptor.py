@@ -21,7 +21,7 @@ from .geometry import CartesianGrid, julia_round
 from .ilst import BulkState
 from .molsys import MolecularSystem
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 FUNC_BITS = {"mfmt": 0x1, "TPT1mfmt": 0x2, "msa": 0x4, "TPT1msa": 0x8}
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -73,6 +73,7 @@ class Numerics(C.Structure):
         ("mixing_max", C.c_double),
         ("switch_tole", C.c_double),
         ("tole", C.c_double),
+        ("mixed_switch", C.c_double),
     ]
 
 
@@ -85,6 +86,7 @@ def numerics_from_dict(num: dict) -> Numerics:
         mixing_max=float(num.get("mixing_max", 1.0)),
         switch_tole=float(num.get("switch_tole", 1e-3)),
         tole=float(num.get("tole", 1e-6)),
+        mixed_switch=float(num.get("mixed_switch", 0.0)),
     )
 
 

@@ -23,4 +23,4 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert native.lib().sdft_abi_version() == 1
+    assert native.lib().sdft_abi_version() == 2
