@@ -57,8 +57,8 @@ def parse():
                     help="profiling case: only batched solves capped at --max-iters, one short line out")
     ap.add_argument("--max-iters", type=int, default=0)
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=600)
-    ap.add_argument("--serve-rate", type=float, default=150.0, help="offered requests/s of the serving stream")
+    ap.add_argument("--serve-requests", type=int, default=1500)
+    ap.add_argument("--serve-rate", type=float, default=100.0, help="offered requests/s of the serving stream")
     ap.add_argument("--serve-iters", type=int, default=25, help="Anderson iterations per server launch")
     return ap.parse_args()
 
