@@ -187,6 +187,52 @@ int sdft_server_step(sdft_server_t server, int32_t iters, int32_t* active, int32
 int sdft_server_poll(sdft_server_t server, int64_t* tags, int32_t* status, int32_t* iters, double* errs,
                      double* device_ms, int32_t max, int32_t* n);
 
+/* ---- bulk (iLST) state evaluation on the host --------------------------------
+ * One evaluation of the bulk residual's expensive steps, for the host solve of
+ * the bulk state that seeds every request (src/iLST/evaluation/objective/
+ * residual_bulkstate.jl:26-35): eval_bulk_density! (eval_bulk_density.jl:9-22
+ * with the freely-jointed / monomer-bead accumulate_densities!) followed by
+ * bulk_chemical_potential (bulk_chemical_potential.jl:9-25).  Topologies are
+ * general trees: per segment its parent (-1 for the root), children, and the
+ * segments grouped by level (root level first). */
+#define SDFT_BULK_IDEAL     1u
+#define SDFT_BULK_MFMT      2u
+#define SDFT_BULK_TPT1MFMT  4u
+#define SDFT_BULK_MSA       8u
+#define SDFT_BULK_TPT1MSA  16u
+
+typedef struct sdft_bulk_species {
+  int32_t n_seg, max_states, max_children, n_levels;
+  int32_t monomerbead;           /* 1: monomer-bead model (state sum of segment 0) */
+  const int32_t* n_states;       /* [n_seg] */
+  const int32_t* states;         /* [n_seg * max_states] bead type of each state */
+  const int32_t* parent;         /* [n_seg] */
+  const int32_t* n_children;     /* [n_seg] */
+  const int32_t* children;       /* [n_seg * max_children] */
+  const int32_t* level_ptr;      /* [n_levels + 1] */
+  const int32_t* level_segs;     /* [n_seg] */
+} sdft_bulk_species;
+
+typedef struct sdft_bulk_system {
+  int32_t nb, mb, ns;
+  uint32_t models;               /* SDFT_BULK_* bits */
+  const double* diameter;        /* [nb] */
+  const double* valence;         /* [nb] */
+  const double* delta_muH;       /* [nb] */
+  const int32_t* bond_types;     /* [2 * mb] sorted pairs */
+  const sdft_bulk_species* species; /* [ns] */
+  double bjerrum_length;
+} sdft_bulk_system;
+
+/* Inputs: species densities [ns], mu_ex [nb] and lng [mb] of the previous
+ * evaluation.  Outputs: segment densities (per species max_states x n_seg,
+ * state index fastest, species after species), bead densities [nb], bond-end
+ * densities [2 x mb] (row-major), mu_species [ns], the new mu_ex [nb] and lng
+ * [mb], and the partition functions Xi [ns].  Host only; no device call. */
+int sdft_bulk_eval(const sdft_bulk_system* sys, const double* rho_species, const double* mu_ex_in,
+                   const double* lng_in, double* rho_segments, double* rho_beads, double* rho_bonds,
+                   double* mu_species, double* mu_ex, double* lng, double* xi);
+
 /* Bytes of the static device array behind sdft_objective_noalloc (16 MiB). */
 #define SDFT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 

@@ -16,6 +16,7 @@ includes.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 from dataclasses import dataclass, field
 from typing import List
@@ -553,7 +554,116 @@ def balance_charge(ms: MolecularSystem, bulk: BulkState, Q: float, adjustable: L
             bulk.rho_species[i] = ms.input_densities[i]
 
 
-def residual_bulkstate(ms: MolecularSystem, bulk: BulkState, sol, adjustable) -> np.ndarray:
+# --------------------------------------------------------------------------
+# native evaluation (sdft_bulk_eval of libsoftdft.so)
+# --------------------------------------------------------------------------
+_MODEL_BITS = {"ideal": 1, "mfmt": 2, "TPT1mfmt": 4, "msa": 8, "TPT1msa": 16, "coul": 0}
+
+
+class _BulkSpecies(ctypes.Structure):
+    _fields_ = [("n_seg", ctypes.c_int32), ("max_states", ctypes.c_int32), ("max_children", ctypes.c_int32),
+                ("n_levels", ctypes.c_int32), ("monomerbead", ctypes.c_int32),
+                ("n_states", ctypes.c_void_p), ("states", ctypes.c_void_p), ("parent", ctypes.c_void_p),
+                ("n_children", ctypes.c_void_p), ("children", ctypes.c_void_p), ("level_ptr", ctypes.c_void_p),
+                ("level_segs", ctypes.c_void_p)]
+
+
+class _BulkSystem(ctypes.Structure):
+    _fields_ = [("nb", ctypes.c_int32), ("mb", ctypes.c_int32), ("ns", ctypes.c_int32), ("models", ctypes.c_uint32),
+                ("diameter", ctypes.c_void_p), ("valence", ctypes.c_void_p), ("delta_muH", ctypes.c_void_p),
+                ("bond_types", ctypes.c_void_p), ("species", ctypes.c_void_p), ("bjerrum_length", ctypes.c_double)]
+
+
+def _native_bulk(ms: MolecularSystem):
+    """ctypes descriptor of the molecular system for sdft_bulk_eval (cached on ms)."""
+    cached = getattr(ms, "_bulk_native", None)
+    if cached is not None:
+        return cached
+    from .. import native
+    lib = native.lib()
+    keep = []
+
+    def arr(a, dt):
+        v = np.ascontiguousarray(np.asarray(a, dtype=dt))
+        keep.append(v)
+        return v.ctypes.data
+
+    models = 0
+    for m in ms.fe_model:
+        if m not in _MODEL_BITS:
+            raise NotImplementedError(f"model '{m}' is not supported")
+        models |= _MODEL_BITS[m]
+    sp = (_BulkSpecies * len(ms.configurations))()
+    seg_sizes = []
+    for u, cfg in enumerate(ms.configurations):
+        fam, topo = cfg.state_family, cfg.topology
+        n = len(cfg.sequence)
+        S = max(max(len(f) for f in fam), 1)
+        C = max(max((len(c) for c in topo.children), default=0), 1)
+        states = np.full((n, S), -1, dtype=np.int32)
+        for g, f in enumerate(fam):
+            states[g, :len(f)] = f
+        children = np.full((n, C), -1, dtype=np.int32)
+        for g, ch in enumerate(topo.children):
+            children[g, :len(ch)] = ch
+        parent = [p[0] if p else -1 for p in topo.parents]
+        level_ptr = np.cumsum([0] + [len(l) for l in topo.levels])
+        level_segs = [g for l in topo.levels for g in l]
+        sp[u] = _BulkSpecies(n, S, C, len(topo.levels), 1 if cfg.model == "monomerbead" else 0,
+                             arr([len(f) for f in fam], np.int32), arr(states, np.int32), arr(parent, np.int32),
+                             arr([len(c) for c in topo.children], np.int32), arr(children, np.int32),
+                             arr(level_ptr, np.int32), arr(level_segs, np.int32))
+        seg_sizes.append((S, n))
+    keep.append(sp)
+    sysd = _BulkSystem(len(ms.monomers), len(ms.bond_types), len(ms.configurations), models,
+                       arr(ms.diameters, np.float64), arr(ms.valences, np.float64), arr(ms.delta_muH, np.float64),
+                       arr([x for b in ms.bond_types for x in b], np.int32), ctypes.addressof(sp),
+                       float(ms.bjerrum_length))
+    f = lib.sdft_bulk_eval
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p] * 11
+    cached = (lib, sysd, keep, seg_sizes)
+    ms._bulk_native = cached
+    return cached
+
+
+def eval_bulk_state_native(ms: MolecularSystem, bulk: BulkState) -> None:
+    """eval_bulk_density followed by bulk_chemical_potential in one native call."""
+    lib, sysd, _, seg_sizes = _native_bulk(ms)
+    nb, mb, ns = len(ms.monomers), len(ms.bond_types), len(ms.configurations)
+    segs = np.zeros(sum(S * n for S, n in seg_sizes))
+    rb = np.zeros(nb)
+    rbo = np.zeros(2 * mb + 1)
+    mus = np.zeros(ns)
+    mu = np.zeros(nb)
+    lng = np.zeros(mb + 1)
+    xi = np.zeros(ns)
+    rs = np.ascontiguousarray(bulk.rho_species, dtype=np.float64)
+    mu_in = np.ascontiguousarray(bulk.mu_ex, dtype=np.float64)
+    lng_in = np.ascontiguousarray(np.concatenate([bulk.lng, [0.0]]), dtype=np.float64)
+    p = lambda a: a.ctypes.data
+    rc = lib.sdft_bulk_eval(ctypes.byref(sysd), p(rs), p(mu_in), p(lng_in), p(segs), p(rb), p(rbo), p(mus), p(mu),
+                            p(lng), p(xi))
+    if rc != 0:
+        raise RuntimeError(f"sdft_bulk_eval failed ({rc})")
+    off = 0
+    for u, (S, n) in enumerate(seg_sizes):
+        bulk.rho_segments[u][:, :] = segs[off: off + S * n].reshape(n, S).T
+        off += S * n
+    bulk.rho_beads[:] = rb
+    bulk.rho_bonds[:, :] = rbo[: 2 * mb].reshape(2, mb)
+    bulk.mu_species[:] = mus
+    bulk.mu_ex[:] = mu
+    bulk.lng[:] = lng[:mb]
+    bulk.Xi[:] = xi
+
+
+def _use_native() -> bool:
+    from .. import native
+    return native.library_present()
+
+
+def residual_bulkstate(ms: MolecularSystem, bulk: BulkState, sol, adjustable, native_eval: bool = True) -> np.ndarray:
     """`evaluation/objective/residual_bulkstate.jl:26-35` +
     `functions/update_bulk_structures.jl:10-44` + `functions/eval_residuals.jl:26-60`."""
     log_rxn, log_ph, Q = sol
@@ -565,8 +675,11 @@ def residual_bulkstate(ms: MolecularSystem, bulk: BulkState, sol, adjustable) ->
             bulk.rho_species[i] = math.exp(log_ph[ip]); ip += 1
         elif s in inr:
             bulk.rho_species[i] = math.exp(log_rxn[ir]); ir += 1
-    eval_bulk_density(ms, bulk)
-    bulk_chemical_potential(ms, bulk)
+    if native_eval and _use_native():
+        eval_bulk_state_native(ms, bulk)
+    else:
+        eval_bulk_density(ms, bulk)
+        bulk_chemical_potential(ms, bulk)
     res = []
     unit = concentration_to_density(1.0, ms.constants)
     for i in range(len(ms.species)):

@@ -25,13 +25,18 @@ EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_num
            "sdft_request_create", "sdft_request_destroy", "sdft_request_sizes", "sdft_set_state",
            "sdft_get_state", "sdft_objective", "sdft_solve", "sdft_get_densities", "sdft_grand_potential",
            "sdft_num_species", "sdft_solve_batch", "sdft_last_batch_stats", "sdft_server_create",
-           "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll"]
+           "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll", "sdft_bulk_eval"]
 
 
 class SdftError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
         self.code = code
+
+
+def library_present() -> bool:
+    """True when the shared library has been built next to this module."""
+    return os.path.exists(LIB_PATH)
 
 
 def lib():
