@@ -16,13 +16,7 @@
 #include "common.cuh"
 
 namespace sdft {
-
-struct SolveCfg {
-  int max_iters;
-  int anderm;
-  double damping, mixing_max, switch_tole, tole;
-  double mixed_switch;  // residual below which a mixed-precision request evaluates in FP64
-};
+namespace {  // internal linkage: each kernel build (kernels.cuh) has its own copy
 
 struct AndersonState {
   int use_picard;
@@ -249,4 +243,5 @@ __device__ int anderson_step(const DReq& r, const SolveCfg& cfg, int iter, Ander
   return err < cfg.tole ? ST_OK : ST_RUNNING;
 }
 
+}  // namespace
 }  // namespace sdft

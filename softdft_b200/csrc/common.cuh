@@ -21,6 +21,8 @@ constexpr int kMaxBeads = 32;        // bead types
 constexpr int kMaxBonds = 64;        // bond types
 constexpr int kMaxAnderson = 16;     // Anderson depth m
 constexpr int kMaxTB = 4;            // transforms in flight per CTA
+constexpr int kMaxRadices = 24;      // stages of a general-length FFT
+constexpr int kMaxGenRadix = 61;     // largest prime factor of a general-length FFT
 constexpr double kPi = 3.14159265358979323846;
 
 // status codes written by the kernels (mirror sdft_status)
@@ -60,7 +62,10 @@ struct DSpecies {
 
 struct DReq {
   // sizes
-  int NP, M, L;       // grid points P, FFT length M = P/2, log2(M)
+  int NP, M, L;       // grid points P, FFT length M = P/2, log2(M) (power-of-two M)
+  int gen;            // 1: M is not a power of two (mixed-radix tables below)
+  int nrad;           // general length: number of radices
+  int rad[kMaxRadices];  // general length: radices r_0 .. r_{nrad-1}, M = their product
   int NB, MB, NS;
   int funcs;          // SDFT_FUNC_* bits
   int TB;             // transform buffers in shared memory for this launch (1..kMaxTB)
@@ -86,7 +91,8 @@ struct DReq {
   const double* Wmsa;     // [NB * P]
   const double* Wcoul;    // [P]
   // FFT tables
-  const double2* tw;      // [M/2] e^{-2 pi i k / M}
+  const double2* tw;      // [M/2] e^{-2 pi i k / M} ([M] for a general length)
+  const int* slot;        // general length: [M] digit-reversed slot of natural index m
   const double2* twP;     // [M+1] e^{-2 pi i k / P}
   const double2* twD;     // [M+1] e^{-i pi k / (2P)}
   const float2* tw32;     // FP32 copies of tw, twP, twD (mixed precision)
@@ -207,5 +213,40 @@ __device__ __forceinline__ void block_sum_vec(double* vals, int k, double* red) 
     vals[q] = t;
   }
 }
+
+// ---- solve configuration and per-request solver state (host and device) ----
+struct SolveCfg {
+  int max_iters;
+  int anderm;
+  double damping, mixing_max, switch_tole, tole;
+  double mixed_switch;  // residual below which a mixed-precision request evaluates in FP64
+};
+
+struct SolveSlot {       // per-request solver state kept across launches
+  int iter;
+  int status;
+  int use_picard;
+  int pad;
+  double err;
+  unsigned long long t0, t1;  // %globaltimer (ns) at the first and the last iteration
+  double lam[kMaxAnderson];
+};
+
+constexpr int kRedDoubles = 1024;              // reduction scratch ahead of the transform buffers
+constexpr size_t kMaxSmemBytes = 227 * 1024;   // dynamic shared memory a CTA may opt into
+
+// ---- kernel launches ----
+// The kernels are compiled twice (kernels_pow2.cu, kernels_gen.cu): once with
+// the power-of-two FFT passes and once with the general-length ones, so that
+// neither build carries the other's code.  A launch runs one CTA per request
+// and skips the requests of the other kind.
+cudaError_t launch_objective_pow2(const DReq* reqs, int n, size_t smem, cudaStream_t s);
+cudaError_t launch_solve_pow2(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, int max_chunk, int n, size_t smem,
+                              cudaStream_t s);
+cudaError_t launch_omega_pow2(const DReq* reqs, double* out, size_t smem, cudaStream_t s);
+cudaError_t launch_objective_gen(const DReq* reqs, int n, size_t smem, cudaStream_t s);
+cudaError_t launch_solve_gen(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, int max_chunk, int n, size_t smem,
+                             cudaStream_t s);
+cudaError_t launch_omega_gen(const DReq* reqs, double* out, size_t smem, cudaStream_t s);
 
 }  // namespace sdft

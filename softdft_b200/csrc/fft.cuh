@@ -20,7 +20,9 @@
 // bit-reversed order and radix-8/4/2 decimation-in-time passes (three radix-2
 // stages per pass, in registers) leave natural order.  Inverse: radix-8/4/2
 // decimation-in-frequency passes take natural order and leave bit-reversed
-// order, undone by the gather of the store.  The DCT twiddle step only couples
+// order, undone by the gather of the store.  A length M that is not a power of
+// two runs mixed-radix passes instead (radices 4, 2, 3, 5, 7 and primes up to
+// kMaxGenRadix) with a digit-reversed load and store.  The DCT twiddle step only couples
 // Z[k] and Z[M-k], so a convolution is: load, FFT, one in-place pair pass that
 // also applies the weight, IFFT, store.
 //
@@ -30,7 +32,14 @@
 
 #include "common.cuh"
 
+// SDFT_FFT_GEN selects the transform passes this build carries: 0 for
+// power-of-two M, 1 for a general M (see kernels.cuh)
+#ifndef SDFT_FFT_GEN
+#error "define SDFT_FFT_GEN (0: power-of-two FFT lengths, 1: general lengths) before including fft.cuh"
+#endif
+
 namespace sdft {
+namespace {  // internal linkage: each kernel build (kernels.cuh) has its own copy
 
 __device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
 
@@ -44,7 +53,10 @@ struct FftCtxT {
   C* z;              // TB buffers of `stride` slots
   int stride;        // M + M/8
   int P, M, L, H;    // H = M/2
-  const C* __restrict__ tw;   // [M/2] e^{-2 pi i k / M}
+  int nrad;          // general length: mixed-radix passes over rad[0 .. nrad-1]
+  const int* rad;
+  const int* __restrict__ slot;  // general length: digit-reversed slot of natural index m
+  const C* __restrict__ tw;   // [M/2] e^{-2 pi i k / M} ([M] for a general length)
   const C* __restrict__ twP;  // [M+1] e^{-2 pi i k / P}
   const C* __restrict__ twD;  // [M+1] e^{-i pi k / 2P}
 };
@@ -58,6 +70,9 @@ __device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
   c.P = r.NP;
   c.H = r.M >> 1;
   c.stride = r.M + (r.M >> 3);
+  c.nrad = r.nrad;
+  c.rad = r.rad;
+  c.slot = r.slot;
   c.tw = r.tw;
   c.twP = r.twP;
   c.twD = r.twD;
@@ -73,37 +88,63 @@ __device__ __forceinline__ FftCtxT<float2> make_fft32(double2* z, const DReq& r)
   c.P = r.NP;
   c.H = r.M >> 1;
   c.stride = r.M + (r.M >> 3);
+  c.nrad = r.nrad;
+  c.rad = r.rad;
+  c.slot = r.slot;
   c.tw = r.tw32;
   c.twP = r.twP32;
   c.twD = r.twD32;
   return c;
 }
 
-// position of real sample K in the packed complex buffer: (bit-reversed index, component)
-__device__ __forceinline__ void dct_slot(int K, int P, int L, int* pos, int* comp) {
-  int q = (K & 1) ? (P - 1 - (K >> 1)) : (K >> 1);  // Makhoul reorder v[q]
-  *pos = brev_bits(q >> 1, L);
+// The loops below come in two instantiations: G = false for power-of-two M
+// (bit reversal, shifts), G = true for a general M (digit-reversal table,
+// divisions); the entry points instantiate the one of this build.
+
+// buffer slot of natural complex index m
+template <bool G, class C>
+__device__ __forceinline__ int fslot(const FftCtxT<C>& c, int m) {
+  if constexpr (G)
+    return __ldg(&c.slot[m]);
+  else
+    return brev_bits(m, c.L);
+}
+
+// transform index of item it, n items per transform (n = 2^ln when !G)
+template <bool G>
+__device__ __forceinline__ int item_t(int it, int n, int ln) {
+  if constexpr (G)
+    return it / n;
+  else
+    return it >> ln;
+}
+
+// position of real sample K in the packed complex buffer: (slot, component)
+template <bool G, class C>
+__device__ __forceinline__ void dct_slot(const FftCtxT<C>& c, int K, int* pos, int* comp) {
+  int q = (K & 1) ? (c.P - 1 - (K >> 1)) : (K >> 1);  // Makhoul reorder v[q]
+  *pos = fslot<G>(c, q >> 1);
   *comp = q & 1;
 }
 
-template <class F>
+template <bool G, class F>
 __device__ __forceinline__ void load_b(const FftCtx& c, int nT, F f) {
   const int lp = c.L + 1;  // log2 P
-  for (int it = threadIdx.x; it < (nT << lp); it += blockDim.x) {
-    const int t = it >> lp, K = it & (c.P - 1);
+  for (int it = threadIdx.x; it < nT * c.P; it += blockDim.x) {
+    const int t = item_t<G>(it, c.P, lp), K = it - t * c.P;
     int pos, comp;
-    dct_slot(K, c.P, c.L, &pos, &comp);
+    dct_slot<G>(c, K, &pos, &comp);
     reinterpret_cast<double*>(c.z + (size_t)t * c.stride + fpad(pos))[comp] = f(t, K);
   }
 }
 
-template <class S>
+template <bool G, class S>
 __device__ __forceinline__ void store_b(const FftCtx& c, int nT, double scale, S st) {
   const int lp = c.L + 1;
-  for (int it = threadIdx.x; it < (nT << lp); it += blockDim.x) {
-    const int t = it >> lp, K = it & (c.P - 1);
+  for (int it = threadIdx.x; it < nT * c.P; it += blockDim.x) {
+    const int t = item_t<G>(it, c.P, lp), K = it - t * c.P;
     int pos, comp;
-    dct_slot(K, c.P, c.L, &pos, &comp);
+    dct_slot<G>(c, K, &pos, &comp);
     st(t, K, reinterpret_cast<const double*>(c.z + (size_t)t * c.stride + fpad(pos))[comp] * scale);
   }
 }
@@ -117,52 +158,54 @@ __device__ __forceinline__ void stcg2(double* p, double2 v) { __stcg(reinterpret
 __device__ __forceinline__ float2 ldcg2(const float* p) { return __ldcg(reinterpret_cast<const float2*>(p)); }
 __device__ __forceinline__ void stcg2(float* p, float2 v) { __stcg(reinterpret_cast<float2*>(p), v); }
 
-template <class C, class V>
+template <bool G, class C, class V>
 __device__ __forceinline__ void put_pair(const FftCtxT<C>& c, int t, int kp, V v) {
   using R = typename Cx<C>::R;
   R* zb = reinterpret_cast<R*>(c.z + (size_t)t * c.stride);
   const int q1 = c.P - 1 - kp;
-  zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)] = (R)v.x;
-  zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)] = (R)v.y;
+  zb[2 * fpad(fslot<G>(c, kp >> 1)) + (kp & 1)] = (R)v.x;
+  zb[2 * fpad(fslot<G>(c, q1 >> 1)) + (q1 & 1)] = (R)v.y;
 }
-template <class C>
+template <bool G, class C>
 __device__ __forceinline__ C get_pair(const FftCtxT<C>& c, int t, int kp) {
   using R = typename Cx<C>::R;
   const R* zb = reinterpret_cast<const R*>(c.z + (size_t)t * c.stride);
   const int q1 = c.P - 1 - kp;
-  return Cx<C>::make(zb[2 * fpad(brev_bits(kp >> 1, c.L)) + (kp & 1)], zb[2 * fpad(brev_bits(q1 >> 1, c.L)) + (q1 & 1)]);
+  return Cx<C>::make(zb[2 * fpad(fslot<G>(c, kp >> 1)) + (kp & 1)], zb[2 * fpad(fslot<G>(c, q1 >> 1)) + (q1 & 1)]);
 }
 
 // f2(t, K) -> (f(K), f(K+1)) for even K
-template <class C, class F2>
+template <bool G, class C, class F2>
 __device__ __forceinline__ void load_b2(const FftCtxT<C>& c, int nT, F2 f2) {
-  const int lm = c.L;
-  const int total = nT << lm;
+  const int lm = c.L, M = c.M;
+  const int total = nT * M;
   for (int b0 = threadIdx.x; b0 < total; b0 += 2 * blockDim.x) {
     const int i1 = b0 + blockDim.x;
-    const auto v0 = f2(b0 >> lm, (b0 & (c.M - 1)) << 1);
+    const int t0 = item_t<G>(b0, M, lm), k0 = b0 - t0 * M;
+    const int t1 = item_t<G>(i1, M, lm), k1 = i1 - t1 * M;
+    const auto v0 = f2(t0, k0 << 1);
     auto v1 = v0;
-    if (i1 < total) v1 = f2(i1 >> lm, (i1 & (c.M - 1)) << 1);
-    put_pair(c, b0 >> lm, b0 & (c.M - 1), v0);
-    if (i1 < total) put_pair(c, i1 >> lm, i1 & (c.M - 1), v1);
+    if (i1 < total) v1 = f2(t1, k1 << 1);
+    put_pair<G>(c, t0, k0, v0);
+    if (i1 < total) put_pair<G>(c, t1, k1, v1);
   }
 }
 
 // put2(t, K, (y_K, y_K+1) * scale, pre2(t, K)) for even K; pre2 holds the loads
-template <class C, class A2, class S2>
+template <bool G, class C, class A2, class S2>
 __device__ __forceinline__ void store_b2(const FftCtxT<C>& c, int nT, typename Cx<C>::R scale, A2 pre2, S2 put2) {
-  const int lm = c.L;
-  const int total = nT << lm;
+  const int lm = c.L, M = c.M;
+  const int total = nT * M;
   for (int b0 = threadIdx.x; b0 < total; b0 += 2 * blockDim.x) {
     const int i1 = b0 + blockDim.x;
-    const int t0 = b0 >> lm, K0 = (b0 & (c.M - 1)) << 1;
-    C y0 = get_pair(c, t0, K0 >> 1);
+    const int t0 = item_t<G>(b0, M, lm), K0 = (b0 - t0 * M) << 1;
+    C y0 = get_pair<G>(c, t0, K0 >> 1);
     const auto a0 = pre2(t0, K0);
     C y1 = y0;
     auto a1 = a0;
-    const int t1 = i1 >> lm, K1 = (i1 & (c.M - 1)) << 1;
+    const int t1 = item_t<G>(i1, M, lm), K1 = (i1 - t1 * M) << 1;
     if (i1 < total) {
-      y1 = get_pair(c, t1, K1 >> 1);
+      y1 = get_pair<G>(c, t1, K1 >> 1);
       a1 = pre2(t1, K1);
     }
     y0.x *= scale;
@@ -189,9 +232,150 @@ __device__ __forceinline__ void bfly_dif(C& a, C& b, C w) {  // DIF: (a + b, (a 
   b = cmul(d, w);
 }
 
-// forward FFT of nT buffers: bit-reversed input -> natural output
+// ---- general length M --------------------------------------------------------
+// M = r_0 r_1 ... r_{s-1} with radices 4, 2, 3, 5, 7 and primes up to
+// kMaxGenRadix.  Forward: in-place decimation in time over stages of growing
+// span m = r_0 ... r_{i-1}; the butterfly (group g, offset j < m) takes
+// x_q = z[g m r + j + q m] w_{m r}^{j q} (q < r) and writes its r-point DFT back to
+// the same slots.  Its input order is the mixed-radix digit reversal: natural
+// index n = d_0 M/r_0 + d_1 M/(r_0 r_1) + ... sits in slot d_0 + r_0 (d_1 + r_1 (...)),
+// which the host tabulates as slot[n].  Inverse: the stages in reverse order as
+// decimation in frequency (r-point inverse DFT, then the conjugate twiddles),
+// natural order in, the same digit-reversed order out.  Roots of unity come
+// from tw[k] = e^{-2 pi i k / M}: w_r^e = tw[e M / r].
+
+// r-point DFT in registers (inv: conjugate roots), compile-time r
+template <class C, int R>
+__device__ __forceinline__ void dft_fixed(C* x, const C* __restrict__ tw, int step, bool inv) {
+  if (R == 2) {
+    const C a = x[0], b = x[1];
+    x[0] = add2(a, b);
+    x[1] = sub2(a, b);
+  } else if (R == 4) {
+    const C s02 = add2(x[0], x[2]), d02 = sub2(x[0], x[2]);
+    const C s13 = add2(x[1], x[3]), d13 = sub2(x[1], x[3]);
+    const C jd = inv ? Cx<C>::make(-d13.y, d13.x) : Cx<C>::make(d13.y, -d13.x);  // (+-i) d13
+    x[0] = add2(s02, s13);
+    x[2] = sub2(s02, s13);
+    x[1] = add2(d02, jd);
+    x[3] = sub2(d02, jd);
+  } else {
+    C w[R], X[R];
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      w[k] = __ldg(&tw[k * step]);
+      if (inv) w[k] = conj2(w[k]);
+    }
+#pragma unroll
+    for (int l = 0; l < R; l++) {
+      C acc = x[0];
+#pragma unroll
+      for (int q = 1; q < R; q++) acc = add2(acc, cmul(x[q], w[(q * l) % R]));
+      X[l] = acc;
+    }
+#pragma unroll
+    for (int l = 0; l < R; l++) x[l] = X[l];
+  }
+}
+
+// r-point DFT for a prime r known only at run time (r <= kMaxGenRadix)
+template <class C>
+__device__ __noinline__ void dft_any(C* x, int R, const C* __restrict__ tw, int step, bool inv) {
+  C X[kMaxGenRadix];
+  for (int l = 0; l < R; l++) {
+    C acc = x[0];
+    int e = 0;  // (q l) mod R
+    for (int q = 1; q < R; q++) {
+      e += l;
+      if (e >= R) e -= R;
+      C w = __ldg(&tw[e * step]);
+      if (inv) w = conj2(w);
+      acc = add2(acc, cmul(x[q], w));
+    }
+    X[l] = acc;
+  }
+  for (int l = 0; l < R; l++) x[l] = X[l];
+}
+
+// one stage of radix R (R = 0: run-time radix rr) and span m; DIT forward or DIF inverse
+template <class C, int R>
+__device__ __forceinline__ void gen_stage(const FftCtxT<C>& c, int nT, int m, int rr, bool inv) {
+  constexpr int NX = R > 0 ? R : kMaxGenRadix;
+  const int r = R > 0 ? R : rr;
+  const int M = c.M, nb = M / r, tws = M / (m * r), step = M / r;
+  for (int it = threadIdx.x; it < nT * nb; it += blockDim.x) {
+    const int t = it / nb, b = it - t * nb;
+    const int j = b % m, base = (b - j) * r + j;
+    C* zb = c.z + (size_t)t * c.stride;
+    C x[NX];
+#pragma unroll
+    for (int q = 0; q < NX; q++)
+      if (q < r) x[q] = zb[fpad(base + q * m)];
+    if (!inv) {
+#pragma unroll
+      for (int q = 1; q < NX; q++)
+        if (q < r) x[q] = cmul(x[q], __ldg(&c.tw[j * q * tws]));
+    }
+    if (R > 0)
+      dft_fixed<C, (R > 0 ? R : 2)>(x, c.tw, step, inv);
+    else
+      dft_any(x, r, c.tw, step, inv);
+    if (inv) {
+#pragma unroll
+      for (int q = 1; q < NX; q++)
+        if (q < r) x[q] = cmul(x[q], conj2(__ldg(&c.tw[j * q * tws])));
+    }
+#pragma unroll
+    for (int q = 0; q < NX; q++)
+      if (q < r) zb[fpad(base + q * m)] = x[q];
+  }
+}
+
+template <class C>
+__device__ __forceinline__ void gen_stage_any_radix(const FftCtxT<C>& c, int nT, int m, int r, bool inv) {
+  switch (r) {
+    case 2: gen_stage<C, 2>(c, nT, m, 2, inv); break;
+    case 3: gen_stage<C, 3>(c, nT, m, 3, inv); break;
+    case 4: gen_stage<C, 4>(c, nT, m, 4, inv); break;
+    case 5: gen_stage<C, 5>(c, nT, m, 5, inv); break;
+    case 7: gen_stage<C, 7>(c, nT, m, 7, inv); break;
+    default: gen_stage<C, 0>(c, nT, m, r, inv); break;
+  }
+}
+
+// general-length forward FFT: digit-reversed input -> natural output
+template <class C>
+__device__ __noinline__ void fft_gen_fwd(const FftCtxT<C> c, int nT) {
+  int m = 1;
+  for (int s = 0; s < c.nrad; s++) {
+    const int r = c.rad[s];
+    __syncthreads();
+    gen_stage_any_radix(c, nT, m, r, false);
+    m *= r;
+  }
+  __syncthreads();
+}
+
+// general-length inverse FFT (unscaled): natural input -> digit-reversed output
+template <class C>
+__device__ __noinline__ void fft_gen_inv(const FftCtxT<C> c, int nT) {
+  int m = c.M;
+  for (int s = c.nrad - 1; s >= 0; s--) {
+    const int r = c.rad[s];
+    m /= r;
+    __syncthreads();
+    gen_stage_any_radix(c, nT, m, r, true);
+  }
+  __syncthreads();
+}
+
+// forward FFT of nT buffers: bit-reversed (digit-reversed) input -> natural output
 template <class C>
 __device__ __forceinline__ void fft_fwd_b(const FftCtxT<C>& c, int nT) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    fft_gen_fwd(c, nT);
+    return;
+  }
   const int M = c.M, L = c.L;
   for (int s = 0; s < L;) {
     const int rr = min(3, L - s);
@@ -257,9 +441,13 @@ __device__ __forceinline__ void fft_fwd_b(const FftCtxT<C>& c, int nT) {
   __syncthreads();
 }
 
-// inverse FFT of nT buffers (unscaled): natural input -> bit-reversed output
+// inverse FFT of nT buffers (unscaled): natural input -> bit-reversed (digit-reversed) output
 template <class C>
 __device__ __forceinline__ void fft_inv_b(const FftCtxT<C>& c, int nT) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    fft_gen_inv(c, nT);
+    return;
+  }
   const int M = c.M, L = c.L;
   for (int top = L; top > 0;) {
     const int rr = min(3, top);
@@ -398,21 +586,22 @@ __device__ __forceinline__ C mid_inverse(typename Cx<C>::R eh, typename Cx<C>::R
   return conj2(V);
 }
 
-// pair items: it -> (t, k) with k in [0, H); k = 0 also handles k = H
+// pair items: it -> (t, k) with k in [0, (M+1)/2); k = 0 also handles k = H = M/2
+// when M is even (odd M has no middle coefficient pair)
 #define SDFT_PAIR_LOOP(c, nT)                                           \
-  const int lH_ = (c).L - 1;                                            \
-  for (int it = threadIdx.x; it < ((nT) << lH_); it += blockDim.x) {   \
-    const int t = it >> lH_, k = it & ((c).H - 1);                      \
+  const int lH_ = (c).L - 1, cnt_ = ((c).M + 1) >> 1;                   \
+  for (int it = threadIdx.x; it < (nT) * cnt_; it += blockDim.x) {     \
+    const int t = item_t<GEN>(it, cnt_, lH_), k = it - t * cnt_;        \
     auto* zb = (c).z + (size_t)t * (c).stride;
 
 // ---- whole transforms ------------------------------------------------------
 
 // C[q] for q in [0, P): forward DCT-II of f(t, .); emit(t, q, C[q])
-template <class F, class E>
-__device__ __forceinline__ void dct2_forward_b(const FftCtx& c, int nT, F f, E emit) {
+template <bool GEN, class F, class E>
+__device__ __forceinline__ void dct2_forward_b_impl(const FftCtx& c, int nT, F f, E emit) {
   const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
-  load_b(c, nT, f);
+  load_b<GEN>(c, nT, f);
   fft_fwd_b(c, nT);
   SDFT_PAIR_LOOP(c, nT)
   if (k == 0) {
@@ -420,10 +609,12 @@ __device__ __forceinline__ void dct2_forward_b(const FftCtx& c, int nT, F f, E e
     zero_forward(zb[0], __ldg(&c.twD[M]), &c0, &cM);
     emit(t, 0, c0);
     emit(t, M, cM);
-    double ch, cPh;
-    mid_forward(zb[fpad(H)], __ldg(&c.twD[H]), &ch, &cPh);
-    emit(t, H, ch);
-    emit(t, P - H, cPh);
+    if (!(M & 1)) {
+      double ch, cPh;
+      mid_forward(zb[fpad(H)], __ldg(&c.twD[H]), &ch, &cPh);
+      emit(t, H, ch);
+      emit(t, P - H, cPh);
+    }
   } else {
     Quad q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], __ldg(&c.twP[k]), __ldg(&c.twD[k]), __ldg(&c.twD[M - k]));
     emit(t, k, q.c0);
@@ -435,15 +626,20 @@ __device__ __forceinline__ void dct2_forward_b(const FftCtx& c, int nT, F f, E e
 __syncthreads();
 }
 
+template <class F, class E>
+__device__ __forceinline__ void dct2_forward_b(const FftCtx& c, int nT, F f, E emit) {
+  dct2_forward_b_impl<(SDFT_FFT_GEN != 0)>(c, nT, f, emit);
+}
+
 // y = iDCT2(E_t), E_t[q] = get(t, q); store(t, K, y[K])
-template <class G, class S>
-__device__ __forceinline__ void dct2_inverse_b(const FftCtx& c, int nT, G get, S store) {
+template <bool GEN, class G, class S>
+__device__ __forceinline__ void dct2_inverse_b_impl(const FftCtx& c, int nT, G get, S store) {
   const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
   SDFT_PAIR_LOOP(c, nT)
   if (k == 0) {
     zb[0] = zero_inverse(get(t, 0), get(t, M), __ldg(&c.twD[M]));
-    zb[fpad(H)] = mid_inverse(get(t, H), get(t, P - H), __ldg(&c.twD[H]));
+    if (!(M & 1)) zb[fpad(H)] = mid_inverse(get(t, H), get(t, P - H), __ldg(&c.twD[H]));
   } else {
     Quad e;
     e.c0 = get(t, k);
@@ -457,27 +653,34 @@ __device__ __forceinline__ void dct2_inverse_b(const FftCtx& c, int nT, G get, S
   }
 }
 fft_inv_b(c, nT);
-store_b(c, nT, 1.0 / (double)M, store);
+store_b<GEN>(c, nT, 1.0 / (double)M, store);
 __syncthreads();
 }
 
+template <class G, class S>
+__device__ __forceinline__ void dct2_inverse_b(const FftCtx& c, int nT, G get, S store) {
+  dct2_inverse_b_impl<(SDFT_FFT_GEN != 0)>(c, nT, get, store);
+}
+
 // y = iDCT2(W_t .* DCT2(f_t)); W_t[q] = wgt(t, q); store(t, K, y[K])
-template <class F, class W, class S>
-__device__ __forceinline__ void dct2_convolve_b(const FftCtx& c, int nT, F f, W wgt, S store) {
+template <bool GEN, class F, class W, class S>
+__device__ __forceinline__ void dct2_convolve_b_impl(const FftCtx& c, int nT, F f, W wgt, S store) {
   const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
-  load_b(c, nT, f);
+  load_b<GEN>(c, nT, f);
   fft_fwd_b(c, nT);
   SDFT_PAIR_LOOP(c, nT)
   if (k == 0) {
     const double2 dM = __ldg(&c.twD[M]);
     double c0, cM;
     zero_forward(zb[0], dM, &c0, &cM);
-    const double2 dh = __ldg(&c.twD[H]);
-    double ch, cPh;
-    mid_forward(zb[fpad(H)], dh, &ch, &cPh);
     zb[0] = zero_inverse(c0 * wgt(t, 0), cM * wgt(t, M), dM);
-    zb[fpad(H)] = mid_inverse(ch * wgt(t, H), cPh * wgt(t, P - H), dh);
+    if (!(M & 1)) {
+      const double2 dh = __ldg(&c.twD[H]);
+      double ch, cPh;
+      mid_forward(zb[fpad(H)], dh, &ch, &cPh);
+      zb[fpad(H)] = mid_inverse(ch * wgt(t, H), cPh * wgt(t, P - H), dh);
+    }
   } else {
     const double2 wk = __ldg(&c.twP[k]), dk = __ldg(&c.twD[k]), dk2 = __ldg(&c.twD[M - k]);
     Quad q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], wk, dk, dk2);
@@ -492,29 +695,36 @@ __device__ __forceinline__ void dct2_convolve_b(const FftCtx& c, int nT, F f, W 
   }
 }
 fft_inv_b(c, nT);
-store_b(c, nT, 1.0 / (double)M, store);
+store_b<GEN>(c, nT, 1.0 / (double)M, store);
 __syncthreads();
+}
+
+template <class F, class W, class S>
+__device__ __forceinline__ void dct2_convolve_b(const FftCtx& c, int nT, F f, W wgt, S store) {
+  dct2_convolve_b_impl<(SDFT_FFT_GEN != 0)>(c, nT, f, wgt, store);
 }
 
 // the same convolution with grid-point pair functors (load_b2 / store_b2), in
 // the precision of the context (FP64, or FP32 for mixed-precision propagators)
-template <class C, class F2, class W, class A2, class S2>
-__device__ __forceinline__ void dct2_convolve_b2(const FftCtxT<C>& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
+template <bool GEN, class C, class F2, class W, class A2, class S2>
+__device__ __forceinline__ void dct2_convolve_b2_impl(const FftCtxT<C>& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
   using R = typename Cx<C>::R;
   const int P = c.P, M = c.M, H = c.H;
   __syncthreads();
-  load_b2(c, nT, f2);
+  load_b2<GEN>(c, nT, f2);
   fft_fwd_b(c, nT);
   SDFT_PAIR_LOOP(c, nT)
   if (k == 0) {
     const C dM = __ldg(&c.twD[M]);
     R c0, cM;
     zero_forward(zb[0], dM, &c0, &cM);
-    const C dh = __ldg(&c.twD[H]);
-    R ch, cPh;
-    mid_forward(zb[fpad(H)], dh, &ch, &cPh);
     zb[0] = zero_inverse(c0 * (R)wgt(t, 0), cM * (R)wgt(t, M), dM);
-    zb[fpad(H)] = mid_inverse(ch * (R)wgt(t, H), cPh * (R)wgt(t, P - H), dh);
+    if (!(M & 1)) {
+      const C dh = __ldg(&c.twD[H]);
+      R ch, cPh;
+      mid_forward(zb[fpad(H)], dh, &ch, &cPh);
+      zb[fpad(H)] = mid_inverse(ch * (R)wgt(t, H), cPh * (R)wgt(t, P - H), dh);
+    }
   } else {
     const C wk = __ldg(&c.twP[k]), dk = __ldg(&c.twD[k]), dk2 = __ldg(&c.twD[M - k]);
     QuadT<R> q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], wk, dk, dk2);
@@ -529,8 +739,13 @@ __device__ __forceinline__ void dct2_convolve_b2(const FftCtxT<C>& c, int nT, F2
   }
 }
 fft_inv_b(c, nT);
-store_b2(c, nT, (R)1 / (R)M, pre2, put2);
+store_b2<GEN>(c, nT, (R)1 / (R)M, pre2, put2);
 __syncthreads();
+}
+
+template <class C, class F2, class W, class A2, class S2>
+__device__ __forceinline__ void dct2_convolve_b2(const FftCtxT<C>& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
+  dct2_convolve_b2_impl<(SDFT_FFT_GEN != 0)>(c, nT, f2, wgt, pre2, put2);
 }
 
 #undef SDFT_PAIR_LOOP
@@ -547,4 +762,5 @@ __device__ __forceinline__ void dct2_inverse(const FftCtx& c, G get, S store) {
       c, 1, [&](int, int q) { return get(q); }, [&](int, int K, double y) { store(K, y); });
 }
 
+}  // namespace
 }  // namespace sdft

@@ -20,6 +20,7 @@
 #include "fft.cuh"
 
 namespace sdft {
+namespace {  // internal linkage: each kernel build (kernels.cuh) has its own copy
 
 struct Shared {
   double2* z;   // TB transform buffers (fft.cuh)
@@ -1760,4 +1761,5 @@ __device__ bool objective(const DReq& r, Shared sh, bool fp32 = false) {
   return true;
 }
 
+}  // namespace
 }  // namespace sdft

@@ -12,6 +12,7 @@
 #include "objective.cuh"
 
 namespace sdft {
+namespace {  // internal linkage: each kernel build (kernels.cuh) has its own copy
 
 // out[0] = Omega, out[1 + u] = N_u
 __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
@@ -114,4 +115,5 @@ __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
   __syncthreads();
 }
 
+}  // namespace
 }  // namespace sdft

@@ -1,11 +1,10 @@
-// softdft.cu -- kernels and the C ABI of include/softdft.h.
+// softdft.cu -- the C ABI of include/softdft.h (host side).
 //
-// One CTA owns one request for a whole solve (k_solve): every stage of
-// objective_dft and the Anderson update run back to back in that CTA, with the
-// FFT workspace in shared memory and the request's fields in HBM/L2.  A batch
-// is one launch with one CTA per request; requests of different sizes share the
-// launch.  The host side builds the grid fields and k-space weights of
-// setup_iDFT (src/iDFT/setup/setup_iDFT.jl:9-30) from the plain-C descriptor.
+// The kernels live in kernels.cuh (built by kernels_pow2.cu and kernels_gen.cu);
+// this file validates descriptors, lays out each request's device memory,
+// builds the grid fields and k-space weights of setup_iDFT
+// (src/iDFT/setup/setup_iDFT.jl:9-30) from the plain-C descriptor, and runs the
+// single, batched and serving solves.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,96 +16,9 @@
 #include <vector>
 
 #include "../../include/softdft.h"
-#include "anderson.cuh"
 #include "common.cuh"
-#include "objective.cuh"
-#include "omega.cuh"
 
 using namespace sdft;
-
-// ---------------------------------------------------------------------------
-// kernels
-// ---------------------------------------------------------------------------
-constexpr int kRedDoubles = 1024;
-
-__device__ __forceinline__ Shared make_shared(double* smem) {
-  Shared sh;
-  sh.red = smem;
-  sh.z = reinterpret_cast<double2*>(smem + kRedDoubles);
-  return sh;
-}
-
-struct SolveSlot {       // per-request solver state kept across launches
-  int iter;
-  int status;
-  int use_picard;
-  int pad;
-  double err;
-  unsigned long long t0, t1;  // %globaltimer (ns) at the first and the last iteration
-  double lam[kMaxAnderson];
-};
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_objective(const DReq* reqs) {
-  extern __shared__ double smem[];
-  const DReq& r = reqs[blockIdx.x];
-  Shared sh = make_shared(smem);
-  bool ok = objective(r, sh, r.prec == 1);
-  if (threadIdx.x == 0) *r.status = ok ? ST_OK : ST_NORM;
-}
-
-extern "C" __global__ void __launch_bounds__(kThreads, 3) sdft_k_solve(const DReq* reqs, SolveSlot* slots, SolveCfg cfg,
-                                                                    int max_chunk) {
-  extern __shared__ double smem[];
-  const DReq& r = reqs[blockIdx.x];
-  SolveSlot* sl = &slots[blockIdx.x];
-  Shared sh = make_shared(smem);
-  if (sl->status != ST_RUNNING) return;
-  if (threadIdx.x == 0 && sl->iter == 0) sl->t0 = global_ns();
-  AndersonState st;
-  st.use_picard = sl->use_picard;
-  for (int c = 0; c < kMaxAnderson; c++) st.lam[c] = sl->lam[c];
-  int iter = sl->iter;
-  int status = ST_RUNNING;
-  double err = sl->err;
-  for (int step = 0; step < max_chunk && iter < cfg.max_iters; step++) {
-    iter++;
-    // mixed precision: FP32 propagators while the residual is above the switch
-    if (!objective(r, sh, r.prec == 1 && err > cfg.mixed_switch)) {
-      status = ST_NORM;
-      break;
-    }
-    int s = anderson_step(r, cfg, iter, st, sh.red, &err);
-    if (s != ST_RUNNING) {
-      status = s;
-      break;
-    }
-  }
-  if (status == ST_RUNNING && iter >= cfg.max_iters) status = ST_MAX_ITERS;
-  if (threadIdx.x == 0) {
-    sl->iter = iter;
-    sl->status = status;
-    sl->use_picard = st.use_picard;
-    sl->err = err;
-    sl->t1 = global_ns();
-    for (int c = 0; c < kMaxAnderson; c++) sl->lam[c] = st.lam[c];
-    *r.status = status;
-    *r.iters = iter;
-    *r.err = err;
-  }
-}
-
-extern "C" __global__ void __launch_bounds__(kThreads) sdft_k_omega(const DReq* reqs, double* out) {
-  extern __shared__ double smem[];
-  const DReq& r = reqs[blockIdx.x];
-  Shared sh = make_shared(smem);
-  grand_potential(r, sh, out);
-}
 
 // ---------------------------------------------------------------------------
 // host side
@@ -198,6 +110,9 @@ int bond_lookup(const std::vector<int>& bonds, int a, int b) {
 // history), sdft_objective_noalloc in the library's static scratch array.
 struct Plan {
   int P = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
+  bool gen = false;              // M is not a power of two: mixed-radix FFT
+  std::vector<int> rad;          // general length: radices, M = their product
+  std::vector<int> slot;         // general length: [M] digit-reversed slot of natural index m
   long long n = 0;
   bool history = false;
   std::vector<int> bonds;
@@ -208,7 +123,7 @@ struct Plan {
   size_t o_sig = 0, o_z = 0, o_dmu = 0, o_bonds = 0, o_grp = 0, o_grp_sig = 0, o_sp = 0;
   std::vector<size_t> o_states, o_nst, o_bnd, o_md, o_gC, o_gP, o_rho, o_expo, o_bslot, o_bslot_bond, o_eslot, o_eslot_bead;
   size_t o_Ext = 0, o_tr = 0, o_Csurf = 0, o_Wbond = 0, o_Wfmt = 0, o_Wmsa = 0, o_Wcoul = 0, o_tw = 0, o_twP = 0, o_twD = 0;
-  size_t o_tw32 = 0, o_twP32 = 0, o_twD32 = 0, o_fbe32 = 0;
+  size_t o_tw32 = 0, o_twP32 = 0, o_twD32 = 0, o_fbe32 = 0, o_slot_tab = 0;
   int prec = SDFT_PREC_FP64;
   size_t o_x = 0, o_g = 0, o_lam = 0, o_rb = 0, o_rbo = 0, o_Cb = 0, o_Cbond = 0, o_Cmu = 0, o_Clng = 0;
   size_t o_wa = 0, o_wb = 0, o_wc = 0, o_wd = 0, o_fbe = 0, o_elam = 0;
@@ -221,12 +136,56 @@ struct Plan {
   std::vector<float2> tw32, twP32, twD32;
 };
 
+// radices of a general-length FFT of M points (4s, then 2, 3, 5, 7 and larger
+// primes up to kMaxGenRadix); false when M has a larger prime factor
+static bool fft_radices(int M, std::vector<int>& rad) {
+  rad.clear();
+  int m = M;
+  while (m % 4 == 0) {
+    rad.push_back(4);
+    m /= 4;
+  }
+  if (m % 2 == 0) {
+    rad.push_back(2);
+    m /= 2;
+  }
+  for (int p = 3; p <= kMaxGenRadix && m > 1; p += 2)
+    while (m % p == 0) {
+      rad.push_back(p);
+      m /= p;
+    }
+  return m == 1 && (int)rad.size() <= kMaxRadices;
+}
+
+// slot[n] = buffer position of natural index n at the input of the
+// decimation-in-time passes: n = d_0 M/r_0 + d_1 M/(r_0 r_1) + ... sits at
+// d_0 + r_0 (d_1 + r_1 (d_2 + ...))
+static void fft_digit_slots(int M, const std::vector<int>& rad, std::vector<int>& slot) {
+  slot.assign(M, 0);
+  for (int pos = 0; pos < M; pos++) {
+    int p = pos, n = 0, span = M;
+    for (int r : rad) {
+      const int dgt = p % r;
+      p /= r;
+      span /= r;
+      n += dgt * span;
+    }
+    slot[n] = pos;
+  }
+}
+
 // validation of the descriptor (the device solve's supported subset) and the
 // per-species host data
 int plan_species(const sdft_system_desc* d, Plan& pl) {
   const int P = d->np;
-  if (P < 16 || (P & (P - 1)) != 0)
-    return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP = 2^k >= 16 (got " + std::to_string(P) + ")");
+  if (P < 16 || (P & 1) != 0)
+    return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs an even NP >= 16 (got " + std::to_string(P) + ")");
+  if (!fft_radices(P / 2, pl.rad))
+    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(P) + ": NP/2 has a prime factor above " +
+                                             std::to_string(kMaxGenRadix));
+  pl.gen = (P & (P - 1)) != 0;
+  if (smem_bytes(P / 2) > kMaxSmemBytes)
+    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(P) + " needs more shared memory than a CTA has");
   if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
   if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
   if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
@@ -389,11 +348,13 @@ void plan_layout(Plan& pl, bool history) {
   pl.o_Wfmt = lay.take<double>((size_t)NB * 3 * P);
   pl.o_Wmsa = lay.take<double>((size_t)NB * P);
   pl.o_Wcoul = lay.take<double>(P);
-  pl.o_tw = lay.take<double2>(M / 2 + 1);
+  const size_t ntw = pl.gen ? (size_t)M : (size_t)(M / 2 + 1);
+  pl.o_tw = lay.take<double2>(ntw);
+  pl.o_slot_tab = pl.gen ? lay.take<int>(M) : 0;
   pl.o_twP = lay.take<double2>(M + 1);
   pl.o_twD = lay.take<double2>(M + 1);
   if (pl.prec == SDFT_PREC_MIXED) {
-    pl.o_tw32 = lay.take<float2>(M / 2 + 1);
+    pl.o_tw32 = lay.take<float2>(ntw);
     pl.o_twP32 = lay.take<float2>(M + 1);
     pl.o_twD32 = lay.take<float2>(M + 1);
     pl.o_fbe32 = lay.take<float>((size_t)4 * MB * P + 1);
@@ -494,10 +455,11 @@ void plan_tables(const sdft_system_desc* d, Plan& pl) {
   }
   for (int k = 0; k < P; k++) pl.Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
   const long double PI_L = 3.14159265358979323846264338327950288L;
-  pl.tw.resize(M / 2 + 1);
+  pl.tw.resize(pl.gen ? M : M / 2 + 1);
   pl.twP.resize(M + 1);
   pl.twD.resize(M + 1);
-  for (int k = 0; k <= M / 2; k++) pl.tw[k] = cis(-2.0L * PI_L * k / M);
+  for (size_t k = 0; k < pl.tw.size(); k++) pl.tw[k] = cis(-2.0L * PI_L * (long double)k / M);
+  if (pl.gen) fft_digit_slots(M, pl.rad, pl.slot);
   for (int k = 0; k <= M; k++) pl.twP[k] = cis(-2.0L * PI_L * k / P);
   for (int k = 0; k <= M; k++) pl.twD[k] = cis(-PI_L * k / (2.0L * P));
   if (pl.prec == SDFT_PREC_MIXED) {
@@ -579,6 +541,10 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.Wmsa = (const double*)at(pl.o_Wmsa);
   r.Wcoul = (const double*)at(pl.o_Wcoul);
   r.tw = (const double2*)at(pl.o_tw);
+  r.gen = pl.gen ? 1 : 0;
+  r.nrad = pl.gen ? (int)pl.rad.size() : 0;
+  for (int i = 0; i < r.nrad; i++) r.rad[i] = pl.rad[i];
+  r.slot = pl.gen ? (const int*)at(pl.o_slot_tab) : nullptr;
   r.twP = (const double2*)at(pl.o_twP);
   r.twD = (const double2*)at(pl.o_twD);
   const bool mixed = pl.prec == SDFT_PREC_MIXED;
@@ -645,6 +611,7 @@ cudaError_t plan_upload(const sdft_system_desc* d, const Plan& pl, char* base, c
   up(pl.o_Wmsa, pl.Wmsa.data(), sizeof(double) * pl.Wmsa.size());
   up(pl.o_Wcoul, pl.Wcoul.data(), sizeof(double) * P);
   up(pl.o_tw, pl.tw.data(), sizeof(double2) * pl.tw.size());
+  if (pl.gen) up(pl.o_slot_tab, pl.slot.data(), sizeof(int) * pl.slot.size());
   up(pl.o_twP, pl.twP.data(), sizeof(double2) * pl.twP.size());
   up(pl.o_twD, pl.twD.data(), sizeof(double2) * pl.twD.size());
   if (pl.prec == SDFT_PREC_MIXED) {
@@ -781,9 +748,27 @@ static size_t smem_bytes(int M) {
   return sizeof(double) * kRedDoubles + sizeof(double2) * (size_t)(M + M / 8) * (size_t)tb_for(M);
 }
 
-static int prepare_kernel(const void* fn, size_t smem) {
-  if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  return SDFT_OK;
+// launches of the kernel build that matches the request (power-of-two or general FFT length)
+static cudaError_t launch_objective(bool gen, const DReq* reqs, size_t smem, cudaStream_t s) {
+  return gen ? launch_objective_gen(reqs, 1, smem, s) : launch_objective_pow2(reqs, 1, smem, s);
+}
+static cudaError_t launch_omega(bool gen, const DReq* reqs, double* out, size_t smem, cudaStream_t s) {
+  return gen ? launch_omega_gen(reqs, out, smem, s) : launch_omega_pow2(reqs, out, smem, s);
+}
+// a batch: one launch of each build that has requests in it; *launches counts them
+static cudaError_t launch_solve(bool any_pow2, bool any_gen, const DReq* reqs, SolveSlot* slots, const SolveCfg& cfg,
+                                int max_chunk, int n, size_t smem, cudaStream_t s, int* launches) {
+  if (any_pow2) {
+    cudaError_t e = launch_solve_pow2(reqs, slots, cfg, max_chunk, n, smem, s);
+    if (e != cudaSuccess) return e;
+    (*launches)++;
+  }
+  if (any_gen) {
+    cudaError_t e = launch_solve_gen(reqs, slots, cfg, max_chunk, n, smem, s);
+    if (e != cudaSuccess) return e;
+    (*launches)++;
+  }
+  return cudaSuccess;
 }
 
 extern "C" int sdft_set_state(sdft_handle h, const double* mu_ex_K, const double* lng_K, const double* Psi,
@@ -821,10 +806,7 @@ extern "C" int sdft_get_state(sdft_handle h, double* mu_ex_K, double* lng_K, dou
 extern "C" int sdft_objective(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
   size_t sm = smem_bytes(h->M);
-  int rc = prepare_kernel((const void*)sdft_k_objective, sm);
-  if (rc) return rc;
-  sdft_k_objective<<<1, kThreads, sm, h->stream>>>(h->dreq);
-  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(launch_objective(h->h.gen != 0, h->dreq, sm, h->stream));
   int st = 0;
   CUDA_TRY(cudaMemcpyAsync(&st, h->h.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -856,9 +838,11 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
   if (rc) return rc;
   cudaStream_t stream = hs[0]->stream;
   size_t sm = 0;
-  for (int i = 0; i < n; i++) sm = std::max(sm, smem_bytes(hs[i]->M));
-  rc = prepare_kernel((const void*)sdft_k_solve, sm);
-  if (rc) return rc;
+  bool any_pow2 = false, any_gen = false;
+  for (int i = 0; i < n; i++) {
+    sm = std::max(sm, smem_bytes(hs[i]->M));
+    (hs[i]->h.gen ? any_gen : any_pow2) = true;
+  }
   DReq* dreqs = nullptr;
   SolveSlot* dslots = nullptr;
   CUDA_TRY(cudaMallocAsync(&dreqs, sizeof(DReq) * n, stream));
@@ -897,10 +881,8 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
   int launches = 0;
   for (;;) {
     CUDA_TRY(cudaEventRecord(ev0, stream));
-    sdft_k_solve<<<n, kThreads, sm, stream>>>(dreqs, dslots, cfg, chunk);
-    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(launch_solve(any_pow2, any_gen, dreqs, dslots, cfg, chunk, n, sm, stream, &launches));
     CUDA_TRY(cudaEventRecord(ev1, stream));
-    launches++;
     CUDA_TRY(cudaMemcpyAsync(slots.data(), dslots, sizeof(SolveSlot) * n, cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));
     float ms = 0.f;
@@ -1070,14 +1052,14 @@ extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active
   }
   int hi = 0;
   size_t sm = 0;
+  bool any_pow2 = false, any_gen = false;
   for (int i = 0; i < sv->max_slots; i++)
     if (sv->owner[i]) {
       hi = i + 1;
       sm = std::max(sm, smem_bytes(sv->owner[i]->M));
+      (sv->owner[i]->h.gen ? any_gen : any_pow2) = true;
     }
   if (hi > 0) {
-    int rc = prepare_kernel((const void*)sdft_k_solve, sm);
-    if (rc) return rc;
     CUDA_TRY(cudaMemcpyAsync(sv->dreqs, sv->hreq.data(), sizeof(DReq) * hi, cudaMemcpyHostToDevice, sv->stream));
     CUDA_TRY(cudaMemcpyAsync(sv->dslots, sv->hslot.data(), sizeof(SolveSlot) * hi, cudaMemcpyHostToDevice, sv->stream));
     SolveCfg cfg;
@@ -1088,8 +1070,8 @@ extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active
     cfg.switch_tole = sv->num.switch_tole;
     cfg.tole = sv->num.tole;
     cfg.mixed_switch = mixed_switch(&sv->num);
-    sdft_k_solve<<<hi, kThreads, sm, sv->stream>>>(sv->dreqs, sv->dslots, cfg, iters);
-    CUDA_TRY(cudaGetLastError());
+    int launched = 0;
+    CUDA_TRY(launch_solve(any_pow2, any_gen, sv->dreqs, sv->dslots, cfg, iters, hi, sm, sv->stream, &launched));
     CUDA_TRY(cudaMemcpyAsync(sv->hslot.data(), sv->dslots, sizeof(SolveSlot) * hi, cudaMemcpyDeviceToHost, sv->stream));
     CUDA_TRY(cudaStreamSynchronize(sv->stream));
     for (int i = 0; i < hi; i++) {
@@ -1151,10 +1133,7 @@ extern "C" int sdft_get_densities(sdft_handle h, double* const* rho_segments, do
 
 static int run_omega(sdft_handle h, std::vector<double>& out) {
   size_t sm = smem_bytes(h->M);
-  int rc = prepare_kernel((const void*)sdft_k_omega, sm);
-  if (rc) return rc;
-  sdft_k_omega<<<1, kThreads, sm, h->stream>>>(h->dreq, h->dout);
-  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(launch_omega(h->h.gen != 0, h->dreq, h->dout, sm, h->stream));
   out.assign(1 + h->NS, 0.0);
   CUDA_TRY(cudaMemcpyAsync(out.data(), h->dout, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1242,10 +1221,7 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
   CUDA_TRY(cudaMemsetAsync(base, 0, pl.bytes, stream));
   CUDA_TRY(plan_upload(d, pl, base, r, dsp, stream));
   size_t sm = smem_bytes(M);
-  rc = prepare_kernel((const void*)sdft_k_objective, sm);
-  if (rc) return rc;
-  sdft_k_objective<<<1, kThreads, sm, stream>>>((const DReq*)(base + pl.o_dreq));
-  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(launch_objective(pl.gen, (const DReq*)(base + pl.o_dreq), sm, stream));
   int st = 0;
   CUDA_TRY(cudaMemcpyAsync(&st, r.status, sizeof(int), cudaMemcpyDeviceToHost, stream));
   CUDA_TRY(cudaStreamSynchronize(stream));

@@ -19,6 +19,7 @@ _LIB = None
 
 SDFT_OK = 0
 SDFT_MAX_ITERS = 1
+SDFT_ERR_UNSUPPORTED = 3
 STATUS_NAMES = {0: "OK", 1: "MAX_ITERS", 2: "ERR_ARG", 3: "ERR_UNSUPPORTED", 4: "ERR_CUDA", 5: "ERR_OOM",
                 6: "ERR_NORM", 7: "ERR_NONFINITE", 8: "ERR_TIMEOUT"}
 EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_numerics_default",

@@ -50,6 +50,16 @@ CASES["grid_8192"] = small_slit(np_=8192, dz=0.02)
 CASES["grid_16384"] = small_slit(np_=16384, dz=0.02)
 # the 200-segment diblock on the 16384-point grid (one transform buffer)
 CASES["diblock_16384"] = workloads.diblock_slit(16384)
+# grids that are not powers of two: mixed-radix transforms of M = NP/2 points
+# (radices in brackets; 11 and 13 run the run-time-radix butterfly, odd M has
+# no middle coefficient pair)
+CASES["grid_1000"] = small_slit(np_=1000, dz=0.02)                 # M = 500  [4 5 5 5]
+CASES["grid_250_odd_m"] = small_slit(np_=250, dz=0.05)             # M = 125  [5 5 5]
+CASES["grid_286_radix_11_13"] = small_slit(np_=286, dz=0.05)       # M = 143  [11 13]
+CASES["grid_770_mfmt_msa"] = small_slit(np_=770, dz=0.02, models=["ideal", "mfmt", "msa"])  # M = 385 [5 7 11]
+CASES["grid_1458"] = small_slit(np_=1458, dz=0.01)                 # M = 729  [3 3 3 3 3 3]
+CASES["grid_6000"] = small_slit(np_=6000, dz=0.005)                # M = 3000 [4 2 3 5 5 5]
+CASES["brush_600"] = workloads.grafted_brush(600, 0.05, 10, 0.05, 4.5, 7.0, 0.01)  # M = 300 [4 3 5 5]
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -92,7 +102,7 @@ def test_picard_trajectory_matches():
     assert abs(eg - eo) / eo < 1e-10
 
 
-@pytest.mark.parametrize("name", ["acid_salt", "brush"])
+@pytest.mark.parametrize("name", ["acid_salt", "brush", "grid_1000", "brush_600"])
 def test_converged_state_matches(name):
     ds = copy.deepcopy(CASES[name])
     ds["numerical"]["tole"] = 1e-10
@@ -145,3 +155,28 @@ def test_max_iters_status_and_nonfinite():
     with pytest.raises(native.SdftError) as e:
         g.solve(num)
     assert e.value.code == 7
+
+
+def test_batch_mixes_grid_kinds():
+    """One batch over power-of-two and general-length requests (one launch of
+    each kernel build) gives each request the state of its own single solve."""
+    num = numerics_from_dict(dict(CASES["acid_salt"]["numerical"], max_iters=40))
+    dss = [CASES["acid_salt"], CASES["grid_250_odd_m"], CASES["grid_1000"], CASES["grid_286_radix_11_13"]]
+    singles = []
+    for ds in dss:
+        s = native.DeviceSystem(descriptor(ds).descriptor)
+        s.solve(num)
+        singles.append(s.get_x())
+    batch = [native.DeviceSystem(descriptor(ds).descriptor) for ds in dss]
+    native.solve_batch(batch, num)
+    for b, x in zip(batch, singles):
+        assert rel(b.get_x(), x) == 0.0
+
+
+@pytest.mark.parametrize("np_,why", [(1001, "even NP"), (1002, "prime factor above 61")])
+def test_unsupported_grids_are_refused(np_, why):
+    dft = descriptor(small_slit(np_=np_, dz=0.02))
+    with pytest.raises(native.SdftError) as e:
+        native.DeviceSystem(dft.descriptor)
+    assert e.value.code == native.SDFT_ERR_UNSUPPORTED
+    assert why in str(e.value)
