@@ -62,7 +62,8 @@ struct DSpecies {
 
 struct DReq {
   // sizes
-  int NP, M, L;       // grid points P, FFT length M = P/2, log2(M) (power-of-two M)
+  int NP, M, L;       // stride of per-point arrays, FFT length, log2(M) (power-of-two M)
+  int NPt;            // grid points: NP for even grids, NP - 1 for odd ones (the last point pads)
   int gen;            // 1: M is not a power of two (mixed-radix tables below)
   int nrad;           // general length: number of radices
   int rad[kMaxRadices];  // general length: radices r_0 .. r_{nrad-1}, M = their product

@@ -67,7 +67,7 @@ __device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
   c.z = z;
   c.M = r.M;
   c.L = r.L;
-  c.P = r.NP;
+  c.P = r.NPt;
   c.H = r.M >> 1;
   c.stride = r.M + (r.M >> 3);
   c.nrad = r.nrad;
@@ -85,7 +85,7 @@ __device__ __forceinline__ FftCtxT<float2> make_fft32(double2* z, const DReq& r)
   c.z = reinterpret_cast<float2*>(z);
   c.M = r.M;
   c.L = r.L;
-  c.P = r.NP;
+  c.P = r.NPt;
   c.H = r.M >> 1;
   c.stride = r.M + (r.M >> 3);
   c.nrad = r.nrad;
@@ -594,6 +594,165 @@ __device__ __forceinline__ C mid_inverse(typename Cx<C>::R eh, typename Cx<C>::R
     const int t = item_t<GEN>(it, cnt_, lH_), k = it - t * cnt_;        \
     auto* zb = (c).z + (size_t)t * (c).stride;
 
+// ---- odd P (general build) ---------------------------------------------------
+// The Makhoul sequence v[q] of an odd P is transformed by a complex FFT of
+// M = P points with zero imaginary parts, V[k] = sum_q v[q] e^{-2 pi i q k / P}.
+// Then C[0] = Re V[0], C[k] = Re(d_k V[k]) and C[P-k] = Re(d_{P-k} conj V[k])
+// with d_k = e^{-i pi k / 2P} (twD).  The inverse builds V'[0] = E[0],
+// V'[k] = conj(d_k) (E[k] - i E[P-k]), V'[P-k] = conj V'[k]; the real part of
+// the unscaled inverse FFT divided by P is v'.  The grid-point pairs (K, K+1)
+// run over the padded stride P + 1: the pad sample K + 1 = P is not loaded and
+// is stored as 0.
+__device__ __forceinline__ int makhoul_q(int K, int P) { return (K & 1) ? (P - 1 - (K >> 1)) : (K >> 1); }
+
+template <class F>
+__device__ __forceinline__ void load_b_odd(const FftCtx& c, int nT, F f) {
+  for (int it = threadIdx.x; it < nT * c.P; it += blockDim.x) {
+    const int t = it / c.P, K = it - t * c.P;
+    c.z[(size_t)t * c.stride + fpad(fslot<true>(c, makhoul_q(K, c.P)))] = make_double2(f(t, K), 0.0);
+  }
+}
+
+template <class S>
+__device__ __forceinline__ void store_b_odd(const FftCtx& c, int nT, double scale, S st) {
+  for (int it = threadIdx.x; it < nT * c.P; it += blockDim.x) {
+    const int t = it / c.P, K = it - t * c.P;
+    st(t, K, c.z[(size_t)t * c.stride + fpad(fslot<true>(c, makhoul_q(K, c.P)))].x * scale);
+  }
+}
+
+template <class C, class F2>
+__device__ __forceinline__ void load_b2_odd(const FftCtxT<C>& c, int nT, F2 f2) {
+  using R = typename Cx<C>::R;
+  const int np = (c.P + 1) >> 1;
+  for (int b = threadIdx.x; b < nT * np; b += blockDim.x) {
+    const int t = b / np, kp = b - t * np, K = 2 * kp;
+    const auto v = f2(t, K);
+    C* zb = c.z + (size_t)t * c.stride;
+    zb[fpad(fslot<true>(c, kp))] = Cx<C>::make((R)v.x, (R)0);
+    if (K + 1 < c.P) zb[fpad(fslot<true>(c, c.P - 1 - kp))] = Cx<C>::make((R)v.y, (R)0);
+  }
+}
+
+template <class C, class A2, class S2>
+__device__ __forceinline__ void store_b2_odd(const FftCtxT<C>& c, int nT, typename Cx<C>::R scale, A2 pre2, S2 put2) {
+  using R = typename Cx<C>::R;
+  const int np = (c.P + 1) >> 1;
+  for (int b = threadIdx.x; b < nT * np; b += blockDim.x) {
+    const int t = b / np, kp = b - t * np, K = 2 * kp;
+    const C* zb = c.z + (size_t)t * c.stride;
+    const R y0 = zb[fpad(fslot<true>(c, kp))].x;
+    const R y1 = (K + 1 < c.P) ? zb[fpad(fslot<true>(c, c.P - 1 - kp))].x : (R)0;
+    const auto a = pre2(t, K);
+    put2(t, K, Cx<C>::make(y0 * scale, y1 * scale), a);
+  }
+}
+
+// C[k], C[P-k] from V[k] (natural order after the forward FFT), k in [1, P/2)
+template <class C>
+__device__ __forceinline__ void odd_forward(C A, C dk, C dpk, typename Cx<C>::R* ck, typename Cx<C>::R* cpk) {
+  *ck = cmul(dk, A).x;
+  *cpk = cmul(dpk, conj2(A)).x;
+}
+template <class C>
+__device__ __forceinline__ C odd_inverse(typename Cx<C>::R ek, typename Cx<C>::R epk, C dk) {
+  return cmul(conj2(dk), Cx<C>::make(ek, -epk));
+}
+
+template <class F, class E>
+__device__ __forceinline__ void dct2_forward_odd(const FftCtx& c, int nT, F f, E emit) {
+  const int P = c.P, cnt = (P + 1) >> 1;
+  __syncthreads();
+  load_b_odd(c, nT, f);
+  fft_fwd_b(c, nT);
+  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
+    const int t = it / cnt, k = it - t * cnt;
+    const double2 A = c.z[(size_t)t * c.stride + fpad(k)];
+    if (k == 0) {
+      emit(t, 0, A.x);
+    } else {
+      double ck, cpk;
+      odd_forward(A, __ldg(&c.twD[k]), __ldg(&c.twD[P - k]), &ck, &cpk);
+      emit(t, k, ck);
+      emit(t, P - k, cpk);
+    }
+  }
+  __syncthreads();
+}
+
+template <class G, class S>
+__device__ __forceinline__ void dct2_inverse_odd(const FftCtx& c, int nT, G get, S store) {
+  const int P = c.P, cnt = (P + 1) >> 1;
+  __syncthreads();
+  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
+    const int t = it / cnt, k = it - t * cnt;
+    double2* zb = c.z + (size_t)t * c.stride;
+    if (k == 0) {
+      zb[0] = make_double2(get(t, 0), 0.0);
+    } else {
+      const double2 V = odd_inverse(get(t, k), get(t, P - k), __ldg(&c.twD[k]));
+      zb[fpad(k)] = V;
+      zb[fpad(P - k)] = conj2(V);
+    }
+  }
+  fft_inv_b(c, nT);
+  store_b_odd(c, nT, 1.0 / (double)P, store);
+  __syncthreads();
+}
+
+template <class F, class W, class S>
+__device__ __forceinline__ void dct2_convolve_odd(const FftCtx& c, int nT, F f, W wgt, S store) {
+  const int P = c.P, cnt = (P + 1) >> 1;
+  __syncthreads();
+  load_b_odd(c, nT, f);
+  fft_fwd_b(c, nT);
+  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
+    const int t = it / cnt, k = it - t * cnt;
+    double2* zb = c.z + (size_t)t * c.stride;
+    const double2 A = zb[fpad(k)];
+    if (k == 0) {
+      zb[0] = make_double2(A.x * wgt(t, 0), 0.0);
+    } else {
+      const double2 dk = __ldg(&c.twD[k]);
+      double ck, cpk;
+      odd_forward(A, dk, __ldg(&c.twD[P - k]), &ck, &cpk);
+      const double2 V = odd_inverse(ck * wgt(t, k), cpk * wgt(t, P - k), dk);
+      zb[fpad(k)] = V;
+      zb[fpad(P - k)] = conj2(V);
+    }
+  }
+  fft_inv_b(c, nT);
+  store_b_odd(c, nT, 1.0 / (double)P, store);
+  __syncthreads();
+}
+
+template <class C, class F2, class W, class A2, class S2>
+__device__ __forceinline__ void dct2_convolve_b2_odd(const FftCtxT<C>& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
+  using R = typename Cx<C>::R;
+  const int P = c.P, cnt = (P + 1) >> 1;
+  __syncthreads();
+  load_b2_odd(c, nT, f2);
+  fft_fwd_b(c, nT);
+  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
+    const int t = it / cnt, k = it - t * cnt;
+    C* zb = c.z + (size_t)t * c.stride;
+    const C A = zb[fpad(k)];
+    if (k == 0) {
+      zb[0] = Cx<C>::make(A.x * (R)wgt(t, 0), (R)0);
+    } else {
+      const C dk = __ldg(&c.twD[k]);
+      R ck, cpk;
+      odd_forward(A, dk, __ldg(&c.twD[P - k]), &ck, &cpk);
+      const C V = odd_inverse(ck * (R)wgt(t, k), cpk * (R)wgt(t, P - k), dk);
+      zb[fpad(k)] = V;
+      zb[fpad(P - k)] = conj2(V);
+    }
+  }
+  fft_inv_b(c, nT);
+  store_b2_odd(c, nT, (R)1 / (R)P, pre2, put2);
+  __syncthreads();
+}
+
 // ---- whole transforms ------------------------------------------------------
 
 // C[q] for q in [0, P): forward DCT-II of f(t, .); emit(t, q, C[q])
@@ -628,6 +787,12 @@ __syncthreads();
 
 template <class F, class E>
 __device__ __forceinline__ void dct2_forward_b(const FftCtx& c, int nT, F f, E emit) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    if (c.P & 1) {
+      dct2_forward_odd(c, nT, f, emit);
+      return;
+    }
+  }
   dct2_forward_b_impl<(SDFT_FFT_GEN != 0)>(c, nT, f, emit);
 }
 
@@ -659,6 +824,12 @@ __syncthreads();
 
 template <class G, class S>
 __device__ __forceinline__ void dct2_inverse_b(const FftCtx& c, int nT, G get, S store) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    if (c.P & 1) {
+      dct2_inverse_odd(c, nT, get, store);
+      return;
+    }
+  }
   dct2_inverse_b_impl<(SDFT_FFT_GEN != 0)>(c, nT, get, store);
 }
 
@@ -701,6 +872,12 @@ __syncthreads();
 
 template <class F, class W, class S>
 __device__ __forceinline__ void dct2_convolve_b(const FftCtx& c, int nT, F f, W wgt, S store) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    if (c.P & 1) {
+      dct2_convolve_odd(c, nT, f, wgt, store);
+      return;
+    }
+  }
   dct2_convolve_b_impl<(SDFT_FFT_GEN != 0)>(c, nT, f, wgt, store);
 }
 
@@ -745,6 +922,12 @@ __syncthreads();
 
 template <class C, class F2, class W, class A2, class S2>
 __device__ __forceinline__ void dct2_convolve_b2(const FftCtxT<C>& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    if (c.P & 1) {
+      dct2_convolve_b2_odd(c, nT, f2, wgt, pre2, put2);
+      return;
+    }
+  }
   dct2_convolve_b2_impl<(SDFT_FFT_GEN != 0)>(c, nT, f2, wgt, pre2, put2);
 }
 

@@ -76,7 +76,7 @@ __device__ void stage_bond_factors(const DReq& r, Shared sh, bool fp32) {
     const double fin = exp(-r.lambda[(size_t)j * P + K] + l / 2.0) * r.trapez[(size_t)j * P + K];
     r.fbe[idx] = fin;
     r.fbe[(size_t)nbe * P + idx] = exp(l / 2.0);
-    if (isfinite(fin)) mx = fmax(mx, fin);
+    if (K < r.NPt && isfinite(fin)) mx = fmax(mx, fin);
   }
   for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) r.elam[idx] = exp(-r.lambda[idx]);
   if (fp32 && r.fbe32) {
@@ -122,11 +122,13 @@ __device__ __forceinline__ double2 to_d2(float2 v) { return make_double2((double
 
 // fp32_bounds: the propagators feed FP32 convolutions (mixed precision) and
 // are kept in [2^-30, 2^30], so that the FP32 inputs (factors <= 1 times
-// propagator sums) stay far from the float range; FP64 keeps [2^-400, 2^400]
-__device__ int renormalise_block(double* a, int count_per_K, int P, double* red, bool fp32_bounds) {
+// propagator sums) stay far from the float range; FP64 keeps [2^-400, 2^400].
+// P is the stride, Pt the number of grid points (the maximum ignores the pad
+// point of odd grids)
+__device__ int renormalise_block(double* a, int count_per_K, int P, int Pt, double* red, bool fp32_bounds) {
   const double lo = fp32_bounds ? 0x1p-30 : 0x1p-400, hi = fp32_bounds ? 0x1p30 : 0x1p400;
   double mx = 0.0;
-  for (int K = threadIdx.x; K < P; K += blockDim.x)
+  for (int K = threadIdx.x; K < Pt; K += blockDim.x)
     for (int q = 0; q < count_per_K; q++) mx = fmax(mx, fabs(a[(size_t)q * P + K]));
   mx = block_max(mx, red);
   if (!(mx > 0.0) || !isfinite(mx)) return 0;
@@ -173,7 +175,7 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
         const double renorm = 2.0 * Dij;
         const double el = exp(lng_pi[Kp] / 2.0);
         double acc = 0.0;
-        for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+        for (int K1 = threadIdx.x; K1 < r.NPt; K1 += blockDim.x) {
           double d2 = dist2_grid(K1, Kp, r.dz);
           if (d2 <= Dij2) {
             double f = exp(-lam_j[K1] + lng_pj[K1] / 2.0);
@@ -245,7 +247,7 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
           for (int q = 0; q < S * S; q++) gC[((size_t)p * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
-    const int e = renormalise_block(gC + (size_t)p * S * S * P, S * S, P, sh.red, sizeof(R) == 4);
+    const int e = renormalise_block(gC + (size_t)p * S * S * P, S * S, P, r.NPt, sh.red, sizeof(R) == 4);
     e_child += e + sc;
     scaled |= (e + sc) != 0;
     if (threadIdx.x == 0) s.expo[p] = e_child;
@@ -305,7 +307,7 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
         double tq = 0.0;
         for (int q = 0; q < S; q++) tq += gpp[(size_t)q * P + Kp];
         const double f = exp(-r.lambda[(size_t)sj * P + Kp] + lng_pj[Kp] / 2.0) * tq;
-        for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+        for (int K1 = threadIdx.x; K1 < r.NPt; K1 += blockDim.x) {
           double d2 = dist2_grid(K1, Kp, r.dz);
           if (d2 <= Dij2) {
             double v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm / s.normative;
@@ -364,7 +366,7 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
           for (int q = 0; q < S * S; q++) gP[((size_t)c * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
-    const int e = renormalise_block(gP + (size_t)c * S * S * P, S * S, P, sh.red, sizeof(R) == 4);
+    const int e = renormalise_block(gP + (size_t)c * S * S * P, S * S, P, r.NPt, sh.red, sizeof(R) == 4);
     e_parent += e + sc;
     scaled |= (e + sc) != 0;
     if (threadIdx.x == 0) s.expo[N + c] = e_parent;
@@ -385,7 +387,7 @@ __device__ bool chain_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_o
     s.mu_species = 0.0;
     const int parent = 1;  // first free segment
     double acc = 0.0;
-    for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    for (int K = threadIdx.x; K < r.NPt; K += blockDim.x) {
       for (int ii = 0; ii < s.nst[parent]; ii++) {
         const int si = s.states[parent * S + ii];
         double sp = 0.0;
@@ -1470,9 +1472,9 @@ __device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
 constexpr int kGammaLanes = 4;
 
 __device__ __noinline__ void msa_gamma_pass(const DReq& r, double* out) {
-  const int P = r.NP, nb = r.NB;
+  const int P = r.NP, Pt = r.NPt, nb = r.NB;  // stride, grid points
   if (r.ngrp != 1) {
-    for (int K = threadIdx.x; K < P; K += blockDim.x) {
+    for (int K = threadIdx.x; K < Pt; K += blockDim.x) {
       double rho[kMaxBeads];
       for (int j = 0; j < nb; j++) rho[j] = r.wa[(size_t)j * P + K];
       const MsaGamma gm = gamma_msa_point(r, rho);
@@ -1485,7 +1487,7 @@ __device__ __noinline__ void msa_gamma_pass(const DReq& r, double* out) {
   }
   const double lB = r.lB, tol = 1e-10, sg = r.grp_sig[0];
   const int bd = blockDim.x;
-  for (int K0 = threadIdx.x; K0 < P; K0 += kGammaLanes * bd) {
+  for (int K0 = threadIdx.x; K0 < Pt; K0 += kGammaLanes * bd) {
     double G[kGammaLanes], eta[kGammaLanes], H[kGammaLanes], cg[kGammaLanes], bg[kGammaLanes], ag[kGammaLanes],
         term2[kGammaLanes];
     bool live[kGammaLanes];
@@ -1495,7 +1497,7 @@ __device__ __noinline__ void msa_gamma_pass(const DReq& r, double* out) {
       live[u] = false;
       G[u] = eta[u] = H[u] = 0.0;
       cg[u] = bg[u] = ag[u] = term2[u] = 0.0;
-      if (K >= P) continue;
+      if (K >= Pt) continue;
       double s = 0.0, sr = 0.0, srs = 0.0, s3 = 0.0;
       for (int j = 0; j < nb; j++) {
         const double rj = r.wa[(size_t)j * P + K], zj = r.z[j], sj = r.sig[j];
@@ -1543,7 +1545,7 @@ __device__ __noinline__ void msa_gamma_pass(const DReq& r, double* out) {
 #pragma unroll
     for (int u = 0; u < kGammaLanes; u++) {
       const int K = K0 + u * bd;
-      if (K < P) {
+      if (K < Pt) {
         out[K] = G[u];
         out[(size_t)P + K] = eta[u];
         out[(size_t)2 * P + K] = H[u];
@@ -1668,7 +1670,7 @@ __device__ double stage_neutrality(const DReq& r, Shared sh) {
         if (g == 0 && s.fixed >= 0) {
           if (threadIdx.x == 0) nn = rs[s.fixed];
         } else {
-          for (int K = threadIdx.x; K < P; K += blockDim.x) nn += rs[K] * r.trapez[(size_t)st * P + K] * r.dz;
+          for (int K = threadIdx.x; K < r.NPt; K += blockDim.x) nn += rs[K] * r.trapez[(size_t)st * P + K] * r.dz;
         }
         part[2 * u] += nn;
         part[2 * u + 1] += nn * r.z[st];
@@ -1757,6 +1759,9 @@ __device__ bool objective(const DReq& r, Shared sh, bool fp32 = false) {
   }
   const double shift = stage_neutrality(r, sh);
   if (threadIdx.x == 0) g[off_psic(r)] = r.x[off_psic(r)] + shift;
+  // the pad point of odd grids is not an unknown: G(x) keeps it at 0 there, as x does
+  if (r.NPt != P)
+    for (int w = threadIdx.x; w < nout; w += blockDim.x) g[(size_t)w * P + r.NPt] = 0.0;
   __syncthreads();
   return true;
 }

@@ -110,6 +110,8 @@ int bond_lookup(const std::vector<int>& bonds, int a, int b) {
 // history), sdft_objective_noalloc in the library's static scratch array.
 struct Plan {
   int P = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
+  int Pt = 0;                    // grid points; P is the stride of per-point arrays (Pt + 1 for odd Pt)
+  long long n_caller = 0;        // unknowns in the caller's layout (rows of Pt points)
   bool gen = false;              // M is not a power of two: mixed-radix FFT
   std::vector<int> rad;          // general length: radices, M = their product
   std::vector<int> slot;         // general length: [M] digit-reversed slot of natural index m
@@ -177,28 +179,35 @@ static void fft_digit_slots(int M, const std::vector<int>& rad, std::vector<int>
 // validation of the descriptor (the device solve's supported subset) and the
 // per-species host data
 int plan_species(const sdft_system_desc* d, Plan& pl) {
-  const int P = d->np;
-  if (P < 16 || (P & 1) != 0)
-    return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs an even NP >= 16 (got " + std::to_string(P) + ")");
-  if (!fft_radices(P / 2, pl.rad))
-    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(P) + ": NP/2 has a prime factor above " +
-                                             std::to_string(kMaxGenRadix));
-  pl.gen = (P & (P - 1)) != 0;
-  if (smem_bytes(P / 2) > kMaxSmemBytes)
-    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(P) + " needs more shared memory than a CTA has");
+  // even NP: the DCT runs through a complex FFT of NP/2 points; odd NP: through
+  // one of NP points on real data, with every per-point device array padded to
+  // the even stride NP + 1 (the pad point lies beyond the grid)
+  const int Pt = d->np;
+  if (Pt < 16) return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP >= 16 (got " + std::to_string(Pt) + ")");
+  const bool odd = (Pt & 1) != 0;
+  const int P = odd ? Pt + 1 : Pt;
+  const int Mf = odd ? Pt : Pt / 2;
+  if (!fft_radices(Mf, pl.rad))
+    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(Pt) + ": " + (odd ? "NP" : "NP/2") +
+                                             " has a prime factor above " + std::to_string(kMaxGenRadix));
+  pl.gen = (Mf & (Mf - 1)) != 0;
+  if (smem_bytes(Mf) > kMaxSmemBytes)
+    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(Pt) + " needs more shared memory than a CTA has");
   if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
   if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
   if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
   if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
   if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
   pl.P = P;
-  pl.M = P / 2;
+  pl.Pt = Pt;
+  pl.M = Mf;
   pl.L = 0;
   while ((1 << pl.L) < pl.M) pl.L++;
   pl.NB = d->nb;
   pl.MB = d->mb;
   pl.NS = d->n_species;
   pl.n = (long long)P * (pl.NB + 2 * pl.MB + 1) + 1;
+  pl.n_caller = (long long)Pt * (pl.NB + 2 * pl.MB + 1) + 1;
   pl.bonds.assign(d->bond_types, d->bond_types + 2 * pl.MB);
   const int NB = pl.NB;
   for (int u = 0; u < pl.NS; u++) {
@@ -222,7 +231,7 @@ int plan_species(const sdft_system_desc* d, Plan& pl) {
       h.fixed = s.fixed_coord[0];
     }
     if (h.fixed >= 0) {
-      if (h.fixed >= P || h.n_seg < 2 || !s.max_distance)
+      if (h.fixed >= Pt || h.n_seg < 2 || !s.max_distance)
         return set_err(SDFT_ERR_ARG, "fixed segment needs a grid point, a free segment and max_distance");
       if (h.n_seg == 2 && h.nst[1] > 1) return set_err(SDFT_ERR_UNSUPPORTED, "grafted dimer with a multi-state free segment");
       h.md.resize(h.n_seg);
@@ -394,11 +403,16 @@ void plan_layout(Plan& pl, bool history) {
 }
 
 void plan_tables(const sdft_system_desc* d, Plan& pl) {
-  const int P = pl.P, NB = pl.NB, MB = pl.MB, M = pl.M, NPS = 2 * P;
+  const int P = pl.P, Pt = pl.Pt, NB = pl.NB, MB = pl.MB, M = pl.M, NPS = 2 * Pt;
   pl.Ext.assign((size_t)NB * P, 0.0);
   pl.tr.assign((size_t)NB * P, 1.0);
+  if (P != Pt)  // the pad point of odd grids: excluded and unweighted
+    for (int j = 0; j < NB; j++) {
+      pl.Ext[(size_t)j * P + Pt] = 1.0e20;
+      pl.tr[(size_t)j * P + Pt] = 0.0;
+    }
   if (d->hard_walls) {  // hard_walls.jl:6-46
-    for (int K = 0; K < P; K++) {
+    for (int K = 0; K < Pt; K++) {
       int idx = K + 1;
       for (int j = 0; j < NB; j++) {
         double dd = d->diameter[j];
@@ -420,18 +434,18 @@ void plan_tables(const sdft_system_desc* d, Plan& pl) {
       }
     }
   }
-  std::vector<double> surf(P, 0.0);
+  std::vector<double> surf(Pt, 0.0);
   pl.Csurf.assign(P, 0.0);
   if (d->charged_walls) {  // charged_walls.jl:7-57
     double pos[2] = {0.0, d->length};
     for (int w = 0; w < 2; w++) {
       int gp = jround(pos[w] / d->bin_width) + 1;
-      if (gp >= 1 && gp <= P) surf[gp - 1] += d->wall_charge[w] * (1.0 / d->bin_width);
+      if (gp >= 1 && gp <= Pt) surf[gp - 1] += d->wall_charge[w] * (1.0 / d->bin_width);
     }
-    for (int k = 0; k < P; k++) {
+    for (int k = 0; k < Pt; k++) {
       long double acc = 0.0L;
-      for (int K = 0; K < P; K++)
-        if (surf[K] != 0.0) acc += (long double)surf[K] * cosl(3.14159265358979323846264338327950288L * k * (2 * K + 1) / (2.0L * P));
+      for (int K = 0; K < Pt; K++)
+        if (surf[K] != 0.0) acc += (long double)surf[K] * cosl(3.14159265358979323846264338327950288L * k * (2 * K + 1) / (2.0L * Pt));
       pl.Csurf[k] = (double)acc;
     }
   }
@@ -441,27 +455,27 @@ void plan_tables(const sdft_system_desc* d, Plan& pl) {
   pl.Wcoul.assign(P, 0.0);
   for (int u = 0; u < MB; u++) {
     double sij = (d->diameter[pl.bonds[2 * u]] + d->diameter[pl.bonds[2 * u + 1]]) / 2.0;
-    for (int k = 0; k < P; k++)
+    for (int k = 0; k < Pt; k++)
       pl.Wbond[(size_t)u * P + k] = filter_k(k, NPS, d->bin_width) * (w_delta(k, NPS, d->bin_width, sij) / (4.0 * kPi * (sij * sij)));
   }
   for (int j = 0; j < NB; j++) {
     double b = d->diameter[j] / 2.0;
-    for (int k = 0; k < P; k++) {
+    for (int k = 0; k < Pt; k++) {
       pl.Wfmt[((size_t)j * 3 + 0) * P + k] = w_delta(k, NPS, d->bin_width, b);
       pl.Wfmt[((size_t)j * 3 + 1) * P + k] = w_step(k, NPS, d->bin_width, b);
       pl.Wfmt[((size_t)j * 3 + 2) * P + k] = w_vec(k, NPS, d->bin_width, b);
       pl.Wmsa[(size_t)j * P + k] = w_delta(k, NPS, d->bin_width, b) / (4.0 * kPi * (b * b));
     }
   }
-  for (int k = 0; k < P; k++) pl.Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
+  for (int k = 0; k < Pt; k++) pl.Wcoul[k] = w_coul(k, NPS, d->bin_width, d->bjerrum_length);
   const long double PI_L = 3.14159265358979323846264338327950288L;
   pl.tw.resize(pl.gen ? M : M / 2 + 1);
   pl.twP.resize(M + 1);
   pl.twD.resize(M + 1);
   for (size_t k = 0; k < pl.tw.size(); k++) pl.tw[k] = cis(-2.0L * PI_L * (long double)k / M);
   if (pl.gen) fft_digit_slots(M, pl.rad, pl.slot);
-  for (int k = 0; k <= M; k++) pl.twP[k] = cis(-2.0L * PI_L * k / P);
-  for (int k = 0; k <= M; k++) pl.twD[k] = cis(-PI_L * k / (2.0L * P));
+  for (int k = 0; k <= M; k++) pl.twP[k] = cis(-2.0L * PI_L * k / Pt);
+  for (int k = 0; k <= M; k++) pl.twD[k] = cis(-PI_L * k / (2.0L * Pt));
   if (pl.prec == SDFT_PREC_MIXED) {
     auto f2 = [](double2 v) { return make_float2((float)v.x, (float)v.y); };
     pl.tw32.resize(pl.tw.size());
@@ -474,10 +488,10 @@ void plan_tables(const sdft_system_desc* d, Plan& pl) {
   if (pl.history) {
     pl.x0.assign(pl.n, 0.0);
     for (int j = 0; j < NB; j++)
-      for (int K = 0; K < P; K++) pl.x0[(size_t)j * P + K] = d->mu_ex_bulk[j];
+      for (int K = 0; K < Pt; K++) pl.x0[(size_t)j * P + K] = d->mu_ex_bulk[j];
     for (int u = 0; u < MB; u++)
       for (int e2 = 0; e2 < 2; e2++)
-        for (int K = 0; K < P; K++) pl.x0[(size_t)P * NB + (size_t)(u * 2 + e2) * P + K] = d->lng_bulk[u];
+        for (int K = 0; K < Pt; K++) pl.x0[(size_t)P * NB + (size_t)(u * 2 + e2) * P + K] = d->lng_bulk[u];
   }
 }
 
@@ -513,6 +527,7 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   }
   DReq r{};
   r.NP = pl.P;
+  r.NPt = pl.Pt;
   r.M = pl.M;
   r.L = pl.L;
   r.NB = pl.NB;
@@ -631,7 +646,9 @@ struct sdft_request {
   cudaStream_t stream = nullptr;
   int precision = SDFT_PREC_FP64;
   int NP = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
+  int NPt = 0;            // grid points (NP: stride of the device arrays)
   long long n = 0;
+  long long n_caller = 0;  // unknowns in the caller's layout
   std::vector<SpeciesHost> sp;
   char* dmem = nullptr;
   size_t bytes = 0;
@@ -682,6 +699,8 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
   cudaGetDevice(&q->device);
   q->precision = precision;
   q->NP = pl.P;
+  q->NPt = pl.Pt;
+  q->n_caller = pl.n_caller;
   q->M = pl.M;
   q->L = pl.L;
   q->NB = pl.NB;
@@ -730,7 +749,7 @@ extern "C" int sdft_request_destroy(sdft_handle h) {
 
 extern "C" int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* device_bytes) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
-  if (n_unknowns) *n_unknowns = h->n;
+  if (n_unknowns) *n_unknowns = h->n_caller;
   if (device_bytes) *device_bytes = (int64_t)h->bytes;
   return SDFT_OK;
 }
@@ -771,15 +790,25 @@ static cudaError_t launch_solve(bool any_pow2, bool any_gen, const DReq* reqs, S
   return cudaSuccess;
 }
 
+// `rows` fields of NPt points between the caller's packed layout and the device
+// layout of stride NP (equal for even grids; the pad point of odd grids is not copied)
+static cudaError_t rows_copy(const sdft_request* h, double* dst, const double* src, size_t rows, cudaMemcpyKind kind) {
+  const size_t Pt = h->NPt, P = h->NP;
+  if (P == Pt) return cudaMemcpyAsync(dst, src, sizeof(double) * P * rows, kind, h->stream);
+  const bool to_dev = kind == cudaMemcpyHostToDevice;
+  return cudaMemcpy2DAsync(dst, sizeof(double) * (to_dev ? P : Pt), src, sizeof(double) * (to_dev ? Pt : P),
+                           sizeof(double) * Pt, rows, kind, h->stream);
+}
+
 extern "C" int sdft_set_state(sdft_handle h, const double* mu_ex_K, const double* lng_K, const double* Psi,
                               const double* PsiC) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
   const size_t P = h->NP;
   double* x = h->h.x;
-  if (mu_ex_K) CUDA_TRY(cudaMemcpyAsync(x, mu_ex_K, sizeof(double) * P * h->NB, cudaMemcpyHostToDevice, h->stream));
-  if (lng_K && h->MB)
-    CUDA_TRY(cudaMemcpyAsync(x + P * h->NB, lng_K, sizeof(double) * P * 2 * h->MB, cudaMemcpyHostToDevice, h->stream));
-  if (Psi) CUDA_TRY(cudaMemcpyAsync(x + P * (h->NB + 2 * h->MB), Psi, sizeof(double) * P, cudaMemcpyHostToDevice, h->stream));
+  const cudaMemcpyKind H2D = cudaMemcpyHostToDevice;
+  if (mu_ex_K) CUDA_TRY(rows_copy(h, x, mu_ex_K, h->NB, H2D));
+  if (lng_K && h->MB) CUDA_TRY(rows_copy(h, x + P * h->NB, lng_K, 2 * h->MB, H2D));
+  if (Psi) CUDA_TRY(rows_copy(h, x + P * (h->NB + 2 * h->MB), Psi, 1, H2D));
   if (PsiC)
     CUDA_TRY(cudaMemcpyAsync(x + P * (h->NB + 2 * h->MB + 1), PsiC, sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -788,10 +817,10 @@ extern "C" int sdft_set_state(sdft_handle h, const double* mu_ex_K, const double
 
 static int copy_vec_out(sdft_handle h, const double* dv, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
   const size_t P = h->NP;
-  if (mu_ex_K) CUDA_TRY(cudaMemcpyAsync(mu_ex_K, dv, sizeof(double) * P * h->NB, cudaMemcpyDeviceToHost, h->stream));
-  if (lng_K && h->MB)
-    CUDA_TRY(cudaMemcpyAsync(lng_K, dv + P * h->NB, sizeof(double) * P * 2 * h->MB, cudaMemcpyDeviceToHost, h->stream));
-  if (Psi) CUDA_TRY(cudaMemcpyAsync(Psi, dv + P * (h->NB + 2 * h->MB), sizeof(double) * P, cudaMemcpyDeviceToHost, h->stream));
+  const cudaMemcpyKind D2H = cudaMemcpyDeviceToHost;
+  if (mu_ex_K) CUDA_TRY(rows_copy(h, mu_ex_K, dv, h->NB, D2H));
+  if (lng_K && h->MB) CUDA_TRY(rows_copy(h, lng_K, dv + P * h->NB, 2 * h->MB, D2H));
+  if (Psi) CUDA_TRY(rows_copy(h, Psi, dv + P * (h->NB + 2 * h->MB), 1, D2H));
   if (PsiC)
     CUDA_TRY(cudaMemcpyAsync(PsiC, dv + P * (h->NB + 2 * h->MB + 1), sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1121,12 +1150,10 @@ extern "C" int sdft_get_densities(sdft_handle h, double* const* rho_segments, do
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     for (int u = 0; u < h->NS; u++)
       if (rho_segments[u])
-        CUDA_TRY(cudaMemcpyAsync(rho_segments[u], dsp[u].rho_seg, sizeof(double) * P * h->sp[u].S * h->sp[u].n_seg,
-                                 cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(rows_copy(h, rho_segments[u], dsp[u].rho_seg, (size_t)h->sp[u].S * h->sp[u].n_seg, cudaMemcpyDeviceToHost));
   }
-  if (rho_beads_K) CUDA_TRY(cudaMemcpyAsync(rho_beads_K, h->h.rho_beads, sizeof(double) * P * h->NB, cudaMemcpyDeviceToHost, h->stream));
-  if (rho_bonds_K && h->MB)
-    CUDA_TRY(cudaMemcpyAsync(rho_bonds_K, h->h.rho_bonds, sizeof(double) * P * 2 * h->MB, cudaMemcpyDeviceToHost, h->stream));
+  if (rho_beads_K) CUDA_TRY(rows_copy(h, rho_beads_K, h->h.rho_beads, h->NB, cudaMemcpyDeviceToHost));
+  if (rho_bonds_K && h->MB) CUDA_TRY(rows_copy(h, rho_bonds_K, h->h.rho_bonds, 2 * h->MB, cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   return SDFT_OK;
 }
@@ -1203,6 +1230,8 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
   Plan pl;
   int rc = plan_species(d, pl);
   if (rc) return rc;
+  if (pl.P != pl.Pt)  // x and G(x) are the caller's arrays in the packed layout
+    return set_err(SDFT_ERR_UNSUPPORTED, "sdft_objective_noalloc needs an even NP (got " + std::to_string(pl.Pt) + ")");
   // layout inside the scratch array (no Anderson history: G(x) only)
   plan_layout(pl, false);
   if (pl.bytes > (size_t)SDFT_NOALLOC_SCRATCH_BYTES)

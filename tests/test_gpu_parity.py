@@ -60,6 +60,21 @@ CASES["grid_770_mfmt_msa"] = small_slit(np_=770, dz=0.02, models=["ideal", "mfmt
 CASES["grid_1458"] = small_slit(np_=1458, dz=0.01)                 # M = 729  [3 3 3 3 3 3]
 CASES["grid_6000"] = small_slit(np_=6000, dz=0.005)                # M = 3000 [4 2 3 5 5 5]
 CASES["brush_600"] = workloads.grafted_brush(600, 0.05, 10, 0.05, 4.5, 7.0, 0.01)  # M = 300 [4 3 5 5]
+# odd grids: a complex FFT of M = NP points on real data, device arrays padded
+# to the stride NP + 1 (H = 20 sigma at dz = 0.02 gives the reference NP = 1001)
+CASES["grid_1001"] = small_slit(np_=1001, dz=0.02)                 # M = 1001 [7 11 13]
+CASES["grid_125_mfmt_msa"] = small_slit(np_=125, dz=0.05, models=["ideal", "mfmt", "msa"])  # M = 125 [5 5 5]
+CASES["charged_walls_1001"] = small_slit(np_=1001, dz=0.02, wall_charge=-0.05)
+CASES["brush_999"] = workloads.grafted_brush(999, 0.05, 10, 0.05, 4.5, 7.0, 0.01)  # M = 999 [3 3 3 37]
+
+
+def _diblock_odd():
+    ds = workloads.diblock_slit(1001)
+    ds["species"][0]["sequence"] = "A" * 6 + "C" * 6
+    return ds
+
+
+CASES["diblock_1001"] = _diblock_odd()
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -102,7 +117,7 @@ def test_picard_trajectory_matches():
     assert abs(eg - eo) / eo < 1e-10
 
 
-@pytest.mark.parametrize("name", ["acid_salt", "brush", "grid_1000", "brush_600"])
+@pytest.mark.parametrize("name", ["acid_salt", "brush", "grid_1000", "brush_600", "grid_1001", "brush_999"])
 def test_converged_state_matches(name):
     ds = copy.deepcopy(CASES[name])
     ds["numerical"]["tole"] = 1e-10
@@ -161,7 +176,8 @@ def test_batch_mixes_grid_kinds():
     """One batch over power-of-two and general-length requests (one launch of
     each kernel build) gives each request the state of its own single solve."""
     num = numerics_from_dict(dict(CASES["acid_salt"]["numerical"], max_iters=40))
-    dss = [CASES["acid_salt"], CASES["grid_250_odd_m"], CASES["grid_1000"], CASES["grid_286_radix_11_13"]]
+    dss = [CASES["acid_salt"], CASES["grid_250_odd_m"], CASES["grid_1000"], CASES["grid_286_radix_11_13"],
+           CASES["grid_1001"]]
     singles = []
     for ds in dss:
         s = native.DeviceSystem(descriptor(ds).descriptor)
@@ -173,7 +189,8 @@ def test_batch_mixes_grid_kinds():
         assert rel(b.get_x(), x) == 0.0
 
 
-@pytest.mark.parametrize("np_,why", [(1001, "even NP"), (1002, "prime factor above 61")])
+@pytest.mark.parametrize("np_,why", [(1009, "NP has a prime factor above 61"),
+                                     (1002, "NP/2 has a prime factor above 61")])
 def test_unsupported_grids_are_refused(np_, why):
     dft = descriptor(small_slit(np_=np_, dz=0.02))
     with pytest.raises(native.SdftError) as e:
