@@ -1167,7 +1167,7 @@ __device__ void fmt_weighted(const DReq& r, Shared sh, bool tpt1) {
         fc, nT,
         [&](int t, int q) {
           if (q == 0) return 0.0;
-          const int k = P - q;
+          const int k = r.NPt - q;  // coefficient reversal over the grid points (not the stride)
           double s = 0.0;
           for (int j = 0; j < NB; j++) {
             double c = r.Cb[(size_t)j * P + k] * r.Wfmt[((size_t)j * 3 + 2) * P + k];
@@ -1264,7 +1264,7 @@ __device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
         [&](int t, int k, double v) {
           const int q = g0 + t;
           if (q < 4) CD[(size_t)q * P + k] = v;
-          else if (k > 0) CD[(size_t)q * P + (P - k)] = v;
+          else if (k > 0) CD[(size_t)q * P + (r.NPt - k)] = v;
         });
   }
   // mu_ex coefficients (accumulate_mu_ex!, TPT1mfmt.jl:244-283)
