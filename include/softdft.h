@@ -130,6 +130,13 @@ int sdft_request_create(const sdft_system_desc* desc, int32_t precision, sdft_ha
 int sdft_request_destroy(sdft_handle h);
 /* sizes: n = NP*(NB + 2*MB + 1) + 1 (Anderson vector length) */
 int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* device_bytes);
+/* SDFT_OK when the device solve runs a grid of np points, else
+ * SDFT_ERR_UNSUPPORTED with the reason in sdft_last_error().  No reference
+ * counterpart (FFTW plans any length): the device transform takes np >= 16
+ * whose FFT length (np/2 for even np, np for odd np) has no prime factor above
+ * 61 and fits one CTA's shared memory (an FFT length of at most 12459 points).
+ * Host-only: needs no GPU. */
+int sdft_grid_supported(int32_t np);
 
 /* Unknowns x = (mu_ex_K, lng_K, Psi, PsiC), solver_dft.jl:13 */
 int sdft_set_state(sdft_handle h, const double* mu_ex_K, const double* lng_K,

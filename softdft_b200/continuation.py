@@ -25,11 +25,13 @@ from the same wall (linear interpolation; the previous slit's midpoint value
 beyond its half width).  With an unchanged grid spacing and a change of H by
 whole grid spacings this is the routines' index copy of the near-wall halves.
 
-Grid.  The device transform needs NP = 2^k.  When `pow2` is set (the default)
-a step with wall separation H keeps the requested spacing as an upper bound:
-NP is the smallest power of two with NP >= cld(H, dz) + 1 and the spacing is
-H / (NP - 1) (nudged so that the reference's rule NP = cld(H, dz) + 1 gives
-exactly NP).
+Grid.  A step with wall separation H and requested spacing dz uses the
+reference's grid NP = cld(H, dz) + 1 whenever the device transform runs it
+(native.grid_supported: NP >= 16 whose FFT length has no prime factor above 61
+and fits one CTA's shared memory); otherwise the spacing is an upper bound and
+NP is the next supported size, at spacing H / (NP - 1) (nudged so that the
+reference's rule gives exactly NP).  `grid="pow2"` keeps the earlier policy of
+power-of-two grids, `grid="exact"` the requested spacing as is.
 """
 from __future__ import annotations
 
@@ -61,15 +63,44 @@ def pow2_bin_width(H: float, dz: float) -> float:
     return w
 
 
-def set_distance(data: dict, H: float, dz: Optional[float] = None, pow2: bool = True) -> None:
-    """Wall separation H in place (data["geometry"]["dimensions"] = [H])."""
+def _width_for(H: float, dz: float, NP: int) -> float:
+    """Spacing near H / (NP - 1) for which NP = cld(H, spacing) + 1 exactly."""
+    w = H / (NP - 1)
+    while cld(H, w) + 1 > NP:
+        w = math.nextafter(w, math.inf)
+    while cld(H, w) + 1 < NP:
+        w = math.nextafter(w, 0.0)
+    return w
+
+
+def supported_bin_width(H: float, dz: float) -> float:
+    """dz when the device runs the reference's grid cld(H, dz) + 1, else the
+    spacing < dz of the next grid size the device runs."""
+    NP = cld(H, dz) + 1
+    if native.grid_supported(NP):
+        return dz
+    NP = max(NP, 16)
+    while not native.grid_supported(NP):
+        NP += 1
+        if NP > 1 << 16:
+            raise ValueError(f"no device grid for H = {H} at spacing <= {dz}")
+    return _width_for(H, dz, NP)
+
+
+def set_distance(data: dict, H: float, dz: Optional[float] = None, grid: str = "device") -> None:
+    """Wall separation H in place (data["geometry"]["dimensions"] = [H]); the
+    spacing follows `grid` ("device", "pow2" or "exact", see the module text)."""
     g = data["geometry"]
     g["dimensions"] = [H]
-    if pow2:
-        base = float(dz if dz is not None else g["bin_width"][0])
+    base = float(dz if dz is not None else g["bin_width"][0])
+    if grid == "device":
+        g["bin_width"] = [supported_bin_width(H, base)]
+    elif grid == "pow2":
         g["bin_width"] = [pow2_bin_width(H, base)]
-    elif dz is not None:
-        g["bin_width"] = [dz]
+    elif grid == "exact":
+        g["bin_width"] = [base]
+    else:
+        raise ValueError(f"grid must be 'device', 'pow2' or 'exact' (got {grid!r})")
 
 
 def _resample(f: np.ndarray, np_old: int, dz_old: float, np_new: int, dz_new: float) -> np.ndarray:
@@ -117,7 +148,7 @@ def _fmt_dir(prefix: str, v: float, digits: int = 2) -> str:
 
 
 def adjust_distancesZ(data: dict, startZ: float = 1.6, stopZ: float = 20.0, stepZ: float = 0.02, errP: float = 1e-6,
-                      out_root: Optional[str] = "dist_sweep", dz: Optional[float] = None, pow2: bool = True,
+                      out_root: Optional[str] = "dist_sweep", dz: Optional[float] = None, grid: str = "device",
                       max_count: int = 20) -> List[dict]:
     """routines/adjust_distanceZ.jl:15-155 (files under out_root when given)."""
     data = copy.deepcopy(data)
@@ -130,7 +161,7 @@ def adjust_distancesZ(data: dict, startZ: float = 1.6, stopZ: float = 20.0, step
     while count < max_count:
         distance += stepZ
         i += 1
-        set_distance(data, distance, dz, pow2)
+        set_distance(data, distance, dz, grid)
         geom = geometry_system(data)
         dft = setup_iDFT(data, bulk, geom)
         step_dir = None
@@ -267,7 +298,7 @@ def adjust_pH(data: dict, startZ: float = 3.0, stopZ: float = 10.0, stepZ: float
 # ---- batched branches -----------------------------------------------------------
 
 def batched_distance_sweep(branches: Sequence[dict], distances: Sequence[float], dz: Optional[float] = None,
-                           pow2: bool = True, num=None) -> List[List[dict]]:
+                           grid: str = "device", num=None) -> List[List[dict]]:
     """Wall-separation sweep of independent branches (input datasets, one per
     branch, sharing the numerics): at every distance all branches are solved in
     one batched launch, each starting from its own previous solution.  Returns
@@ -281,7 +312,7 @@ def batched_distance_sweep(branches: Sequence[dict], distances: Sequence[float],
     for step, H in enumerate(distances, start=1):
         dfts = []
         for b, d in enumerate(datas):
-            set_distance(d, H, dz, pow2)
+            set_distance(d, H, dz, grid)
             geom = geometry_system(d)
             dft = setup_iDFT(d, bulks[b], geom)
             if prev[b] is not None:

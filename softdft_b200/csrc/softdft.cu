@@ -178,11 +178,10 @@ static void fft_digit_slots(int M, const std::vector<int>& rad, std::vector<int>
 
 // validation of the descriptor (the device solve's supported subset) and the
 // per-species host data
-int plan_species(const sdft_system_desc* d, Plan& pl) {
-  // even NP: the DCT runs through a complex FFT of NP/2 points; odd NP: through
-  // one of NP points on real data, with every per-point device array padded to
-  // the even stride NP + 1 (the pad point lies beyond the grid)
-  const int Pt = d->np;
+// grid size: even NP runs the DCT through a complex FFT of NP/2 points, odd NP
+// through one of NP points on real data, with every per-point device array
+// padded to the even stride NP + 1 (the pad point lies beyond the grid)
+static int plan_grid(int Pt, Plan& pl) {
   if (Pt < 16) return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP >= 16 (got " + std::to_string(Pt) + ")");
   const bool odd = (Pt & 1) != 0;
   const int P = odd ? Pt + 1 : Pt;
@@ -193,16 +192,23 @@ int plan_species(const sdft_system_desc* d, Plan& pl) {
   pl.gen = (Mf & (Mf - 1)) != 0;
   if (smem_bytes(Mf) > kMaxSmemBytes)
     return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(Pt) + " needs more shared memory than a CTA has");
-  if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
-  if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
-  if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
-  if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
-  if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
   pl.P = P;
   pl.Pt = Pt;
   pl.M = Mf;
   pl.L = 0;
   while ((1 << pl.L) < pl.M) pl.L++;
+  return SDFT_OK;
+}
+
+int plan_species(const sdft_system_desc* d, Plan& pl) {
+  int rc = plan_grid(d->np, pl);
+  if (rc) return rc;
+  const int P = pl.P, Pt = pl.Pt;
+  if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
+  if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
+  if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
+  if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
+  if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
   pl.NB = d->nb;
   pl.MB = d->mb;
   pl.NS = d->n_species;
@@ -745,6 +751,11 @@ extern "C" int sdft_request_destroy(sdft_handle h) {
   cudaStreamDestroy(h->stream);
   delete h;
   return SDFT_OK;
+}
+
+extern "C" int sdft_grid_supported(int32_t np) {
+  Plan pl;
+  return plan_grid(np, pl);
 }
 
 extern "C" int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* device_bytes) {

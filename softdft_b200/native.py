@@ -26,13 +26,22 @@ EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_num
            "sdft_request_create", "sdft_request_destroy", "sdft_request_sizes", "sdft_set_state",
            "sdft_get_state", "sdft_objective", "sdft_solve", "sdft_get_densities", "sdft_grand_potential",
            "sdft_num_species", "sdft_solve_batch", "sdft_last_batch_stats", "sdft_server_create",
-           "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll", "sdft_bulk_eval"]
+           "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll", "sdft_bulk_eval",
+           "sdft_grid_supported"]
 
 
 class SdftError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
         self.code = code
+
+
+def grid_supported(np_: int) -> bool:
+    """True when the device solve runs a grid of np_ points (sdft_grid_supported)."""
+    f = lib().sdft_grid_supported
+    f.argtypes = [C.c_int32]
+    f.restype = C.c_int
+    return f(int(np_)) == SDFT_OK
 
 
 def library_present() -> bool:

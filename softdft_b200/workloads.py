@@ -144,12 +144,21 @@ def diblock_slit(np_: int = 16384) -> dict:
 
 
 def batch_uneven(n: int = 512, seed: int = 3, np_lo: int = 2048, np_hi: int = 16384,
-                 n_lo: int = 10, n_hi: int = 300) -> List[dict]:
-    """Seeded uneven batch; NP is drawn log-uniform and rounded to a power of two."""
+                 n_lo: int = 10, n_hi: int = 300, pow2: bool = False) -> List[dict]:
+    """Seeded uneven batch.  NP is drawn log-uniform and moved up to the next
+    grid size the device transform runs (FFT length without prime factors above
+    61), or rounded to a power of two with ``pow2``."""
+    from . import native
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
-        np_ = int(2 ** round(math.log2(math.exp(rng.uniform(math.log(np_lo), math.log(np_hi))))))
+        draw = math.exp(rng.uniform(math.log(np_lo), math.log(np_hi)))
+        if pow2:
+            np_ = int(2 ** round(math.log2(draw)))
+        else:
+            np_ = int(round(draw))
+            while not native.grid_supported(np_):
+                np_ += 1
         nch = int(rng.integers(n_lo, n_hi + 1))
         pH = float(rng.uniform(2.0, 12.0))
         salt = float(math.exp(rng.uniform(math.log(1e-3), math.log(1.0))))
