@@ -325,7 +325,7 @@ def run_uneven(args):
            "config": {"workload": "uneven_batch", "requests": len(systems), "np_range": [lo, hi], "chain_range": [nlo, nhi],
                       "np": {"min": int(min(d.NP for d in dfts)), "median": float(np.median([d.NP for d in dfts])),
                              "max": int(max(d.NP for d in dfts)), "odd": int(sum(d.NP % 2 for d in dfts)),
-                             "draw": "log-uniform, next size the device transform runs"},
+                             "draw": "log-uniform, next 7-smooth size"},
                       "max_iters": num.max_iters, "seed": 3, "host_setup_s": setup_s},
            "status_counts": {str(k): int(v) for k, v in zip(*np.unique(status, return_counts=True))},
            "iterations": {"min": int(iters.min()), "median": float(np.median(iters)), "max": int(iters.max())},

@@ -233,7 +233,7 @@ __device__ __forceinline__ void bfly_dif(C& a, C& b, C w) {  // DIF: (a + b, (a 
 }
 
 // ---- general length M --------------------------------------------------------
-// M = r_0 r_1 ... r_{s-1} with radices 4, 2, 3, 5, 7 and primes up to
+// M = r_0 r_1 ... r_{s-1} with radices 4, 2, 3, 5, 7, 11, 13 and primes up to
 // kMaxGenRadix.  Forward: in-place decimation in time over stages of growing
 // span m = r_0 ... r_{i-1}; the butterfly (group g, offset j < m) takes
 // x_q = z[g m r + j + q m] w_{m r}^{j q} (q < r) and writes its r-point DFT back to
@@ -244,14 +244,57 @@ __device__ __forceinline__ void bfly_dif(C& a, C& b, C w) {  // DIF: (a + b, (a 
 // natural order in, the same digit-reversed order out.  Roots of unity come
 // from tw[k] = e^{-2 pi i k / M}: w_r^e = tw[e M / r].
 
+// r-point DFT of an odd prime r in registers: x_q and x_{r-q} are paired,
+// S_q = x_q + x_{r-q}, D_q = x_q - x_{r-q}, and for l = 1 .. (r-1)/2
+//   X_l, X_{r-l} = A_l -+ i B_l,  A_l = x_0 + sum_q S_q cos(2 pi q l / r),
+//   B_l = sum_q D_q sin(2 pi q l / r)   (signs swapped for the inverse),
+// real weights only, a quarter of the multiplies of the plain sum
+template <class C, int R>
+__device__ __forceinline__ void dft_odd_prime(C* x, const C* __restrict__ tw, int step, bool inv) {
+  using T = typename Cx<C>::R;
+  constexpr int H = (R - 1) / 2;
+  T cs[H + 1], sn[H + 1];
+#pragma unroll
+  for (int e = 1; e <= H; e++) {
+    const C w = __ldg(&tw[e * step]);  // e^{-2 pi i e / r}
+    cs[e] = w.x;
+    sn[e] = -w.y;
+  }
+  C S[H], D[H];
+#pragma unroll
+  for (int q = 1; q <= H; q++) {
+    S[q - 1] = add2(x[q], x[R - q]);
+    D[q - 1] = sub2(x[q], x[R - q]);
+  }
+  C X0 = x[0];
+#pragma unroll
+  for (int q = 0; q < H; q++) X0 = add2(X0, S[q]);
+#pragma unroll
+  for (int l = 1; l <= H; l++) {
+    C A = x[0], B = Cx<C>::make((T)0, (T)0);
+#pragma unroll
+    for (int q = 1; q <= H; q++) {
+      const int e = (q * l) % R;
+      const T cv = e <= H ? cs[e] : cs[R - e];
+      const T sv = e <= H ? sn[e] : -sn[R - e];
+      A = add2(A, scl2(S[q - 1], cv));
+      B = add2(B, scl2(D[q - 1], sv));
+    }
+    const C iB = inv ? Cx<C>::make(-B.y, B.x) : Cx<C>::make(B.y, -B.x);  // +i B (inverse), -i B (forward)
+    x[l] = add2(A, iB);
+    x[R - l] = sub2(A, iB);
+  }
+  x[0] = X0;
+}
+
 // r-point DFT in registers (inv: conjugate roots), compile-time r
 template <class C, int R>
 __device__ __forceinline__ void dft_fixed(C* x, const C* __restrict__ tw, int step, bool inv) {
-  if (R == 2) {
+  if constexpr (R == 2) {
     const C a = x[0], b = x[1];
     x[0] = add2(a, b);
     x[1] = sub2(a, b);
-  } else if (R == 4) {
+  } else if constexpr (R == 4) {
     const C s02 = add2(x[0], x[2]), d02 = sub2(x[0], x[2]);
     const C s13 = add2(x[1], x[3]), d13 = sub2(x[1], x[3]);
     const C jd = inv ? Cx<C>::make(-d13.y, d13.x) : Cx<C>::make(d13.y, -d13.x);  // (+-i) d13
@@ -260,41 +303,38 @@ __device__ __forceinline__ void dft_fixed(C* x, const C* __restrict__ tw, int st
     x[1] = add2(d02, jd);
     x[3] = sub2(d02, jd);
   } else {
-    C w[R], X[R];
-#pragma unroll
-    for (int k = 0; k < R; k++) {
-      w[k] = __ldg(&tw[k * step]);
-      if (inv) w[k] = conj2(w[k]);
-    }
-#pragma unroll
-    for (int l = 0; l < R; l++) {
-      C acc = x[0];
-#pragma unroll
-      for (int q = 1; q < R; q++) acc = add2(acc, cmul(x[q], w[(q * l) % R]));
-      X[l] = acc;
-    }
-#pragma unroll
-    for (int l = 0; l < R; l++) x[l] = X[l];
+    dft_odd_prime<C, R>(x, tw, step, inv);
   }
 }
 
-// r-point DFT for a prime r known only at run time (r <= kMaxGenRadix)
+// the same paired DFT for an odd prime r known only at run time (r <= kMaxGenRadix)
 template <class C>
 __device__ __noinline__ void dft_any(C* x, int R, const C* __restrict__ tw, int step, bool inv) {
-  C X[kMaxGenRadix];
-  for (int l = 0; l < R; l++) {
-    C acc = x[0];
+  using T = typename Cx<C>::R;
+  constexpr int HM = (kMaxGenRadix - 1) / 2;
+  const int H = (R - 1) / 2;
+  C S[HM], D[HM];
+  C X0 = x[0];
+  for (int q = 1; q <= H; q++) {
+    S[q - 1] = add2(x[q], x[R - q]);
+    D[q - 1] = sub2(x[q], x[R - q]);
+    X0 = add2(X0, S[q - 1]);
+  }
+  for (int l = 1; l <= H; l++) {
+    C A = x[0], B = Cx<C>::make((T)0, (T)0);
     int e = 0;  // (q l) mod R
-    for (int q = 1; q < R; q++) {
+    for (int q = 1; q <= H; q++) {
       e += l;
       if (e >= R) e -= R;
-      C w = __ldg(&tw[e * step]);
-      if (inv) w = conj2(w);
-      acc = add2(acc, cmul(x[q], w));
+      const C w = __ldg(&tw[e * step]);  // cos = w.x, sin = -w.y
+      A = add2(A, scl2(S[q - 1], w.x));
+      B = add2(B, scl2(D[q - 1], -w.y));
     }
-    X[l] = acc;
+    const C iB = inv ? Cx<C>::make(-B.y, B.x) : Cx<C>::make(B.y, -B.x);
+    x[l] = add2(A, iB);
+    x[R - l] = sub2(A, iB);
   }
-  for (int l = 0; l < R; l++) x[l] = X[l];
+  x[0] = X0;
 }
 
 // one stage of radix R (R = 0: run-time radix rr) and span m; DIT forward or DIF inverse
@@ -339,6 +379,8 @@ __device__ __forceinline__ void gen_stage_any_radix(const FftCtxT<C>& c, int nT,
     case 4: gen_stage<C, 4>(c, nT, m, 4, inv); break;
     case 5: gen_stage<C, 5>(c, nT, m, 5, inv); break;
     case 7: gen_stage<C, 7>(c, nT, m, 7, inv); break;
+    case 11: gen_stage<C, 11>(c, nT, m, 11, inv); break;
+    case 13: gen_stage<C, 13>(c, nT, m, 13, inv); break;
     default: gen_stage<C, 0>(c, nT, m, r, inv); break;
   }
 }

@@ -785,20 +785,34 @@ static cudaError_t launch_objective(bool gen, const DReq* reqs, size_t smem, cud
 static cudaError_t launch_omega(bool gen, const DReq* reqs, double* out, size_t smem, cudaStream_t s) {
   return gen ? launch_omega_gen(reqs, out, smem, s) : launch_omega_pow2(reqs, out, smem, s);
 }
-// a batch: one launch of each build that has requests in it; *launches counts them
+// a batch: one launch of each build that has requests in it; *launches counts
+// them.  With both kinds present the general build runs on a second stream that
+// forks from and joins back into s, so the two launches share the GPU (each
+// writes only the slots of its own requests).
 static cudaError_t launch_solve(bool any_pow2, bool any_gen, const DReq* reqs, SolveSlot* slots, const SolveCfg& cfg,
                                 int max_chunk, int n, size_t smem, cudaStream_t s, int* launches) {
-  if (any_pow2) {
-    cudaError_t e = launch_solve_pow2(reqs, slots, cfg, max_chunk, n, smem, s);
-    if (e != cudaSuccess) return e;
-    (*launches)++;
+  if (!(any_pow2 && any_gen)) {
+    cudaError_t e = any_gen ? launch_solve_gen(reqs, slots, cfg, max_chunk, n, smem, s)
+                            : launch_solve_pow2(reqs, slots, cfg, max_chunk, n, smem, s);
+    if (e == cudaSuccess) (*launches)++;
+    return e;
   }
-  if (any_gen) {
-    cudaError_t e = launch_solve_gen(reqs, slots, cfg, max_chunk, n, smem, s);
-    if (e != cudaSuccess) return e;
-    (*launches)++;
-  }
-  return cudaSuccess;
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(fork, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
+  if (e == cudaSuccess) e = launch_solve_pow2(reqs, slots, cfg, max_chunk, n, smem, s);
+  if (e == cudaSuccess) e = launch_solve_gen(reqs, slots, cfg, max_chunk, n, smem, s2);
+  if (e == cudaSuccess) e = cudaEventRecord(join, s2);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+  if (e == cudaSuccess) *launches += 2;
+  if (join) cudaEventDestroy(join);
+  if (fork) cudaEventDestroy(fork);
+  if (s2) cudaStreamDestroy(s2);
+  return e;
 }
 
 // `rows` fields of NPt points between the caller's packed layout and the device

@@ -143,12 +143,18 @@ def diblock_slit(np_: int = 16384) -> dict:
     }
 
 
+def _smooth7(n: int) -> bool:
+    for p in (2, 3, 5, 7):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
 def batch_uneven(n: int = 512, seed: int = 3, np_lo: int = 2048, np_hi: int = 16384,
                  n_lo: int = 10, n_hi: int = 300, pow2: bool = False) -> List[dict]:
     """Seeded uneven batch.  NP is drawn log-uniform and moved up to the next
-    grid size the device transform runs (FFT length without prime factors above
-    61), or rounded to a power of two with ``pow2``."""
-    from . import native
+    7-smooth size (prime factors 2, 3, 5, 7 only), or rounded to a power of two
+    with ``pow2``."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
@@ -157,7 +163,7 @@ def batch_uneven(n: int = 512, seed: int = 3, np_lo: int = 2048, np_hi: int = 16
             np_ = int(2 ** round(math.log2(draw)))
         else:
             np_ = int(round(draw))
-            while not native.grid_supported(np_):
+            while not _smooth7(np_):
                 np_ += 1
         nch = int(rng.integers(n_lo, n_hi + 1))
         pH = float(rng.uniform(2.0, 12.0))
