@@ -43,10 +43,11 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import native
-from .api import IsingDFT, densities, eval_inhomogeneous, geometry_system, grand_potential, iLST, setup_iDFT
+from .api import (IsingDFT, densities, eval_inhomogeneous, geometry_system, grand_potential, iLST, setup_iDFT,
+                  state_fractions)
 from .host.descriptor import numerics_from_dict
 from .host.geometry import cld
-from .output import contact_value_theorem_arrays, jl
+from .output import brush_height_values, call_analysis, contact_value_theorem_arrays, jl
 
 
 # ---- grid and warm start ------------------------------------------------------
@@ -327,4 +328,187 @@ def batched_distance_sweep(branches: Sequence[dict], distances: Sequence[float],
                            "residual": float(errs[b]), "batch_device_ms": device_ms})
             prev[b] = (dft.state, dft.geometry)
             dft.handle().close()
+    return out
+
+
+# ---- pseudo-arclength continuation in pH -----------------------------------------
+#
+# Restates src/NonlinearSolvers/continuation/objective_pac.jl:41-289 on the
+# unknowns the solver uses today, X = (mu_ex_K, lng_K, Psi, PsiC, pH) (the
+# reference file flattens the segment densities, bond densities and PsiC, which
+# the current solver_dft no longer iterates on).  As there:
+#   * two natural steps start the branch (pH0, then pH0 + ds_init);
+#   * the tangent is the normalised secant of the last two points, or the
+#     three-point backward difference in arclength once three exist (:128-146);
+#   * the predictor is X_k + dS t (:150-152);
+#   * the corrected point satisfies G(x) = x and the hyperplane constraint
+#     t . (X - X_k) = dS (objective_pac, :253-289);
+#   * the arclength grows by |X - X_prev| and dS <- (dS + |X - X_prev|) / 2 (:164-172);
+#   * the sweep stops outside pH (1.99, 12.01) or when alpha passes 0.99 going up
+#     or 0.01 going down (:233-241).
+# Differences: the reference folds the constraint into every Anderson step
+# (pH <- pH_k + (dS - t_x . (G(x) - x_k)) / t_pH) and rebuilds the whole system
+# per evaluation; here pH enters through the bulk state and the descriptor, so
+# the corrector is a secant iteration on pH whose every evaluation is a
+# warm-started device solve of x(pH) (the first update is the reference's
+# formula).  The constraint uses the current dS (the reference freezes ds_init
+# into it), and the alpha stop looks at the direction of pH along the tangent
+# (the reference tests sign(dS), which is always positive).
+
+def _pac_tangent(X_hist: Sequence[np.ndarray], S_hist: Sequence[float]) -> np.ndarray:
+    """Unit tangent of the branch at its last point (objective_pac.jl:128-148)."""
+    if len(X_hist) < 3:
+        t = X_hist[-1] - X_hist[-2]
+    else:
+        ds1 = S_hist[-1] - S_hist[-2]
+        ds2 = S_hist[-2] - S_hist[-3]
+        a = ds1 / (ds2 * (ds1 + ds2))
+        b = -(ds1 + ds2) / (ds1 * ds2)
+        c = (2.0 * ds1 + ds2) / (ds1 * (ds1 + ds2))
+        t = a * X_hist[-3] + b * X_hist[-2] + c * X_hist[-1]
+    return t / np.linalg.norm(t)
+
+
+def _branch_pH(data: dict) -> float:
+    for sp in data["species"]:
+        if sp.get("sequence") == "Y":
+            return float(sp["pSpecies"])
+    raise ValueError("pH continuation needs the proton species Y with a pSpecies")
+
+
+def _alpha(dft: IsingDFT) -> float:
+    """Average fraction of state 2 over the dissociating segments of the first
+    species that has them (the routine's read_avg_state_fraction)."""
+    for v in state_fractions(dft).values():
+        a = v["avg"]
+        return float(a[1]) if len(a) > 1 else float("nan")
+    return float("nan")
+
+
+def _solve_points(datas, pHs, x0s, num):
+    """One batched device solve: branch b at pH pHs[b], warm-started from x0s[b]
+    (None: the reference's initial guess).  Returns the solved systems."""
+    dfts = []
+    for d, pH, x0 in zip(datas, pHs, x0s):
+        _set_pH(d, pH)
+        dft = setup_iDFT(d, iLST(d), geometry_system(d))
+        if x0 is not None:
+            dft.handle().set_x(x0)
+        dfts.append(dft)
+    iters, errs, status = native.solve_batch([t.handle() for t in dfts], num)
+    for b, dft in enumerate(dfts):
+        dft.iterations, dft.residual, dft.status = int(iters[b]), float(errs[b]), int(status[b])
+    return dfts
+
+
+def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: int = 200, num=None,
+                    pH_range=(1.99, 12.01), corrector_tol: float = 1e-6, max_corrector: int = 10,
+                    out_root: Optional[str] = None) -> List[List[dict]]:
+    """Pseudo-arclength continuation in pH of independent branches (one input
+    dataset each); every solve of a step is one batched launch over the branches
+    still running.  Returns per branch the list of per-point records (pH, alpha,
+    brush height, Omega, arclength, step length, corrector iterations).  With
+    out_root, each point's analysis files go to out_root/b<branch>/pH_<pH>."""
+    datas = [copy.deepcopy(b) for b in branches]
+    if num is None:
+        num = numerics_from_dict(datas[0].get("numerical") or {})
+    nb = len(datas)
+    out: List[List[dict]] = [[] for _ in datas]
+    X_hist: List[List[np.ndarray]] = [[] for _ in datas]
+    S_hist: List[List[float]] = [[] for _ in datas]
+    dS = [float(ds_init)] * nb
+    s = [0.0] * nb
+    active = [True] * nb
+
+    def record(b, dft, pH, step, corr, used_ds):
+        x = dft.handle().get_x()
+        X = np.concatenate([x, [pH]])
+        rec = {"step": step, "pH": pH, "alpha": _alpha(dft), "omega": grand_potential(dft),
+               "iterations": dft.iterations, "status": dft.status, "residual": dft.residual,
+               "corrector_iterations": corr, "dS": used_ds}
+        hb = brush_height_values(densities(dft)[0], dft.bulk_system.molsys, dft.geometry, dft.descriptor.fixed_coord)
+        rec["brush_height"] = next(iter(hb.values())) if hb else float("nan")
+        if X_hist[b]:
+            ds_actual = float(np.linalg.norm(X - X_hist[b][-1]))
+            s[b] += ds_actual
+            rec["ds_actual"] = ds_actual
+        rec["arclength"] = s[b]
+        X_hist[b] = (X_hist[b] + [X])[-3:]
+        S_hist[b] = (S_hist[b] + [s[b]])[-3:]
+        if out_root is not None:
+            d = os.path.join(out_root, f"b{b}", _fmt_dir("pH_", pH, 3))
+            os.makedirs(d, exist_ok=True)
+            call_analysis(dft, d)
+        out[b].append(rec)
+        return rec
+
+    def ok(dft):
+        return dft.status in (native.SDFT_OK, native.SDFT_MAX_ITERS)
+
+    # two natural steps start every branch (objective_pac.jl:59-113)
+    pH0 = [_branch_pH(d) for d in datas]
+    dfts = _solve_points(datas, pH0, [None] * nb, num)
+    for b, dft in enumerate(dfts):
+        record(b, dft, pH0[b], 1, 0, 0.0)
+        active[b] = ok(dft)
+    x1 = [dft.handle().get_x() for dft in dfts]
+    for dft in dfts:
+        dft.handle().close()
+    idx = [b for b in range(nb) if active[b]]
+    dfts = _solve_points([datas[b] for b in idx], [pH0[b] + dS[b] for b in idx], [x1[b] for b in idx], num)
+    for b, dft in zip(idx, dfts):
+        record(b, dft, pH0[b] + dS[b], 2, 0, dS[b])
+        active[b] = ok(dft)
+        dft.handle().close()
+
+    for step in range(3, max_steps + 1):
+        idx = [b for b in range(nb) if active[b] and pH_range[0] < X_hist[b][-1][-1] < pH_range[1]]
+        if not idx:
+            break
+        tang = {b: _pac_tangent(X_hist[b], S_hist[b]) for b in idx}
+        Xk = {b: X_hist[b][-1] for b in idx}
+        used = {b: dS[b] for b in idx}
+        # corrector: secant on f(pH) = t . (X(pH) - X_k) - dS with X(pH) = (x(pH), pH)
+        lam = {b: Xk[b][-1] + used[b] * tang[b][-1] for b in idx}
+        xstart = {b: (Xk[b] + used[b] * tang[b])[:-1] for b in idx}
+        hist = {b: [] for b in idx}  # (pH, f)
+        done: dict = {}
+        todo = list(idx)
+        for it in range(max_corrector):
+            if not todo:
+                break
+            dfts = _solve_points([datas[b] for b in todo], [lam[b] for b in todo], [xstart[b] for b in todo], num)
+            nxt = []
+            for b, dft in zip(todo, dfts):
+                t = tang[b]
+                x = dft.handle().get_x()
+                f = float(np.dot(t[:-1], x - Xk[b][:-1]) + t[-1] * (lam[b] - Xk[b][-1]) - used[b])
+                hist[b].append((lam[b], f))
+                last = it == max_corrector - 1
+                if not ok(dft) or abs(f) <= corrector_tol * used[b] or last:
+                    done[b] = (dft, it + 1, ok(dft) and abs(f) <= corrector_tol * used[b], f)
+                    continue
+                if len(hist[b]) == 1:
+                    # the reference's constraint update: pH = pH_k + (dS - t_x . (x - x_k)) / t_pH
+                    lam[b] = lam[b] - f / t[-1]
+                else:
+                    (l0, f0), (l1, f1) = hist[b][-2], hist[b][-1]
+                    lam[b] = l1 - f1 * (l1 - l0) / (f1 - f0) if f1 != f0 else l1 - f1 / t[-1]
+                xstart[b] = x
+                dft.handle().close()
+                nxt.append(b)
+            todo = nxt
+        for b in idx:
+            dft, corr, converged, f = done[b]
+            rec = record(b, dft, lam[b], step, corr, used[b])
+            rec["corrector_converged"] = converged
+            rec["constraint_residual"] = f  # t . (X - X_k) - dS at the accepted point
+            dft.handle().close()
+            if not ok(dft):
+                active[b] = False
+                continue
+            dS[b] = (dS[b] + rec["ds_actual"]) / 2.0
+            going_up = tang[b][-1] > 0
+            if (rec["alpha"] >= 0.99 and going_up) or (rec["alpha"] <= 0.01 and not going_up):
+                active[b] = False
     return out

@@ -76,3 +76,39 @@ def test_adjust_pH_sweep_writes_the_routine_files(tmp_path):
     assert lines[0] == "step,pH,brush_height,alpha" and len(lines) == 4
     for name in ("cvt.txt", "grand_potential.txt", "brush_height.txt", "MEP.txt", "rho_beads_K.txt"):
         assert (tmp_path / "pH_sweep" / "pH_5.50" / name).is_file(), name
+
+
+# ---- pseudo-arclength continuation in pH ----
+
+def _pac_branches():
+    out = []
+    for pH in (4.0, 5.0):
+        ds = workloads.grafted_brush(128, 0.05, 8, 0.05, 4.5, pH, 0.01)
+        ds["numerical"] = dict(ds["numerical"], tole=1e-10, max_iters=8000)
+        out.append(ds)
+    return out
+
+
+def test_pac_points_are_solutions_on_the_constraint_hyperplane():
+    res = ct.pac_pH_branches(_pac_branches(), ds_init=0.2, max_steps=5)
+    for pts in res:
+        assert len(pts) == 5
+        for p in pts:
+            assert p["status"] == 0 and p["residual"] < 1e-10
+            assert 0.0 <= p["alpha"] <= 1.0
+        for p in pts[2:]:
+            assert p["corrector_converged"]
+            assert abs(p["constraint_residual"]) <= 1e-6 * p["dS"]
+        # the two natural steps point up in pH; the brush ionises as pH grows
+        assert np.all(np.diff([p["pH"] for p in pts]) > 0)
+        assert np.all(np.diff([p["alpha"] for p in pts]) > 0)
+
+
+def test_pac_batched_branches_equal_branches_alone():
+    br = _pac_branches()
+    together = ct.pac_pH_branches(br, ds_init=0.2, max_steps=4)
+    for b, ds in enumerate(br):
+        alone = ct.pac_pH_branches([ds], ds_init=0.2, max_steps=4)[0]
+        assert len(alone) == len(together[b])
+        for p_t, p_a in zip(together[b], alone):
+            assert p_t["pH"] == p_a["pH"] and p_t["omega"] == p_a["omega"]

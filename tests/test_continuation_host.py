@@ -104,3 +104,15 @@ def test_readers_of_the_routine_files(tmp_path):
     (tmp_path / "t.txt").write_text("segment state1 state2\n1 0.25 0.75\n\n"
                                     "# Average state fractions across all dissociating segments:\navg 0.3 0.7\n")
     assert ct.read_avg_state_fraction(str(tmp_path / "t.txt"), 2) == 0.7
+
+
+def test_pac_tangent_secant_and_three_point_difference():
+    rng = np.random.default_rng(5)
+    a, b, c = rng.normal(size=(3, 7))
+    S = [0.0, 0.7, 1.6]
+    X = [a + b * s + c * s * s for s in S]
+    t2 = ct._pac_tangent(X[:2], S[:2])
+    assert np.allclose(t2, (X[1] - X[0]) / np.linalg.norm(X[1] - X[0]), rtol=0, atol=1e-15)
+    # the three-point backward difference is exact for a quadratic in arclength
+    d = b + 2 * c * S[2]
+    assert np.allclose(ct._pac_tangent(X, S), d / np.linalg.norm(d), rtol=0, atol=1e-12)
