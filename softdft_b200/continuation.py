@@ -331,9 +331,10 @@ def batched_distance_sweep(branches: Sequence[dict], distances: Sequence[float],
     return out
 
 
-# ---- pseudo-arclength continuation in pH -----------------------------------------
+# ---- pseudo-arclength continuation in pH or graft density -------------------------
 #
-# Restates src/NonlinearSolvers/continuation/objective_pac.jl:41-289 on the
+# Restates src/NonlinearSolvers/continuation/objective_pac.jl:41-289 (and its
+# graft-density twin objective_pac_graft.jl, continuation variable ln(density)) on the
 # unknowns the solver uses today, X = (mu_ex_K, lng_K, Psi, PsiC, pH) (the
 # reference file flattens the segment densities, bond densities and PsiC, which
 # the current solver_dft no longer iterates on).  As there:
@@ -385,12 +386,23 @@ def _alpha(dft: IsingDFT) -> float:
     return float("nan")
 
 
-def _solve_points(datas, pHs, x0s, num):
-    """One batched device solve: branch b at pH pHs[b], warm-started from x0s[b]
-    (None: the reference's initial guess).  Returns the solved systems."""
+def _set_log_graft(data: dict, v: float) -> None:
+    """update_cont_var_graft (objective_pac_graft.jl:286-287): the first species'
+    graft density is e^v."""
+    data["species"][0]["fixed"]["density"] = math.exp(v)
+
+
+def _log_graft(data: dict) -> float:
+    return math.log(data["species"][0]["fixed"]["density"])
+
+
+def _solve_points(datas, pHs, x0s, num, setter=_set_pH):
+    """One batched device solve: branch b at parameter pHs[b] (set by `setter`),
+    warm-started from x0s[b] (None: the reference's initial guess).  Returns the
+    solved systems."""
     dfts = []
     for d, pH, x0 in zip(datas, pHs, x0s):
-        _set_pH(d, pH)
+        setter(d, pH)
         dft = setup_iDFT(d, iLST(d), geometry_system(d))
         if x0 is not None:
             dft.handle().set_x(x0)
@@ -409,6 +421,23 @@ def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: 
     still running.  Returns per branch the list of per-point records (pH, alpha,
     brush height, Omega, arclength, step length, corrector iterations).  With
     out_root, each point's analysis files go to out_root/b<branch>/pH_<pH>."""
+    return _pac_branches(branches, "pH", ds_init, max_steps, num, pH_range, corrector_tol, max_corrector, out_root)
+
+
+def pac_graft_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: int = 200, num=None,
+                       log_range=(-math.inf, 1.0), corrector_tol: float = 1e-6, max_corrector: int = 10,
+                       out_root: Optional[str] = None) -> List[List[dict]]:
+    """Pseudo-arclength continuation in the log of the first species' graft
+    density (pac_continuation_graft, objective_pac_graft.jl:36-284): the same
+    scheme with v = ln(density) as the continuation variable, run while v < 1,
+    without the alpha stop; records carry graft_density = e^v, and the analysis
+    files go to out_root/b<branch>/graft_<density>."""
+    return _pac_branches(branches, "graft", ds_init, max_steps, num, log_range, corrector_tol, max_corrector,
+                         out_root)
+
+
+def _pac_branches(branches, kind, ds_init, max_steps, num, pH_range, corrector_tol, max_corrector, out_root):
+    getter, setter = (_branch_pH, _set_pH) if kind == "pH" else (_log_graft, _set_log_graft)
     datas = [copy.deepcopy(b) for b in branches]
     if num is None:
         num = numerics_from_dict(datas[0].get("numerical") or {})
@@ -423,7 +452,7 @@ def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: 
     def record(b, dft, pH, step, corr, used_ds):
         x = dft.handle().get_x()
         X = np.concatenate([x, [pH]])
-        rec = {"step": step, "pH": pH, "alpha": _alpha(dft), "omega": grand_potential(dft),
+        rec = {"step": step, "alpha": _alpha(dft), "omega": grand_potential(dft),
                "iterations": dft.iterations, "status": dft.status, "residual": dft.residual,
                "corrector_iterations": corr, "dS": used_ds}
         hb = brush_height_values(densities(dft)[0], dft.bulk_system.molsys, dft.geometry, dft.descriptor.fixed_coord)
@@ -433,10 +462,16 @@ def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: 
             s[b] += ds_actual
             rec["ds_actual"] = ds_actual
         rec["arclength"] = s[b]
+        if kind == "pH":
+            rec["pH"] = pH
+        else:
+            rec["log_graft_density"] = pH
+            rec["graft_density"] = math.exp(pH)
         X_hist[b] = (X_hist[b] + [X])[-3:]
         S_hist[b] = (S_hist[b] + [s[b]])[-3:]
         if out_root is not None:
-            d = os.path.join(out_root, f"b{b}", _fmt_dir("pH_", pH, 3))
+            d = os.path.join(out_root, f"b{b}", _fmt_dir("pH_", pH, 3) if kind == "pH"
+                             else _fmt_dir("graft_", math.exp(pH), 7))
             os.makedirs(d, exist_ok=True)
             call_analysis(dft, d)
         out[b].append(rec)
@@ -446,8 +481,8 @@ def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: 
         return dft.status in (native.SDFT_OK, native.SDFT_MAX_ITERS)
 
     # two natural steps start every branch (objective_pac.jl:59-113)
-    pH0 = [_branch_pH(d) for d in datas]
-    dfts = _solve_points(datas, pH0, [None] * nb, num)
+    pH0 = [getter(d) for d in datas]
+    dfts = _solve_points(datas, pH0, [None] * nb, num, setter)
     for b, dft in enumerate(dfts):
         record(b, dft, pH0[b], 1, 0, 0.0)
         active[b] = ok(dft)
@@ -455,7 +490,7 @@ def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: 
     for dft in dfts:
         dft.handle().close()
     idx = [b for b in range(nb) if active[b]]
-    dfts = _solve_points([datas[b] for b in idx], [pH0[b] + dS[b] for b in idx], [x1[b] for b in idx], num)
+    dfts = _solve_points([datas[b] for b in idx], [pH0[b] + dS[b] for b in idx], [x1[b] for b in idx], num, setter)
     for b, dft in zip(idx, dfts):
         record(b, dft, pH0[b] + dS[b], 2, 0, dS[b])
         active[b] = ok(dft)
@@ -477,7 +512,8 @@ def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: 
         for it in range(max_corrector):
             if not todo:
                 break
-            dfts = _solve_points([datas[b] for b in todo], [lam[b] for b in todo], [xstart[b] for b in todo], num)
+            dfts = _solve_points([datas[b] for b in todo], [lam[b] for b in todo], [xstart[b] for b in todo], num,
+                                 setter)
             nxt = []
             for b, dft in zip(todo, dfts):
                 t = tang[b]
@@ -509,6 +545,6 @@ def pac_pH_branches(branches: Sequence[dict], ds_init: float = 0.05, max_steps: 
                 continue
             dS[b] = (dS[b] + rec["ds_actual"]) / 2.0
             going_up = tang[b][-1] > 0
-            if (rec["alpha"] >= 0.99 and going_up) or (rec["alpha"] <= 0.01 and not going_up):
+            if kind == "pH" and ((rec["alpha"] >= 0.99 and going_up) or (rec["alpha"] <= 0.01 and not going_up)):
                 active[b] = False
     return out

@@ -112,3 +112,18 @@ def test_pac_batched_branches_equal_branches_alone():
         assert len(alone) == len(together[b])
         for p_t, p_a in zip(together[b], alone):
             assert p_t["pH"] == p_a["pH"] and p_t["omega"] == p_a["omega"]
+
+
+def test_pac_graft_density_branch():
+    """Continuation in ln(graft density) of the first grafted species: converged
+    points on the constraint hyperplane; the denser left brush grows taller."""
+    ds = _pac_branches()[1]
+    pts = ct.pac_graft_branches([ds], ds_init=0.2, max_steps=4)[0]
+    assert len(pts) == 4
+    for p in pts:
+        assert p["status"] == 0 and p["residual"] < 1e-10
+    for p in pts[2:]:
+        assert p["corrector_converged"] and abs(p["constraint_residual"]) <= 1e-6 * p["dS"]
+    dens = [p["graft_density"] for p in pts]
+    assert dens[0] == pytest.approx(0.05, rel=1e-12) and np.all(np.diff(dens) > 0)
+    assert np.all(np.diff([p["brush_height"] for p in pts]) > 0)
