@@ -38,7 +38,7 @@ struct DSpecies {
   int n_seg;          // segments N_u
   int S;              // state slots per segment
   int fixed;          // grid index of the grafted segment 0, -1 if free
-  int pad0;
+  int tree;           // 1: branched topology (general level walks, arrays below)
   const int* states;  // [n_seg * S] bead type per (segment, slot), -1 padding
   const int* nst;     // [n_seg] states per segment
   const int* bnd;     // [(g * S + i) * S + j] bond type between state i of segment g and state j of g+1, -1 if none
@@ -58,6 +58,13 @@ struct DSpecies {
   const int* eslot;       // [g * S + i] slot of bead type states[g * S + i] among the species' beads
   const int* eslot_bead;  // [neslot] bead type of each slot
   int nbslot, neslot;
+  // branched topologies: gC is [(g * S + i) * C + c) * S + j] * P + K (child slot c)
+  int C;                  // most children of a segment
+  int pad1;
+  const int* parent;      // [n_seg] parent segment, -1 for the root
+  const int* nch;         // [n_seg] children per segment
+  const int* child;       // [n_seg * C] children of each segment
+  const int* order;       // [n_seg] segments by level from the root (ascending index within a level)
 };
 
 struct DReq {

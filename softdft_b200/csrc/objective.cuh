@@ -1010,6 +1010,303 @@ __device__ __forceinline__ bool accumulate_fast(const DReq& r, const DSpecies& s
 }
 
 // eval_spatial_density! + update_spatial_structures!; false on a normalisation error
+// ---------------------------------------------------------------------------
+// branched chains: the level walks of child_propagators.jl:53-141 and
+// parent_propagators.jl:54-122 and the tree branches of handle_fixed.jl:41-73
+// and accumulate_densities.jl:95-184, for any tree whose segments have at most
+// S children, in FP64 and without renormalisation (the reference's
+// arithmetic).  The propagators are indexed as the reference's arrays:
+// gC[g][i][c][j] (state i of g, child slot c, state j of that child) and
+// gP[g][i][j] (state i of g, state j of its parent).  Two index quirks of the
+// reference are kept: the other-children factor of a parent propagator reads
+// gC[p][oc][idx_j] with the slots exchanged (parent_propagators.jl:150), and the
+// grafted normalisation of a leaf reads gC[p][0][idx_i] (handle_fixed.jl:55); the
+// host refuses the trees for which these indices leave the arrays, where the
+// reference fails too.  accumulate_densities keeps the last child's sum (the
+// reference assigns temp inside its loop over children).  Only segment 0 (the
+// root) can be grafted in a 1D slit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ size_t tgc(const DSpecies& s, int P, int g, int i, int c, int j) {
+  return ((((size_t)g * s.S + i) * s.C + c) * s.S + j) * P;
+}
+__device__ __forceinline__ size_t tgp(const DSpecies& s, int P, int g, int i, int j) {
+  return (((size_t)g * s.S + i) * s.S + j) * P;
+}
+// sum over the child states of gC[g][i][c][:] at K (sum_gC_states)
+__device__ __forceinline__ double tgc_sum(const DSpecies& s, int P, int K, int g, int i, int c) {
+  double t = 0.0;
+  for (int j = 0; j < s.S; j++) t += s.gC[tgc(s, P, g, i, c, j) + K];
+  return t;
+}
+__device__ __forceinline__ int bond_of(const DReq& r, int a, int b) {
+  const int lo = min(a, b), hi = max(a, b);
+  for (int u = 0; u < r.MB; u++)
+    if (r.bonds[2 * u] == lo && r.bonds[2 * u + 1] == hi) return u;
+  return -1;
+}
+// max-path-distance mask of a grafted species: entries of segment g farther
+// from the graft point than its path distance are zeroed (child_propagators.jl:147-157)
+__device__ void tree_mask(const DReq& r, const DSpecies& s, double* a, int count_per_K, double md) {
+  const int P = r.NP, Pt = r.NPt;
+  const double md2 = md * md;
+  for (int K = threadIdx.x; K < Pt; K += blockDim.x)
+    if (dist2_grid(K, s.fixed, r.dz) > md2)
+      for (int q = 0; q < count_per_K; q++) a[(size_t)q * P + K] = 0.0;
+}
+
+__device__ void tree_child(const DReq& r, const DSpecies& s, Shared sh) {
+  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C, N = s.n_seg;
+  const double* lng = xs_lng(r, r.x);
+  const double* fin = r.fbe;
+  const double* fout = r.fbe + (size_t)2 * r.MB * P;
+  const double inv_norm = 1.0 / s.normative;
+  const FftCtx fc = make_fft(sh.z, r);
+  for (size_t q = threadIdx.x; q < (size_t)N * S * C * S * P; q += blockDim.x) s.gC[q] = 0.0;
+  __syncthreads();
+  for (int o = N - 1; o >= 0; o--) {
+    const int p = s.order[o];
+    const bool graft = p == 0 && s.fixed >= 0;
+    for (int ii = 0; ii < s.nst[p]; ii++) {  // base case gC[p][i][0][0] = 1
+      double* b = s.gC + tgc(s, P, p, ii, 0, 0);
+      if (graft) {
+        if (threadIdx.x == 0) b[s.fixed] = 1.0;
+      } else {
+        for (int K = threadIdx.x; K < Pt; K += blockDim.x) b[K] = 1.0;
+      }
+    }
+    __syncthreads();
+    for (int ic = 0; ic < s.nch[p]; ic++) {
+      const int c = s.child[p * C + ic];
+      for (int ii = 0; ii < s.nst[p]; ii++)
+        for (int jj = 0; jj < s.nst[c]; jj++) {
+          const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
+          const int bond = bond_of(r, si, sj);
+          const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+          double* out = s.gC + tgc(s, P, p, ii, ic, jj);
+          if (graft) {  // grafted parent, free child: local sum within sigma_ij (child_propagators.jl:91-116)
+            const int Kp = s.fixed;
+            const double Dij = (r.sig[si] + r.sig[sj]) / 2.0, Dij2 = Dij * Dij, renorm = 2.0 * Dij;
+            const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
+            const double el = exp(lng[(size_t)(bond * 2 + pair_i) * P + Kp] / 2.0);
+            double acc = 0.0;
+            for (int K1 = threadIdx.x; K1 < Pt; K1 += blockDim.x) {
+              const double d2 = dist2_grid(K1, Kp, r.dz);
+              if (d2 <= Dij2) {
+                double f = exp(-r.lambda[(size_t)sj * P + K1] + lng_pj[K1] / 2.0);
+                for (int gc = 0; gc < s.nch[c]; gc++) f *= tgc_sum(s, P, K1, c, jj, gc);
+                double t = fabs(f) * el * r.dz * r.trapez[(size_t)sj * P + K1] / renorm;
+                if (fabs(d2 - Dij2) <= 1e-6) t /= 2.0;
+                acc += t / s.normative;
+              }
+            }
+            acc = block_sum(acc, sh.red);
+            if (threadIdx.x == 0) out[Kp] = acc;
+            __syncthreads();
+          } else {  // convolution with the bond kernel (child_propagators.jl:118-141)
+            const double* fj = fin + (size_t)(bond * 2 + pair_j) * P;
+            const double* fo = fout + (size_t)(bond * 2 + pair_i) * P;
+            dct2_convolve_b(
+                fc, 1,
+                [&](int, int K) {
+                  double f = fj[K];
+                  for (int gc = 0; gc < s.nch[c]; gc++) f *= tgc_sum(s, P, K, c, jj, gc);
+                  return f;
+                },
+                [&](int, int k) { return __ldg(&r.Wbond[(size_t)bond * P + k]); },
+                [&](int, int K, double y) { out[K] = fabs(y) * fo[K] * inv_norm; });
+          }
+        }
+    }
+    if (s.fixed >= 0) tree_mask(r, s, s.gC + tgc(s, P, p, 0, 0, 0), S * C * S, s.md[p]);
+    __syncthreads();
+  }
+}
+
+__device__ void tree_parent(const DReq& r, const DSpecies& s, Shared sh) {
+  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C, N = s.n_seg;
+  const double* lng = xs_lng(r, r.x);
+  const double* fin = r.fbe;
+  const double* fout = r.fbe + (size_t)2 * r.MB * P;
+  const double inv_norm = 1.0 / s.normative;
+  const FftCtx fc = make_fft(sh.z, r);
+  for (size_t q = threadIdx.x; q < (size_t)N * S * S * P; q += blockDim.x) s.gP[q] = 0.0;
+  __syncthreads();
+  for (int o = 0; o < N; o++) {
+    const int c = s.order[o];
+    for (int ii = 0; ii < s.nst[c]; ii++) {  // base case gP[c][i][0] = 1
+      double* b = s.gP + tgp(s, P, c, ii, 0);
+      if (c == 0 && s.fixed >= 0) {
+        if (threadIdx.x == 0) b[s.fixed] = 1.0;
+      } else {
+        for (int K = threadIdx.x; K < Pt; K += blockDim.x) b[K] = 1.0;
+      }
+    }
+    __syncthreads();
+    const int p = s.parent[c];
+    if (p >= 0) {
+      for (int ii = 0; ii < s.nst[c]; ii++)
+        for (int jj = 0; jj < s.nst[p]; jj++) {
+          const int si = s.states[c * S + ii], sj = s.states[p * S + jj];
+          const int bond = bond_of(r, si, sj);
+          const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+          double* out = s.gP + tgp(s, P, c, ii, jj);
+          // f_parent without the trapezoid weight (parent_propagators.jl:144-153)
+          auto fpar = [&](int K) {
+            double sp = 0.0;
+            for (int q = 0; q < S; q++) sp += s.gP[tgp(s, P, p, jj, q) + K];
+            double f = sp;
+            for (int oc = 0; oc < s.nch[p]; oc++)
+              if (s.child[p * C + oc] != c) f *= tgc_sum(s, P, K, p, oc, jj);  // slots exchanged, as the reference
+            return f;
+          };
+          if (p == 0 && s.fixed >= 0) {  // grafted parent: local write within sigma_ij (parent_propagators.jl:72-94)
+            const int Kp = s.fixed;
+            const double Dij = (r.sig[si] + r.sig[sj]) / 2.0, Dij2 = Dij * Dij, renorm = 2.0 * Dij;
+            const double f = exp(-r.lambda[(size_t)sj * P + Kp] + lng[(size_t)(bond * 2 + pair_j) * P + Kp] / 2.0) *
+                             fpar(Kp);
+            const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
+            for (int K1 = threadIdx.x; K1 < Pt; K1 += blockDim.x) {
+              const double d2 = dist2_grid(K1, Kp, r.dz);
+              if (d2 <= Dij2) {
+                double v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm * inv_norm;
+                if (fabs(d2 - Dij2) <= 1e-6) v /= 2.0;
+                out[K1] = v;
+              }
+            }
+          } else {
+            const double* fj = fin + (size_t)(bond * 2 + pair_j) * P;
+            const double* fo = fout + (size_t)(bond * 2 + pair_i) * P;
+            dct2_convolve_b(
+                fc, 1, [&](int, int K) { return fj[K] * fpar(K); },
+                [&](int, int k) { return __ldg(&r.Wbond[(size_t)bond * P + k]); },
+                [&](int, int K, double y) { out[K] = fabs(y) * fo[K] * inv_norm; });
+          }
+          __syncthreads();
+        }
+    }
+    if (s.fixed >= 0) tree_mask(r, s, s.gP + tgp(s, P, c, 0, 0), S * S, s.md[c]);
+    __syncthreads();
+  }
+}
+
+// handle_fixed.jl:41-73 and :105-112 for a tree
+__device__ bool tree_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_out) {
+  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C;
+  double lam, norm;
+  if (s.fixed >= 0) {
+    norm = s.fixed_density;
+    s.mu_species = 0.0;
+    const int p = 1;  // the first free segment
+    double acc = 0.0;
+    for (int K = threadIdx.x; K < Pt; K += blockDim.x)
+      for (int ii = 0; ii < s.nst[p]; ii++) {
+        const int si = s.states[p * S + ii];
+        double sp = 0.0;
+        for (int q = 0; q < S; q++) sp += s.gP[tgp(s, P, p, ii, q) + K];
+        const double contr = exp(-r.lambda[(size_t)si * P + K]) * sp;
+        double temp;
+        if (s.nch[p] == 0) {
+          temp = tgc_sum(s, P, K, p, 0, ii);  // gC[K, :, idx_i, 1, parent] (handle_fixed.jl:55)
+        } else {
+          temp = 0.0;
+          for (int ic = 0; ic < s.nch[p]; ic++) {
+            const int c = s.child[p * C + ic];
+            double t1 = 0.0;
+            for (int jj = 0; jj < s.nst[c]; jj++) {
+              double t2 = s.gC[tgc(s, P, p, ii, ic, jj) + K];
+              for (int oc = 0; oc < s.nch[p]; oc++)
+                if (oc != ic) t2 *= tgc_sum(s, P, K, p, ii, oc);
+              t1 += t2;
+            }
+            temp = t1;
+          }
+        }
+        acc += contr * temp * r.trapez[(size_t)si * P + K] * r.dz;
+      }
+    lam = block_sum(acc, sh.red);
+  } else {
+    lam = 1.0;
+    norm = s.norm_free;
+  }
+  if (!isfinite(lam) || lam <= 0.0) return false;
+  norm *= 1.0 / lam;
+  s.lambda_fixed = lam / s.norm_free;
+  *norm_out = norm;
+  return true;
+}
+
+// accumulate_densities.jl:95-184 for a tree: segment densities and both bond ends
+__device__ void tree_accumulate(const DReq& r, const DSpecies& s, double norm, bool scaled) {
+  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C, N = s.n_seg;
+  const double mu = s.mu_species;
+  for (int K = threadIdx.x; K < Pt; K += blockDim.x) {
+    for (int g = 0; g < N; g++) {
+      const double lp = scaled ? log_prefactor(s, norm, g) : 0.0;
+      for (int ii = 0; ii < s.nst[g]; ii++) {
+        const int si = s.states[g * S + ii];
+        double sp = 0.0;
+        for (int q = 0; q < S; q++) sp += s.gP[tgp(s, P, g, ii, q) + K];
+        const double contr = scaled ? exp(lp - r.lambda[(size_t)si * P + K]) * sp
+                                    : norm * exp(mu - r.lambda[(size_t)si * P + K]) * sp;
+        double temp;
+        if (s.nch[g] == 0) {
+          temp = tgc_sum(s, P, K, g, ii, 0);
+        } else {
+          temp = 0.0;
+          for (int ic = 0; ic < s.nch[g]; ic++) {
+            const int c = s.child[g * C + ic];
+            double t1 = 0.0;
+            for (int jj = 0; jj < s.nst[c]; jj++) {
+              const int bond = bond_of(r, si, s.states[c * S + jj]);
+              double t2 = s.gC[tgc(s, P, g, ii, ic, jj) + K];
+              for (int oc = 0; oc < s.nch[g]; oc++)
+                if (oc != ic) t2 *= tgc_sum(s, P, K, g, ii, oc);
+              r.rho_bonds[(size_t)(bond * 2 + 0) * P + K] += contr * t2;
+              t1 += t2;
+            }
+            temp = t1;  // the last child's sum, as the reference
+          }
+        }
+        s.rho_seg[(size_t)(g * S + ii) * P + K] += contr * temp;
+      }
+    }
+    for (int c = 0; c < N; c++) {
+      const int p = s.parent[c];
+      if (p < 0) continue;
+      const double lp = scaled ? log_prefactor(s, norm, c) : 0.0;
+      for (int ii = 0; ii < s.nst[c]; ii++) {
+        const int si = s.states[c * S + ii];
+        double contr = scaled ? exp(lp - r.lambda[(size_t)si * P + K]) : norm * exp(mu - r.lambda[(size_t)si * P + K]);
+        for (int gc = 0; gc < s.nch[c]; gc++) contr *= tgc_sum(s, P, K, c, ii, gc);
+        for (int jj = 0; jj < s.nst[p]; jj++) {
+          const int bond = bond_of(r, si, s.states[p * S + jj]);
+          r.rho_bonds[(size_t)(bond * 2 + 1) * P + K] += contr * s.gP[tgp(s, P, c, ii, jj) + K];
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// one branched species: propagators, normalisation and densities (kept out of
+// line so that the linear-chain path of stage_densities carries none of it)
+__device__ __noinline__ bool tree_species(const DReq& r, int u, Shared sh) {
+  DSpecies s = r.sp[u];
+  tree_child(r, s, sh);
+  tree_parent(r, s, sh);
+  double norm;
+  if (!tree_norm(r, s, sh, &norm)) return false;
+  if (threadIdx.x == 0) {
+    DSpecies* w = const_cast<DSpecies*>(&r.sp[u]);
+    w->mu_species = s.mu_species;
+    w->lambda_fixed = s.lambda_fixed;
+  }
+  // the reference's prefactor norm e^{mu - lambda} overflows beyond e^709
+  const bool scaled = fabs(s.mu_species) + (double)(s.n_seg - 1) * fabs(log(s.normative)) > 600.0;
+  tree_accumulate(r, s, norm, scaled);
+  return true;
+}
+
 template <class R>
 __device__ __noinline__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
   const int P = r.NP;
@@ -1024,6 +1321,13 @@ __device__ __noinline__ bool stage_densities(const DReq& r, Shared sh, int* bad_
   for (int u = 0; u < r.NS; u++) {
     DSpecies s = r.sp[u];
     bool scaled = false;
+    if (s.tree) {  // branched topology: FP64 level walks
+      if (!tree_species(r, u, sh)) {
+        *bad_species = u;
+        return false;
+      }
+      continue;
+    }
     if (s.n_seg > 1) {
       scaled |= chain_child<R>(r, s, sh);
       scaled |= chain_parent<R>(r, s, sh);

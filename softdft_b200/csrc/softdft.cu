@@ -45,6 +45,9 @@ static size_t smem_bytes(int M);
 
 struct SpeciesHost {
   int n_seg, S, fixed;
+  bool tree = false;             // branched topology
+  int C = 1;                     // most children of a segment
+  std::vector<int> parent, nch, child, order;
   std::vector<int> states, nst, bnd, bslot, bslot_bond, eslot, eslot_bead;
   std::vector<double> md;
   double fixed_density, mu_species, normative, norm_free;
@@ -124,6 +127,7 @@ struct Plan {
   // layout
   size_t o_sig = 0, o_z = 0, o_dmu = 0, o_bonds = 0, o_grp = 0, o_grp_sig = 0, o_sp = 0;
   std::vector<size_t> o_states, o_nst, o_bnd, o_md, o_gC, o_gP, o_rho, o_expo, o_bslot, o_bslot_bond, o_eslot, o_eslot_bead;
+  std::vector<size_t> o_parent, o_nch, o_child, o_order;
   size_t o_Ext = 0, o_tr = 0, o_Csurf = 0, o_Wbond = 0, o_Wfmt = 0, o_Wmsa = 0, o_Wcoul = 0, o_tw = 0, o_twP = 0, o_twD = 0;
   size_t o_tw32 = 0, o_twP32 = 0, o_twD32 = 0, o_fbe32 = 0, o_slot_tab = 0;
   int prec = SDFT_PREC_FP64;
@@ -224,9 +228,29 @@ int plan_species(const sdft_system_desc* d, Plan& pl) {
     if (h.n_seg < 1 || h.S < 1 || h.S > kMaxStates)
       return set_err(SDFT_ERR_UNSUPPORTED, "segments >= 1 and 1 <= states <= 4 per segment are required");
     for (int g = 0; g < h.n_seg; g++) {
-      if (s.parent[g] != g - 1)
-        return set_err(SDFT_ERR_UNSUPPORTED, "the device solve supports linear chains (parent of segment g is g-1)");
+      if ((g == 0) != (s.parent[g] < 0) || s.parent[g] >= g)
+        return set_err(SDFT_ERR_ARG, "segment 0 must be the root and parents must precede their children");
+      if (s.parent[g] != g - 1) h.tree = true;
       if (s.n_states[g] < 1 || s.n_states[g] > h.S) return set_err(SDFT_ERR_ARG, "n_states out of range");
+    }
+    h.parent.assign(s.parent, s.parent + h.n_seg);
+    h.nch.assign(h.n_seg, 0);
+    for (int g = 1; g < h.n_seg; g++) h.nch[h.parent[g]]++;
+    h.C = 1;
+    for (int g = 0; g < h.n_seg; g++) h.C = std::max(h.C, h.nch[g]);
+    h.child.assign((size_t)h.n_seg * h.C, -1);
+    {
+      std::vector<int> cnt(h.n_seg, 0), depth(h.n_seg, 0);
+      for (int g = 1; g < h.n_seg; g++) {
+        h.child[(size_t)h.parent[g] * h.C + cnt[h.parent[g]]++] = g;
+        depth[g] = depth[h.parent[g]] + 1;
+      }
+      // levels by depth from the root, ascending segment index within a level (parse_topology.jl:41-44)
+      h.order.clear();
+      const int maxd = *std::max_element(depth.begin(), depth.end());
+      for (int l = 0; l <= maxd; l++)
+        for (int g = 0; g < h.n_seg; g++)
+          if (depth[g] == l) h.order.push_back(g);
     }
     h.nst.assign(s.n_states, s.n_states + h.n_seg);
     h.states.assign(s.states, s.states + (size_t)h.n_seg * h.S);
@@ -250,13 +274,23 @@ int plan_species(const sdft_system_desc* d, Plan& pl) {
         int st = h.states[(size_t)g * h.S + i];
         if (st < 0 || st >= NB) return set_err(SDFT_ERR_ARG, "state bead type out of range");
         if (g > 0)
-          for (int j = 0; j < h.nst[g - 1]; j++)
-            if (bond_lookup(pl.bonds, st, h.states[(size_t)(g - 1) * h.S + j]) < 0)
+          for (int j = 0; j < h.nst[h.parent[g]]; j++)
+            if (bond_lookup(pl.bonds, st, h.states[(size_t)h.parent[g] * h.S + j]) < 0)
               return set_err(SDFT_ERR_ARG, "bond missing from bond_types");
       }
-    // bond type between state i of segment g and state j of segment g + 1
+    if (h.tree) {
+      // the reference reads gC[p][oc][idx_j] for the other children of p and, for
+      // a grafted species whose first free segment is a leaf, gC[1][0][idx_i]:
+      // trees for which these leave the arrays fail there, and are refused here
+      for (int g = 0; g < h.n_seg; g++)
+        if (h.nch[g] >= 2 && (h.nch[g] > h.S || h.nst[g] > h.C))
+          return set_err(SDFT_ERR_UNSUPPORTED, "branched topology index out of range (children or states of a branch point)");
+      if (h.fixed >= 0 && h.nch[1] == 0 && h.nst[1] > h.C)
+        return set_err(SDFT_ERR_UNSUPPORTED, "branched topology index out of range (leaf next to the graft)");
+    }
+    // bond type between state i of segment g and state j of segment g + 1 (linear chains)
     h.bnd.assign((size_t)h.n_seg * h.S * h.S, -1);
-    for (int g = 0; g + 1 < h.n_seg; g++)
+    for (int g = 0; !h.tree && g + 1 < h.n_seg; g++)
       for (int i = 0; i < h.nst[g]; i++)
         for (int j = 0; j < h.nst[g + 1]; j++)
           h.bnd[((size_t)g * h.S + i) * h.S + j] =
@@ -340,6 +374,10 @@ void plan_layout(Plan& pl, bool history) {
   pl.o_bslot_bond.resize(NS);
   pl.o_eslot.resize(NS);
   pl.o_eslot_bead.resize(NS);
+  pl.o_parent.resize(NS);
+  pl.o_nch.resize(NS);
+  pl.o_child.resize(NS);
+  pl.o_order.resize(NS);
   for (int u = 0; u < NS; u++) {
     const SpeciesHost& h = pl.sp[u];
     pl.o_states[u] = lay.take<int>(h.states.size());
@@ -347,8 +385,12 @@ void plan_layout(Plan& pl, bool history) {
     pl.o_bnd[u] = lay.take<int>(h.bnd.size());
     pl.o_md[u] = lay.take<double>(h.md.size());
     size_t gsz = h.n_seg > 1 ? (size_t)h.n_seg * h.S * h.S * P : 0;
-    pl.o_gC[u] = lay.take<double>(gsz);
+    pl.o_gC[u] = lay.take<double>(gsz * (size_t)h.C);
     pl.o_gP[u] = lay.take<double>(gsz);
+    pl.o_parent[u] = lay.take<int>(h.parent.size());
+    pl.o_nch[u] = lay.take<int>(h.nch.size());
+    pl.o_child[u] = lay.take<int>(h.child.size());
+    pl.o_order[u] = lay.take<int>(h.order.size());
     pl.o_rho[u] = lay.take<double>((size_t)h.n_seg * h.S * P);
     pl.o_expo[u] = lay.take<int>((size_t)2 * h.n_seg);
     pl.o_bslot[u] = lay.take<int>(h.bslot.size());
@@ -530,6 +572,12 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
     s.eslot_bead = (const int*)at(pl.o_eslot_bead[u]);
     s.nbslot = (int)h.bslot_bond.size();
     s.neslot = (int)h.eslot_bead.size();
+    s.tree = h.tree ? 1 : 0;
+    s.C = h.C;
+    s.parent = (const int*)at(pl.o_parent[u]);
+    s.nch = (const int*)at(pl.o_nch[u]);
+    s.child = (const int*)at(pl.o_child[u]);
+    s.order = (const int*)at(pl.o_order[u]);
   }
   DReq r{};
   r.NP = pl.P;
@@ -618,6 +666,10 @@ cudaError_t plan_upload(const sdft_system_desc* d, const Plan& pl, char* base, c
     up(pl.o_nst[u], h.nst.data(), sizeof(int) * h.nst.size());
     up(pl.o_bnd[u], h.bnd.data(), sizeof(int) * h.bnd.size());
     up(pl.o_md[u], h.md.data(), sizeof(double) * h.md.size());
+    up(pl.o_parent[u], h.parent.data(), sizeof(int) * h.parent.size());
+    up(pl.o_nch[u], h.nch.data(), sizeof(int) * h.nch.size());
+    up(pl.o_child[u], h.child.data(), sizeof(int) * h.child.size());
+    up(pl.o_order[u], h.order.data(), sizeof(int) * h.order.size());
     up(pl.o_bslot[u], h.bslot.data(), sizeof(int) * h.bslot.size());
     up(pl.o_bslot_bond[u], h.bslot_bond.data(), sizeof(int) * h.bslot_bond.size());
     up(pl.o_eslot[u], h.eslot.data(), sizeof(int) * h.eslot.size());

@@ -77,6 +77,28 @@ def _diblock_odd():
 CASES["diblock_1001"] = _diblock_odd()
 
 
+# branched chains (parse_topology.jl syntax: a parenthesised run is a side branch)
+def _branched(seq, **kw):
+    ds = small_slit(**kw)
+    ds["species"][0]["sequence"] = seq
+    return ds
+
+
+def _branched_brush():
+    ds = workloads.grafted_brush(256, 0.05, 6, 0.05, 4.5, 7.0, 0.01)
+    ds["species"][0]["sequence"] = ds["species"][1]["sequence"] = "AA(AA)AA"
+    return ds
+
+
+CASES["branched_acid"] = _branched("AA(AA)AA")
+CASES["branched_two_points"] = _branched("AAA(A)AAA(AA)A")
+CASES["branched_brush"] = _branched_brush()
+CASES["branched_1001"] = _branched("AA(AA)AA", np_=1001, dz=0.02)
+# the branched slit converges under the reference's Anderson driver at a smaller mixing
+CASES["branched_acid_mix5e-4"] = _branched("AA(AA)AA")
+CASES["branched_acid_mix5e-4"]["numerical"]["mixing_max"] = 5e-4
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_objective_matches_oracle(name):
     dft = descriptor(CASES[name])
@@ -117,7 +139,8 @@ def test_picard_trajectory_matches():
     assert abs(eg - eo) / eo < 1e-10
 
 
-@pytest.mark.parametrize("name", ["acid_salt", "brush", "grid_1000", "brush_600", "grid_1001", "brush_999"])
+@pytest.mark.parametrize("name", ["acid_salt", "brush", "grid_1000", "brush_600", "grid_1001", "brush_999",
+                                  "branched_acid_mix5e-4", "branched_brush"])
 def test_converged_state_matches(name):
     ds = copy.deepcopy(CASES[name])
     ds["numerical"]["tole"] = 1e-10
@@ -197,3 +220,12 @@ def test_unsupported_grids_are_refused(np_, why):
         native.DeviceSystem(dft.descriptor)
     assert e.value.code == native.SDFT_ERR_UNSUPPORTED
     assert why in str(e.value)
+
+
+def test_branched_topology_beyond_the_reference_arrays_is_refused():
+    """A branch point with more children than states: the reference's
+    other-children index (parent_propagators.jl:150) leaves its array."""
+    dft = descriptor(_branched("A(AA)(AA)A"))
+    with pytest.raises(native.SdftError) as e:
+        native.DeviceSystem(dft.descriptor)
+    assert e.value.code == native.SDFT_ERR_UNSUPPORTED and "index out of range" in str(e.value)
