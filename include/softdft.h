@@ -240,6 +240,27 @@ int sdft_bulk_eval(const sdft_bulk_system* sys, const double* rho_species, const
                    const double* lng_in, double* rho_segments, double* rho_beads, double* rho_bonds,
                    double* mu_species, double* mu_ex, double* lng, double* xi);
 
+/* input.yaml to a request on the host, without a Julia or Python host.  No
+ * single reference counterpart: this is the host pipeline of iDFT
+ * (src/iDFT/iDFT.jl:24-40: YAML.load_file, iLST, geometry_system, setup_iDFT),
+ * i.e. the molecular system (src/molecular_system/setup/setup_molsys.jl:48-75),
+ * the bulk solve (src/iLST/evaluation/objective/solver_bulkstate.jl:31-104) and
+ * the 1D slit with its fixed segments, restated in C++.
+ * sdft_input_from_yaml: parses the text and builds the descriptor; errors come
+ *   back as SDFT_ERR_ARG / SDFT_ERR_UNSUPPORTED with the reference's message in
+ *   sdft_last_error().  Host only.
+ * sdft_input_descriptor: the descriptor for sdft_request_create; it stays valid
+ *   until sdft_input_destroy.
+ * sdft_input_numerics: the numerical section with the defaults of
+ *   AndersonMixing.jl:74-79.
+ * sdft_input_bulk_stats: iterations and max-norm residual of the bulk solve. */
+typedef struct sdft_input sdft_input;
+int sdft_input_from_yaml(const char* yaml_text, sdft_input** out);
+const sdft_system_desc* sdft_input_descriptor(const sdft_input* in);
+int sdft_input_numerics(const sdft_input* in, sdft_numerics* out);
+int sdft_input_bulk_stats(const sdft_input* in, int32_t* iterations, double* residual);
+int sdft_input_destroy(sdft_input* in);
+
 /* Bytes of the static device array behind sdft_objective_noalloc (16 MiB). */
 #define SDFT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 

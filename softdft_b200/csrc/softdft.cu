@@ -32,6 +32,8 @@ static int set_err(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
+// the same record for the host-only translation units (input.cpp)
+int sdft_record_error(int code, const std::string& msg) { return set_err(code, msg); }
 
 #define CUDA_TRY(expr)                                                                 \
   do {                                                                                 \

@@ -27,7 +27,8 @@ EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_num
            "sdft_get_state", "sdft_objective", "sdft_solve", "sdft_get_densities", "sdft_grand_potential",
            "sdft_num_species", "sdft_solve_batch", "sdft_last_batch_stats", "sdft_server_create",
            "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll", "sdft_bulk_eval",
-           "sdft_grid_supported"]
+           "sdft_grid_supported", "sdft_input_from_yaml", "sdft_input_descriptor", "sdft_input_numerics",
+           "sdft_input_bulk_stats", "sdft_input_destroy"]
 
 
 class SdftError(RuntimeError):
@@ -243,3 +244,51 @@ class Server:
             self._held.pop(int(tags[i]), None)
             out.append((int(tags[i]), int(st[i]), int(it[i]), float(err[i]), float(dms[i])))
         return out
+
+
+class Input:
+    """A request parsed from input.yaml text by the library's host pipeline
+    (sdft_input_from_yaml); ``descriptor()`` feeds DeviceSystem."""
+
+    def __init__(self, yaml_text: str):
+        L = lib()
+        L.sdft_input_from_yaml.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+        L.sdft_input_descriptor.restype = C.c_void_p
+        L.sdft_input_descriptor.argtypes = [C.c_void_p]
+        L.sdft_input_destroy.argtypes = [C.c_void_p]
+        self.h = C.c_void_p()
+        _check(L.sdft_input_from_yaml(yaml_text.encode(), C.byref(self.h)))
+
+    def descriptor(self):
+        from .host.descriptor import Descriptor, SystemDesc
+        d = SystemDesc.from_address(lib().sdft_input_descriptor(self.h))
+        out = Descriptor(desc=d, keep=[self], np_=d.np, nb=d.nb, mb=d.mb, n_species=d.n_species)
+        for u in range(d.n_species):
+            sp = d.species[u]
+            out.n_seg.append(sp.n_seg)
+            out.max_states.append(sp.max_states)
+            out.fixed_coord.append(np.ctypeslib.as_array(sp.fixed_coord, (sp.n_seg,)).copy())
+            out.mu_species.append(sp.mu_species)
+        return out
+
+    def numerics(self):
+        from .host.descriptor import Numerics
+        n = Numerics()
+        _check(lib().sdft_input_numerics(self.h, C.byref(n)))
+        return n
+
+    def bulk_stats(self):
+        it, res = C.c_int32(), C.c_double()
+        _check(lib().sdft_input_bulk_stats(self.h, C.byref(it), C.byref(res)))
+        return int(it.value), float(res.value)
+
+    def close(self):
+        if self.h:
+            lib().sdft_input_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
