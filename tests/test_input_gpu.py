@@ -15,7 +15,7 @@ from tests.helpers import rel
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("np_", [256, 251])
+@pytest.mark.parametrize("np_", [256, 243])
 def test_yaml_request_solves_like_the_python_request(np_):
     ds = workloads.weak_acid_slit(np_, 0.05, 8, 4.5, 7.0, 0.1, 0.3)
     ds["numerical"] = dict(ds["numerical"], tole=1e-10, max_iters=8000)
