@@ -29,6 +29,10 @@ CASES = {
     "brush": workloads.grafted_brush(256, 0.05, 10, 0.05, 4.5, 7.0, 0.01),
     "long_diblock": workloads.diblock_slit(1024),
     "plain_slit": workloads.plain_slit(),
+    # FP32 mixed-radix transforms: an even grid (M = 500) and an odd one (M = 1001, complex FFT of real data)
+    "grid_1000": small_slit(np_=1000, dz=0.02),
+    "grid_1001": small_slit(np_=1001, dz=0.02),
+    "brush_999": workloads.grafted_brush(999, 0.05, 10, 0.05, 4.5, 7.0, 0.01),
 }
 
 
@@ -43,7 +47,7 @@ def test_mixed_objective_close_to_fp64(name):
     assert np.all(np.isfinite(b)) and d < 1e-5
 
 
-@pytest.mark.parametrize("name", ["brush", "plain_slit"])
+@pytest.mark.parametrize("name", ["brush", "plain_slit", "brush_999"])
 def test_mixed_solve_reaches_fp64_fixed_point(name):
     ds = copy.deepcopy(CASES[name])
     ds["numerical"]["tole"] = 1e-10
