@@ -636,22 +636,33 @@ __device__ __forceinline__ C mid_inverse(typename Cx<C>::R eh, typename Cx<C>::R
     const int t = item_t<GEN>(it, cnt_, lH_), k = it - t * cnt_;        \
     auto* zb = (c).z + (size_t)t * (c).stride;
 
-// ---- odd P (general build) ---------------------------------------------------
-// The Makhoul sequence v[q] of an odd P is transformed by a complex FFT of
-// M = P points with zero imaginary parts, V[k] = sum_q v[q] e^{-2 pi i q k / P}.
-// Then C[0] = Re V[0], C[k] = Re(d_k V[k]) and C[P-k] = Re(d_{P-k} conj V[k])
-// with d_k = e^{-i pi k / 2P} (twD).  The inverse builds V'[0] = E[0],
-// V'[k] = conj(d_k) (E[k] - i E[P-k]), V'[P-k] = conj V'[k]; the real part of
-// the unscaled inverse FFT divided by P is v'.  The grid-point pairs (K, K+1)
-// run over the padded stride P + 1: the pad sample K + 1 = P is not loaded and
-// is stored as 0.
+// ---- odd P (general build): two real transforms per complex FFT -------------
+// Transforms 2b and 2b+1 share buffer b as the real and the imaginary part of
+// one complex FFT of M = P points of their Makhoul sequences, Z = V_{2b} + i V_{2b+1};
+// each V is Hermitian, so V_{2b}[k] = (Z[k] + conj Z[P-k]) / 2 and
+// V_{2b+1}[k] = -i (Z[k] - conj Z[P-k]) / 2.  Per transform, C[0] = Re V[0],
+// C[k] = Re(d_k V[k]) and C[P-k] = Re(d_{P-k} conj V[k]) with d_k = e^{-i pi k / 2P}
+// (twD).  The inverse builds V'[0] = E[0] and V'[k] = conj(d_k) (E[k] - i E[P-k])
+// per transform, Z'[k] = V'_{2b}[k] + i V'_{2b+1}[k] and
+// Z'[P-k] = conj V'_{2b}[k] + i conj V'_{2b+1}[k]; the real and imaginary parts of
+// the unscaled inverse FFT, divided by P, are the two outputs.  A lone last
+// transform (odd nT) has a zero partner.  The grid-point pairs (K, K+1) run over
+// the padded stride P + 1: the pad sample K + 1 = P is not loaded and is stored as 0.
 __device__ __forceinline__ int makhoul_q(int K, int P) { return (K & 1) ? (P - 1 - (K >> 1)) : (K >> 1); }
+
+// component t & 1 of buffer t >> 1 at slot s
+template <class C>
+__device__ __forceinline__ typename Cx<C>::R& odd_part(const FftCtxT<C>& c, int t, int s) {
+  using R = typename Cx<C>::R;
+  return reinterpret_cast<R*>(c.z + (size_t)(t >> 1) * c.stride + fpad(s))[t & 1];
+}
 
 template <class F>
 __device__ __forceinline__ void load_b_odd(const FftCtx& c, int nT, F f) {
-  for (int it = threadIdx.x; it < nT * c.P; it += blockDim.x) {
+  const int nT2 = (nT + 1) & ~1;
+  for (int it = threadIdx.x; it < nT2 * c.P; it += blockDim.x) {
     const int t = it / c.P, K = it - t * c.P;
-    c.z[(size_t)t * c.stride + fpad(fslot<true>(c, makhoul_q(K, c.P)))] = make_double2(f(t, K), 0.0);
+    odd_part(c, t, fslot<true>(c, makhoul_q(K, c.P))) = t < nT ? f(t, K) : 0.0;
   }
 }
 
@@ -659,20 +670,24 @@ template <class S>
 __device__ __forceinline__ void store_b_odd(const FftCtx& c, int nT, double scale, S st) {
   for (int it = threadIdx.x; it < nT * c.P; it += blockDim.x) {
     const int t = it / c.P, K = it - t * c.P;
-    st(t, K, c.z[(size_t)t * c.stride + fpad(fslot<true>(c, makhoul_q(K, c.P)))].x * scale);
+    st(t, K, odd_part(c, t, fslot<true>(c, makhoul_q(K, c.P))) * scale);
   }
 }
 
 template <class C, class F2>
 __device__ __forceinline__ void load_b2_odd(const FftCtxT<C>& c, int nT, F2 f2) {
   using R = typename Cx<C>::R;
-  const int np = (c.P + 1) >> 1;
-  for (int b = threadIdx.x; b < nT * np; b += blockDim.x) {
+  const int np = (c.P + 1) >> 1, nT2 = (nT + 1) & ~1;
+  for (int b = threadIdx.x; b < nT2 * np; b += blockDim.x) {
     const int t = b / np, kp = b - t * np, K = 2 * kp;
-    const auto v = f2(t, K);
-    C* zb = c.z + (size_t)t * c.stride;
-    zb[fpad(fslot<true>(c, kp))] = Cx<C>::make((R)v.x, (R)0);
-    if (K + 1 < c.P) zb[fpad(fslot<true>(c, c.P - 1 - kp))] = Cx<C>::make((R)v.y, (R)0);
+    R v0 = (R)0, v1 = (R)0;
+    if (t < nT) {
+      const auto v = f2(t, K);
+      v0 = (R)v.x;
+      v1 = (R)v.y;
+    }
+    odd_part(c, t, fslot<true>(c, kp)) = v0;
+    if (K + 1 < c.P) odd_part(c, t, fslot<true>(c, c.P - 1 - kp)) = v1;
   }
 }
 
@@ -682,19 +697,33 @@ __device__ __forceinline__ void store_b2_odd(const FftCtxT<C>& c, int nT, typena
   const int np = (c.P + 1) >> 1;
   for (int b = threadIdx.x; b < nT * np; b += blockDim.x) {
     const int t = b / np, kp = b - t * np, K = 2 * kp;
-    const C* zb = c.z + (size_t)t * c.stride;
-    const R y0 = zb[fpad(fslot<true>(c, kp))].x;
-    const R y1 = (K + 1 < c.P) ? zb[fpad(fslot<true>(c, c.P - 1 - kp))].x : (R)0;
+    const R y0 = odd_part(c, t, fslot<true>(c, kp));
+    const R y1 = (K + 1 < c.P) ? odd_part(c, t, fslot<true>(c, c.P - 1 - kp)) : (R)0;
     const auto a = pre2(t, K);
     put2(t, K, Cx<C>::make(y0 * scale, y1 * scale), a);
   }
 }
 
-// C[k], C[P-k] from V[k] (natural order after the forward FFT), k in [1, P/2)
+// the two Hermitian spectra packed in Z[k], Z[P-k] (k >= 1)
 template <class C>
-__device__ __forceinline__ void odd_forward(C A, C dk, C dpk, typename Cx<C>::R* ck, typename Cx<C>::R* cpk) {
-  *ck = cmul(dk, A).x;
-  *cpk = cmul(dpk, conj2(A)).x;
+__device__ __forceinline__ void odd_unpack(C A, C B, C* V0, C* V1) {
+  using R = typename Cx<C>::R;
+  const R h = (R)0.5;
+  const C S = add2(A, conj2(B)), D = sub2(A, conj2(B));
+  *V0 = scl2(S, h);
+  *V1 = Cx<C>::make(h * D.y, -h * D.x);  // -i D / 2
+}
+// Z'[k], Z'[P-k] from the two inverse spectra
+template <class C>
+__device__ __forceinline__ void odd_pack(C W0, C W1, C* Zk, C* Zpk) {
+  *Zk = Cx<C>::make(W0.x - W1.y, W0.y + W1.x);
+  *Zpk = Cx<C>::make(W0.x + W1.y, -W0.y + W1.x);
+}
+// C[k], C[P-k] of one spectrum; V'[k] from E[k], E[P-k]
+template <class C>
+__device__ __forceinline__ void odd_forward(C V, C dk, C dpk, typename Cx<C>::R* ck, typename Cx<C>::R* cpk) {
+  *ck = cmul(dk, V).x;
+  *cpk = cmul(dpk, conj2(V)).x;
 }
 template <class C>
 __device__ __forceinline__ C odd_inverse(typename Cx<C>::R ek, typename Cx<C>::R epk, C dk) {
@@ -703,20 +732,29 @@ __device__ __forceinline__ C odd_inverse(typename Cx<C>::R ek, typename Cx<C>::R
 
 template <class F, class E>
 __device__ __forceinline__ void dct2_forward_odd(const FftCtx& c, int nT, F f, E emit) {
-  const int P = c.P, cnt = (P + 1) >> 1;
+  const int P = c.P, cnt = (P + 1) >> 1, nb = (nT + 1) >> 1;
   __syncthreads();
   load_b_odd(c, nT, f);
-  fft_fwd_b(c, nT);
-  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
-    const int t = it / cnt, k = it - t * cnt;
-    const double2 A = c.z[(size_t)t * c.stride + fpad(k)];
+  fft_fwd_b(c, nb);
+  for (int it = threadIdx.x; it < nb * cnt; it += blockDim.x) {
+    const int b = it / cnt, k = it - b * cnt, t0 = 2 * b, t1 = t0 + 1;
+    const double2* zb = c.z + (size_t)b * c.stride;
     if (k == 0) {
-      emit(t, 0, A.x);
+      emit(t0, 0, zb[0].x);
+      if (t1 < nT) emit(t1, 0, zb[0].y);
     } else {
+      double2 V0, V1;
+      odd_unpack(zb[fpad(k)], zb[fpad(P - k)], &V0, &V1);
+      const double2 dk = __ldg(&c.twD[k]), dpk = __ldg(&c.twD[P - k]);
       double ck, cpk;
-      odd_forward(A, __ldg(&c.twD[k]), __ldg(&c.twD[P - k]), &ck, &cpk);
-      emit(t, k, ck);
-      emit(t, P - k, cpk);
+      odd_forward(V0, dk, dpk, &ck, &cpk);
+      emit(t0, k, ck);
+      emit(t0, P - k, cpk);
+      if (t1 < nT) {
+        odd_forward(V1, dk, dpk, &ck, &cpk);
+        emit(t1, k, ck);
+        emit(t1, P - k, cpk);
+      }
     }
   }
   __syncthreads();
@@ -724,46 +762,53 @@ __device__ __forceinline__ void dct2_forward_odd(const FftCtx& c, int nT, F f, E
 
 template <class G, class S>
 __device__ __forceinline__ void dct2_inverse_odd(const FftCtx& c, int nT, G get, S store) {
-  const int P = c.P, cnt = (P + 1) >> 1;
+  const int P = c.P, cnt = (P + 1) >> 1, nb = (nT + 1) >> 1;
   __syncthreads();
-  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
-    const int t = it / cnt, k = it - t * cnt;
-    double2* zb = c.z + (size_t)t * c.stride;
+  for (int it = threadIdx.x; it < nb * cnt; it += blockDim.x) {
+    const int b = it / cnt, k = it - b * cnt, t0 = 2 * b, t1 = t0 + 1;
+    double2* zb = c.z + (size_t)b * c.stride;
     if (k == 0) {
-      zb[0] = make_double2(get(t, 0), 0.0);
+      zb[0] = make_double2(get(t0, 0), t1 < nT ? get(t1, 0) : 0.0);
     } else {
-      const double2 V = odd_inverse(get(t, k), get(t, P - k), __ldg(&c.twD[k]));
-      zb[fpad(k)] = V;
-      zb[fpad(P - k)] = conj2(V);
+      const double2 dk = __ldg(&c.twD[k]);
+      const double2 W0 = odd_inverse(get(t0, k), get(t0, P - k), dk);
+      const double2 W1 = t1 < nT ? odd_inverse(get(t1, k), get(t1, P - k), dk) : make_double2(0.0, 0.0);
+      odd_pack(W0, W1, &zb[fpad(k)], &zb[fpad(P - k)]);
     }
   }
-  fft_inv_b(c, nT);
+  fft_inv_b(c, nb);
   store_b_odd(c, nT, 1.0 / (double)P, store);
   __syncthreads();
 }
 
 template <class F, class W, class S>
 __device__ __forceinline__ void dct2_convolve_odd(const FftCtx& c, int nT, F f, W wgt, S store) {
-  const int P = c.P, cnt = (P + 1) >> 1;
+  const int P = c.P, cnt = (P + 1) >> 1, nb = (nT + 1) >> 1;
   __syncthreads();
   load_b_odd(c, nT, f);
-  fft_fwd_b(c, nT);
-  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
-    const int t = it / cnt, k = it - t * cnt;
-    double2* zb = c.z + (size_t)t * c.stride;
-    const double2 A = zb[fpad(k)];
+  fft_fwd_b(c, nb);
+  for (int it = threadIdx.x; it < nb * cnt; it += blockDim.x) {
+    const int b = it / cnt, k = it - b * cnt, t0 = 2 * b, t1 = t0 + 1;
+    double2* zb = c.z + (size_t)b * c.stride;
     if (k == 0) {
-      zb[0] = make_double2(A.x * wgt(t, 0), 0.0);
+      const double2 A = zb[0];
+      zb[0] = make_double2(A.x * wgt(t0, 0), t1 < nT ? A.y * wgt(t1, 0) : 0.0);
     } else {
-      const double2 dk = __ldg(&c.twD[k]);
+      double2 V0, V1;
+      odd_unpack(zb[fpad(k)], zb[fpad(P - k)], &V0, &V1);
+      const double2 dk = __ldg(&c.twD[k]), dpk = __ldg(&c.twD[P - k]);
       double ck, cpk;
-      odd_forward(A, dk, __ldg(&c.twD[P - k]), &ck, &cpk);
-      const double2 V = odd_inverse(ck * wgt(t, k), cpk * wgt(t, P - k), dk);
-      zb[fpad(k)] = V;
-      zb[fpad(P - k)] = conj2(V);
+      odd_forward(V0, dk, dpk, &ck, &cpk);
+      const double2 W0 = odd_inverse(ck * wgt(t0, k), cpk * wgt(t0, P - k), dk);
+      double2 W1 = make_double2(0.0, 0.0);
+      if (t1 < nT) {
+        odd_forward(V1, dk, dpk, &ck, &cpk);
+        W1 = odd_inverse(ck * wgt(t1, k), cpk * wgt(t1, P - k), dk);
+      }
+      odd_pack(W0, W1, &zb[fpad(k)], &zb[fpad(P - k)]);
     }
   }
-  fft_inv_b(c, nT);
+  fft_inv_b(c, nb);
   store_b_odd(c, nT, 1.0 / (double)P, store);
   __syncthreads();
 }
@@ -771,26 +816,32 @@ __device__ __forceinline__ void dct2_convolve_odd(const FftCtx& c, int nT, F f, 
 template <class C, class F2, class W, class A2, class S2>
 __device__ __forceinline__ void dct2_convolve_b2_odd(const FftCtxT<C>& c, int nT, F2 f2, W wgt, A2 pre2, S2 put2) {
   using R = typename Cx<C>::R;
-  const int P = c.P, cnt = (P + 1) >> 1;
+  const int P = c.P, cnt = (P + 1) >> 1, nb = (nT + 1) >> 1;
   __syncthreads();
   load_b2_odd(c, nT, f2);
-  fft_fwd_b(c, nT);
-  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
-    const int t = it / cnt, k = it - t * cnt;
-    C* zb = c.z + (size_t)t * c.stride;
-    const C A = zb[fpad(k)];
+  fft_fwd_b(c, nb);
+  for (int it = threadIdx.x; it < nb * cnt; it += blockDim.x) {
+    const int b = it / cnt, k = it - b * cnt, t0 = 2 * b, t1 = t0 + 1;
+    C* zb = c.z + (size_t)b * c.stride;
     if (k == 0) {
-      zb[0] = Cx<C>::make(A.x * (R)wgt(t, 0), (R)0);
+      const C A = zb[0];
+      zb[0] = Cx<C>::make(A.x * (R)wgt(t0, 0), t1 < nT ? A.y * (R)wgt(t1, 0) : (R)0);
     } else {
-      const C dk = __ldg(&c.twD[k]);
+      C V0, V1;
+      odd_unpack(zb[fpad(k)], zb[fpad(P - k)], &V0, &V1);
+      const C dk = __ldg(&c.twD[k]), dpk = __ldg(&c.twD[P - k]);
       R ck, cpk;
-      odd_forward(A, dk, __ldg(&c.twD[P - k]), &ck, &cpk);
-      const C V = odd_inverse(ck * (R)wgt(t, k), cpk * (R)wgt(t, P - k), dk);
-      zb[fpad(k)] = V;
-      zb[fpad(P - k)] = conj2(V);
+      odd_forward(V0, dk, dpk, &ck, &cpk);
+      const C W0 = odd_inverse(ck * (R)wgt(t0, k), cpk * (R)wgt(t0, P - k), dk);
+      C W1 = Cx<C>::make((R)0, (R)0);
+      if (t1 < nT) {
+        odd_forward(V1, dk, dpk, &ck, &cpk);
+        W1 = odd_inverse(ck * (R)wgt(t1, k), cpk * (R)wgt(t1, P - k), dk);
+      }
+      odd_pack(W0, W1, &zb[fpad(k)], &zb[fpad(P - k)]);
     }
   }
-  fft_inv_b(c, nT);
+  fft_inv_b(c, nb);
   store_b2_odd(c, nT, (R)1 / (R)P, pre2, put2);
   __syncthreads();
 }

@@ -590,7 +590,8 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.MB = pl.MB;
   r.NS = pl.NS;
   r.funcs = (int)d->functionals;
-  r.TB = tb_for(pl.M);
+  // odd grids pack two real transforms into each buffer
+  r.TB = pl.P != pl.Pt ? std::min(kMaxTB, 2 * tb_for(pl.M)) : tb_for(pl.M);
   r.ngrp = (int)pl.grp_sig.size();
   r.prec = pl.prec;
   r.dz = d->bin_width;
