@@ -1226,7 +1226,6 @@ extern "C" int sdft_server_poll(sdft_server_t sv, int64_t* tags, int32_t* status
 
 extern "C" int sdft_get_densities(sdft_handle h, double* const* rho_segments, double* rho_beads_K, double* rho_bonds_K) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
-  const size_t P = h->NP;
   if (rho_segments) {
     std::vector<DSpecies> dsp(h->NS);
     CUDA_TRY(cudaMemcpyAsync(dsp.data(), h->h.sp, sizeof(DSpecies) * h->NS, cudaMemcpyDeviceToHost, h->stream));
