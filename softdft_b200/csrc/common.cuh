@@ -72,6 +72,7 @@ struct DReq {
   int NP, M, L;       // stride of per-point arrays, FFT length, log2(M) (power-of-two M)
   int NPt;            // grid points: NP for even grids, NP - 1 for odd ones (the last point pads)
   int gen;            // 1: M is not a power of two (mixed-radix tables below)
+  int has_tree;       // 1: a species has a branched topology
   int nrad;           // general length: number of radices
   int rad[kMaxRadices];  // general length: radices r_0 .. r_{nrad-1}, M = their product
   int NB, MB, NS;

@@ -33,6 +33,9 @@ __device__ __forceinline__ const double* xs_psi(const DReq& r, const double* x) 
   return x + (size_t)r.NP * (r.NB + 2 * r.MB);
 }
 __device__ __forceinline__ size_t off_psic(const DReq& r) { return (size_t)r.NP * (r.NB + 2 * r.MB + 1); }
+// grid points: odd grids (their stride NP is one more) only run in the general
+// build, so the power-of-two build reads the stride itself
+__device__ __forceinline__ int grid_points(const DReq& r) { return SDFT_FFT_GEN ? r.NPt : r.NP; }
 
 __device__ __forceinline__ double dist2_grid(int K, int c, double dz) {
   double d = (double)(K - c) * dz;
@@ -76,7 +79,7 @@ __device__ void stage_bond_factors(const DReq& r, Shared sh, bool fp32) {
     const double fin = exp(-r.lambda[(size_t)j * P + K] + l / 2.0) * r.trapez[(size_t)j * P + K];
     r.fbe[idx] = fin;
     r.fbe[(size_t)nbe * P + idx] = exp(l / 2.0);
-    if (K < r.NPt && isfinite(fin)) mx = fmax(mx, fin);
+    if (K < grid_points(r) && isfinite(fin)) mx = fmax(mx, fin);
   }
   for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) r.elam[idx] = exp(-r.lambda[idx]);
   if (fp32 && r.fbe32) {
@@ -175,7 +178,7 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
         const double renorm = 2.0 * Dij;
         const double el = exp(lng_pi[Kp] / 2.0);
         double acc = 0.0;
-        for (int K1 = threadIdx.x; K1 < r.NPt; K1 += blockDim.x) {
+        for (int K1 = threadIdx.x; K1 < grid_points(r); K1 += blockDim.x) {
           double d2 = dist2_grid(K1, Kp, r.dz);
           if (d2 <= Dij2) {
             double f = exp(-lam_j[K1] + lng_pj[K1] / 2.0);
@@ -247,7 +250,7 @@ __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
           for (int q = 0; q < S * S; q++) gC[((size_t)p * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
-    const int e = renormalise_block(gC + (size_t)p * S * S * P, S * S, P, r.NPt, sh.red, sizeof(R) == 4);
+    const int e = renormalise_block(gC + (size_t)p * S * S * P, S * S, P, grid_points(r), sh.red, sizeof(R) == 4);
     e_child += e + sc;
     scaled |= (e + sc) != 0;
     if (threadIdx.x == 0) s.expo[p] = e_child;
@@ -307,7 +310,7 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
         double tq = 0.0;
         for (int q = 0; q < S; q++) tq += gpp[(size_t)q * P + Kp];
         const double f = exp(-r.lambda[(size_t)sj * P + Kp] + lng_pj[Kp] / 2.0) * tq;
-        for (int K1 = threadIdx.x; K1 < r.NPt; K1 += blockDim.x) {
+        for (int K1 = threadIdx.x; K1 < grid_points(r); K1 += blockDim.x) {
           double d2 = dist2_grid(K1, Kp, r.dz);
           if (d2 <= Dij2) {
             double v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm / s.normative;
@@ -366,7 +369,7 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
           for (int q = 0; q < S * S; q++) gP[((size_t)c * S * S + q) * P + K] = 0.0;
     }
     __syncthreads();
-    const int e = renormalise_block(gP + (size_t)c * S * S * P, S * S, P, r.NPt, sh.red, sizeof(R) == 4);
+    const int e = renormalise_block(gP + (size_t)c * S * S * P, S * S, P, grid_points(r), sh.red, sizeof(R) == 4);
     e_parent += e + sc;
     scaled |= (e + sc) != 0;
     if (threadIdx.x == 0) s.expo[N + c] = e_parent;
@@ -387,7 +390,7 @@ __device__ bool chain_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_o
     s.mu_species = 0.0;
     const int parent = 1;  // first free segment
     double acc = 0.0;
-    for (int K = threadIdx.x; K < r.NPt; K += blockDim.x) {
+    for (int K = threadIdx.x; K < grid_points(r); K += blockDim.x) {
       for (int ii = 0; ii < s.nst[parent]; ii++) {
         const int si = s.states[parent * S + ii];
         double sp = 0.0;
@@ -1047,7 +1050,7 @@ __device__ __forceinline__ int bond_of(const DReq& r, int a, int b) {
 // max-path-distance mask of a grafted species: entries of segment g farther
 // from the graft point than its path distance are zeroed (child_propagators.jl:147-157)
 __device__ void tree_mask(const DReq& r, const DSpecies& s, double* a, int count_per_K, double md) {
-  const int P = r.NP, Pt = r.NPt;
+  const int P = r.NP, Pt = grid_points(r);
   const double md2 = md * md;
   for (int K = threadIdx.x; K < Pt; K += blockDim.x)
     if (dist2_grid(K, s.fixed, r.dz) > md2)
@@ -1055,7 +1058,7 @@ __device__ void tree_mask(const DReq& r, const DSpecies& s, double* a, int count
 }
 
 __device__ void tree_child(const DReq& r, const DSpecies& s, Shared sh) {
-  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C, N = s.n_seg;
+  const int P = r.NP, Pt = grid_points(r), S = s.S, C = s.C, N = s.n_seg;
   const double* lng = xs_lng(r, r.x);
   const double* fin = r.fbe;
   const double* fout = r.fbe + (size_t)2 * r.MB * P;
@@ -1123,7 +1126,7 @@ __device__ void tree_child(const DReq& r, const DSpecies& s, Shared sh) {
 }
 
 __device__ void tree_parent(const DReq& r, const DSpecies& s, Shared sh) {
-  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C, N = s.n_seg;
+  const int P = r.NP, Pt = grid_points(r), S = s.S, C = s.C, N = s.n_seg;
   const double* lng = xs_lng(r, r.x);
   const double* fin = r.fbe;
   const double* fout = r.fbe + (size_t)2 * r.MB * P;
@@ -1191,7 +1194,7 @@ __device__ void tree_parent(const DReq& r, const DSpecies& s, Shared sh) {
 
 // handle_fixed.jl:41-73 and :105-112 for a tree
 __device__ bool tree_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_out) {
-  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C;
+  const int P = r.NP, Pt = grid_points(r), S = s.S, C = s.C;
   double lam, norm;
   if (s.fixed >= 0) {
     norm = s.fixed_density;
@@ -1237,7 +1240,7 @@ __device__ bool tree_norm(const DReq& r, DSpecies& s, Shared sh, double* norm_ou
 
 // accumulate_densities.jl:95-184 for a tree: segment densities and both bond ends
 __device__ void tree_accumulate(const DReq& r, const DSpecies& s, double norm, bool scaled) {
-  const int P = r.NP, Pt = r.NPt, S = s.S, C = s.C, N = s.n_seg;
+  const int P = r.NP, Pt = grid_points(r), S = s.S, C = s.C, N = s.n_seg;
   const double mu = s.mu_species;
   for (int K = threadIdx.x; K < Pt; K += blockDim.x) {
     for (int g = 0; g < N; g++) {
@@ -1307,7 +1310,7 @@ __device__ __noinline__ bool tree_species(const DReq& r, int u, Shared sh) {
   return true;
 }
 
-template <class R>
+template <class R, bool TREES>
 __device__ __noinline__ bool stage_densities(const DReq& r, Shared sh, int* bad_species) {
   const int P = r.NP;
   unsigned fast_mask = 0;  // species whose bead densities accumulate_regs added
@@ -1321,7 +1324,7 @@ __device__ __noinline__ bool stage_densities(const DReq& r, Shared sh, int* bad_
   for (int u = 0; u < r.NS; u++) {
     DSpecies s = r.sp[u];
     bool scaled = false;
-    if (s.tree) {  // branched topology: FP64 level walks
+    if (TREES && s.tree) {  // branched topology: FP64 level walks
       if (!tree_species(r, u, sh)) {
         *bad_species = u;
         return false;
@@ -1471,7 +1474,7 @@ __device__ void fmt_weighted(const DReq& r, Shared sh, bool tpt1) {
         fc, nT,
         [&](int t, int q) {
           if (q == 0) return 0.0;
-          const int k = r.NPt - q;  // coefficient reversal over the grid points (not the stride)
+          const int k = grid_points(r) - q;  // coefficient reversal over the grid points (not the stride)
           double s = 0.0;
           for (int j = 0; j < NB; j++) {
             double c = r.Cb[(size_t)j * P + k] * r.Wfmt[((size_t)j * 3 + 2) * P + k];
@@ -1568,7 +1571,7 @@ __device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
         [&](int t, int k, double v) {
           const int q = g0 + t;
           if (q < 4) CD[(size_t)q * P + k] = v;
-          else if (k > 0) CD[(size_t)q * P + (r.NPt - k)] = v;
+          else if (k > 0) CD[(size_t)q * P + (grid_points(r) - k)] = v;
         });
   }
   // mu_ex coefficients (accumulate_mu_ex!, TPT1mfmt.jl:244-283)
@@ -1776,7 +1779,7 @@ __device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
 constexpr int kGammaLanes = 4;
 
 __device__ __noinline__ void msa_gamma_pass(const DReq& r, double* out) {
-  const int P = r.NP, Pt = r.NPt, nb = r.NB;  // stride, grid points
+  const int P = r.NP, Pt = grid_points(r), nb = r.NB;  // stride, grid points
   if (r.ngrp != 1) {
     for (int K = threadIdx.x; K < Pt; K += blockDim.x) {
       double rho[kMaxBeads];
@@ -1974,7 +1977,7 @@ __device__ double stage_neutrality(const DReq& r, Shared sh) {
         if (g == 0 && s.fixed >= 0) {
           if (threadIdx.x == 0) nn = rs[s.fixed];
         } else {
-          for (int K = threadIdx.x; K < r.NPt; K += blockDim.x) nn += rs[K] * r.trapez[(size_t)st * P + K] * r.dz;
+          for (int K = threadIdx.x; K < grid_points(r); K += blockDim.x) nn += rs[K] * r.trapez[(size_t)st * P + K] * r.dz;
         }
         part[2 * u] += nn;
         part[2 * u + 1] += nn * r.z[st];
@@ -2033,7 +2036,10 @@ __device__ bool objective(const DReq& r, Shared sh, bool fp32 = false) {
   stage_lambda(r);
   stage_bond_factors(r, sh, fp32);
   int bad = -1;
-  if (!(fp32 ? stage_densities<float>(r, sh, &bad) : stage_densities<double>(r, sh, &bad))) return false;
+  // requests with branched species run the instantiation that carries the tree path
+  const bool ok = r.has_tree ? stage_densities<double, true>(r, sh, &bad)
+                             : (fp32 ? stage_densities<float, false>(r, sh, &bad) : stage_densities<double, false>(r, sh, &bad));
+  if (!ok) return false;
   stage_rho_hat(r, sh);
   for (size_t q = threadIdx.x; q < (size_t)r.NB * P; q += blockDim.x) r.Cmu[q] = 0.0;
   for (size_t q = threadIdx.x; q < (size_t)r.MB * 2 * P; q += blockDim.x) r.Clng[q] = 0.0;
@@ -2064,7 +2070,7 @@ __device__ bool objective(const DReq& r, Shared sh, bool fp32 = false) {
   const double shift = stage_neutrality(r, sh);
   if (threadIdx.x == 0) g[off_psic(r)] = r.x[off_psic(r)] + shift;
   // the pad point of odd grids is not an unknown: G(x) keeps it at 0 there, as x does
-  if (r.NPt != P)
+  if (SDFT_FFT_GEN && r.NPt != P)
     for (int w = threadIdx.x; w < nout; w += blockDim.x) g[(size_t)w * P + r.NPt] = 0.0;
   __syncthreads();
   return true;

@@ -23,7 +23,7 @@ __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
     if (!(r.funcs & (tpt1 ? 0x2 : 0x1))) continue;
     fmt_weighted(r, sh, tpt1);
     double acc = 0.0;
-    for (int K = threadIdx.x; K < r.NPt; K += blockDim.x) {
+    for (int K = threadIdx.x; K < grid_points(r); K += blockDim.x) {
       double n0 = r.wa[K], n1 = r.wa[(size_t)P + K], n2 = r.wa[(size_t)2 * P + K], n3 = r.wa[(size_t)3 * P + K];
       double v1 = r.wa[(size_t)4 * P + K], v2 = r.wa[(size_t)5 * P + K];
       if (n3 > 0.95) {
@@ -57,7 +57,7 @@ __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
     msa_weighted(r, sh, tpt1);
     __syncthreads();
     double acc = 0.0;
-    for (int K = threadIdx.x; K < r.NPt; K += blockDim.x) {
+    for (int K = threadIdx.x; K < grid_points(r); K += blockDim.x) {
       double rho[kMaxBeads];
       for (int j = 0; j < NB; j++) rho[j] = r.wa[(size_t)j * P + K];
       const MsaGamma gm = gamma_msa_point(r, rho);
@@ -81,9 +81,9 @@ __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
   const double* lng = r.x + (size_t)P * NB;
   double a1 = 0.0, a2 = 0.0;
   for (size_t q = threadIdx.x; q < (size_t)NB * P; q += blockDim.x)
-    if ((int)(q % P) < r.NPt) a1 += r.rho_beads[q] * mu[q] * r.trapez[q];
+    if ((int)(q % P) < grid_points(r)) a1 += r.rho_beads[q] * mu[q] * r.trapez[q];
   for (size_t q = threadIdx.x; q < (size_t)2 * MB * P; q += blockDim.x)
-    if ((int)(q % P) < r.NPt) a2 += r.rho_bonds[q] * lng[q] / 2.0;
+    if ((int)(q % P) < grid_points(r)) a2 += r.rho_bonds[q] * lng[q] / 2.0;
   a1 = block_sum(a1, sh.red);
   a2 = block_sum(a2, sh.red);
   double om = ((fe - a1) + a2) * r.dz;
@@ -100,7 +100,7 @@ __device__ void grand_potential(const DReq& r, Shared sh, double* out) {
           if (threadIdx.x == 0) acc += rs[s.fixed] / (double)s.n_seg;
         } else {
           double nn = 0.0;
-          for (int K = threadIdx.x; K < r.NPt; K += blockDim.x) nn += rs[K] * r.trapez[(size_t)st * P + K] * r.dz;
+          for (int K = threadIdx.x; K < grid_points(r); K += blockDim.x) nn += rs[K] * r.trapez[(size_t)st * P + K] * r.dz;
           acc += nn / (double)s.n_seg;
         }
       }

@@ -614,6 +614,8 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.Wcoul = (const double*)at(pl.o_Wcoul);
   r.tw = (const double2*)at(pl.o_tw);
   r.gen = pl.gen ? 1 : 0;
+  r.has_tree = 0;
+  for (const SpeciesHost& h : pl.sp) r.has_tree |= h.tree ? 1 : 0;
   r.nrad = pl.gen ? (int)pl.rad.size() : 0;
   for (int i = 0; i < r.nrad; i++) r.rad[i] = pl.rad[i];
   r.slot = pl.gen ? (const int*)at(pl.o_slot_tab) : nullptr;
