@@ -1,0 +1,70 @@
+"""Descriptor validation of sdft_request_create, which runs on the host before
+any CUDA call: supported grids and topologies pass it (and, without a GPU, stop
+at "no CUDA device"), unsupported ones are refused with the reason."""
+import ctypes as C
+import copy
+
+import pytest
+
+from softdft_b200 import native, workloads
+from softdft_b200.api import setup_request
+
+from tests.helpers import small_slit
+
+pytestmark = pytest.mark.skipif(not native.library_present(), reason="libsoftdft.so not built")
+
+
+def _create(ds):
+    dft = setup_request(copy.deepcopy(ds))
+    h = C.c_void_p()
+    rc = native.lib().sdft_request_create(C.byref(dft.descriptor.desc), 0, C.byref(h))
+    msg = native.lib().sdft_last_error().decode()
+    if rc == native.SDFT_OK:  # a GPU is present: the request exists
+        native.lib().sdft_request_destroy(h)
+    return rc, msg
+
+
+def _accepted(ds):
+    rc, msg = _create(ds)
+    assert rc == native.SDFT_OK or (rc == 4 and "no CUDA device" in msg), (rc, msg)
+
+
+def _refused(ds, text):
+    rc, msg = _create(ds)
+    assert rc == native.SDFT_ERR_UNSUPPORTED and text in msg, (rc, msg)
+
+
+def _branched(seq, **kw):
+    ds = small_slit(**kw)
+    ds["species"][0]["sequence"] = seq
+    return ds
+
+
+@pytest.mark.parametrize("np_", [128, 1000, 1001, 250, 286, 3969])
+def test_supported_grids_pass_validation(np_):
+    _accepted(small_slit(np_=np_, dz=0.02))
+
+
+@pytest.mark.parametrize("np_,why", [(1009, "NP has a prime factor above 61"),
+                                     (2018, "NP/2 has a prime factor above 61"),
+                                     (32768, "more shared memory than a CTA has")])
+def test_unsupported_grids_are_refused(np_, why):
+    _refused(small_slit(np_=np_, dz=0.02), why)
+
+
+@pytest.mark.parametrize("seq", ["AA(AA)AA", "AAA(A)AAA(AA)A", "A(AB)A"])
+def test_branched_chains_pass_validation(seq):
+    _accepted(_branched(seq))
+
+
+def test_branched_brush_passes_validation():
+    ds = workloads.grafted_brush(256, 0.05, 6, 0.05, 4.5, 7.0, 0.01)
+    ds["species"][0]["sequence"] = ds["species"][1]["sequence"] = "AA(AA)AA"
+    _accepted(ds)
+
+
+@pytest.mark.parametrize("seq", ["A(AA)(AA)A", "A(AB)2A"])
+def test_branch_point_beyond_the_reference_arrays_is_refused(seq):
+    """Three children of one segment with two states: the reference's
+    other-children index (parent_propagators.jl:150) leaves its array."""
+    _refused(_branched(seq), "index out of range")
