@@ -490,59 +490,66 @@ struct Topology {  // structures/TopologyStruct.jl:23-30, 0-based
 };
 
 // parse_topology.jl:16-127: letters, (group) and (group)k repeats; a letter's
-// parent is the letter before it at the enclosing level
+// parent is the letter before it at the enclosing level.  A run of letters is
+// walked iteratively (each letter one level deeper, child of the previous one);
+// only parenthesised groups recurse, so long chains need no deep stack.
 Topology parse_topology(const std::string& sequence) {
   std::vector<char> mons;
   std::vector<std::vector<int>> children, parents, levels;
   int current = 0;
-  std::function<void(const std::string&, int, int)> rec = [&](const std::string& sub, int level, int parent) {
-    const char ch = sub[0];
-    if (std::isalpha((unsigned char)ch)) {
-      const int cur = ++current;
-      mons.push_back(ch);
-      if (level > (int)levels.size()) levels.emplace_back();
-      levels[level - 1].push_back(cur);
-      if (parent == 0) {
-        children.emplace_back();
-        parents.emplace_back();
-      } else {
-        if (parent > (int)children.size()) children.push_back({cur});
-        else children[parent - 1].push_back(cur);
-        if (cur > (int)parents.size()) parents.push_back({parent});
-        else parents[cur - 1].push_back(parent);
-      }
-      if (sub.size() > 1) rec(sub.substr(1), level + 1, cur);
-      else children.emplace_back();
-    } else if (ch == '(') {
-      int bal = 1;
-      size_t end = std::string::npos;
-      for (size_t j = 1; j < sub.size(); j++) {
-        if (sub[j] == '(') bal++;
-        else if (sub[j] == ')') bal--;
-        if (bal == 0) {
-          end = j;
-          break;
+  std::function<void(size_t, size_t, int, int, int)> rec = [&](size_t b, size_t e, int level, int parent, int depth) {
+    if (depth > 256) fail("parenthesised groups nested too deeply");
+    size_t i = b;
+    while (i < e) {
+      const char ch = sequence[i];
+      if (std::isalpha((unsigned char)ch)) {
+        const int cur = ++current;
+        mons.push_back(ch);
+        if (level > (int)levels.size()) levels.emplace_back();
+        levels[level - 1].push_back(cur);
+        if (parent == 0) {
+          children.emplace_back();
+          parents.emplace_back();
+        } else {
+          if (parent > (int)children.size()) children.push_back({cur});
+          else children[parent - 1].push_back(cur);
+          if (cur > (int)parents.size()) parents.push_back({parent});
+          else parents[cur - 1].push_back(parent);
         }
+        if (i + 1 >= e) children.emplace_back();  // the reference's trailing entry after a run's last letter
+        parent = cur;
+        level++;
+        i++;
+      } else if (ch == '(') {
+        int bal = 1;
+        size_t end = std::string::npos;
+        for (size_t j2 = i + 1; j2 < e; j2++) {
+          if (sequence[j2] == '(') bal++;
+          else if (sequence[j2] == ')') bal--;
+          if (bal == 0) {
+            end = j2;
+            break;
+          }
+        }
+        if (end == std::string::npos) fail("Unmatched parenthesis in: " + sequence.substr(i, e - i));
+        if (end == i + 1) fail("empty group in: " + sequence.substr(i, e - i));
+        size_t k = end + 1;
+        int mult = 1;
+        if (k < e && std::isdigit((unsigned char)sequence[k])) {
+          const size_t d0 = k;
+          while (k < e && std::isdigit((unsigned char)sequence[k])) k++;
+          if (k - d0 > 6) fail("group repeat count too large");
+          mult = std::stoi(sequence.substr(d0, k - d0));
+        }
+        for (int r = 0; r < mult; r++) rec(i + 1, end, level, parent, depth + 1);
+        i = k;  // the rest continues at this level from the same parent
+      } else {
+        fail(std::string("Not a recognized character: ") + ch);
       }
-      if (end == std::string::npos) fail("Unmatched parenthesis in: " + sub);
-      const std::string group = sub.substr(1, end - 1);
-      std::string remaining = sub.substr(end + 1);
-      int mult = 1;
-      if (!remaining.empty() && std::isdigit((unsigned char)remaining[0])) {
-        size_t k = 0;
-        while (k < remaining.size() && std::isdigit((unsigned char)remaining[k])) k++;
-        mult = std::stoi(remaining.substr(0, k));
-        remaining = remaining.substr(k);
-      }
-      if (group.empty()) fail("empty group in: " + sub);
-      for (int r = 0; r < mult; r++) rec(group, level, parent);
-      if (!remaining.empty()) rec(remaining, level, parent);
-    } else {
-      fail(std::string("Not a recognized character: ") + ch);
     }
   };
   if (sequence.empty()) fail("empty sequence");
-  rec(sequence, 1, 0);
+  rec(0, sequence.size(), 1, 0, 0);
   Topology t;
   const int n = (int)mons.size();
   t.monomers.assign(mons.begin(), mons.end());
