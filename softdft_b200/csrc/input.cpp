@@ -1045,12 +1045,9 @@ MolSys molecular_system(const Node& ds) {
       for (int b : m.configs[u].sequence) q += m.valences[b];
       m.charge[u] = q;
     }
-  for (Config& cfg : m.configs)  // process_bonding.jl:12-16
-    if (cfg.model == "freely_jointed") {
-      if (m.diameters.empty())
-        fail("Missing 'diameters' in properties.monomers. This is required for freely_jointed species_model.");
-      cfg.max_distance = max_distance_matrix(cfg, m.diameters);
-    }
+  for (Config& cfg : m.configs)  // process_bonding.jl:12-16 (the matrices are built where used: grafted species)
+    if (cfg.model == "freely_jointed" && m.diameters.empty())
+      fail("Missing 'diameters' in properties.monomers. This is required for freely_jointed species_model.");
   if (m.diameters.empty()) m.diameters.assign(nb, 0.0);
   return m;
 }
@@ -1797,7 +1794,10 @@ void build(const std::string& text, sdft_input& in) {
     s.states = in.keep(st);
     s.fixed_coord = in.keep(coords);
     s.fixed_density = dens;
-    s.max_distance = any_fixed ? in.keep(cfg.max_distance) : nullptr;
+    if (any_fixed && n > 20000)
+      fail("grafted chains of more than 20000 segments are not supported (path-length matrix of n^2 entries)",
+           SDFT_ERR_UNSUPPORTED);
+    s.max_distance = any_fixed ? in.keep(max_distance_matrix(cfg, m.diameters)) : nullptr;
     s.mu_species = b.mu_species[u];
   }
   std::vector<int32_t> bonds;
