@@ -149,3 +149,16 @@ def test_errors_carry_the_reference_messages():
     with pytest.raises(native.SdftError) as e:
         native.Input("geometry: [1, 2\n")
     assert e.value.code == 2
+
+
+@pytest.mark.parametrize("text,why", [
+    ("a: 1\na: 2\nspecies: []\n", "duplicate key"),
+    ("geometry:\n\tcoordinate_system: Cartesian\n", "tabs in indentation"),
+    ("base: &b {x: 1}\nother: *b\n", "anchors"),
+    ("note: |\n  text\n", "block scalars"),
+    ("geometry: {coordinate_system: Cartesian\n", "flow"),
+])
+def test_yaml_subset_refuses_what_it_does_not_read(text, why):
+    with pytest.raises(native.SdftError) as e:
+        native.Input(text)
+    assert e.value.code == 2 and why in str(e.value)
