@@ -1607,6 +1607,7 @@ namespace {
 // Julia's cld on Float64: the ceiling of the exact quotient x / y (y > 0)
 long cld_exact(double x, double y) {
   if (!(y > 0) || !std::isfinite(x) || !std::isfinite(y)) fail("bin_width must be positive and finite");
+  if (!(x >= 0) || x / y > 1e8) fail("the slit needs 0 <= dimensions / bin_width <= 1e8");
   long k = (long)std::ceil(x / y);
   while (std::fma((double)k, y, -x) < 0) k++;        // k y < x
   while (std::fma((double)(k - 1), y, -x) >= 0) k--;  // (k - 1) y >= x

@@ -162,3 +162,12 @@ def test_yaml_subset_refuses_what_it_does_not_read(text, why):
     with pytest.raises(native.SdftError) as e:
         native.Input(text)
     assert e.value.code == 2 and why in str(e.value)
+
+
+@pytest.mark.parametrize("dims,bw", [("[10.0]", "[0.0]"), ("[1.0e12]", "[1.0e-3]"), ("[-1.0]", "[0.05]")])
+def test_slit_sizes_out_of_range_are_refused(dims, bw):
+    text = YAML.replace("dimensions: [10.0]", "dimensions: " + dims).replace("bin_width: [0.05]", "bin_width: " + bw)
+    assert text != YAML
+    with pytest.raises(native.SdftError) as e:
+        native.Input(text)
+    assert e.value.code == 2
