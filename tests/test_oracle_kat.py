@@ -33,6 +33,22 @@ def test_bulk_fixed_point_fmt():
     assert abs(psic[0]) < 1e-8
 
 
+@pytest.mark.parametrize("np_", [125, 1001])
+def test_bulk_fixed_point_on_odd_grids(np_):
+    """Odd NP gives a mirrored grid of 2 NP = 2 mod 4 points (250, 2002), which
+    the oracle transforms with Bluestein's algorithm."""
+    ds = small_slit(models=["ideal", "TPT1mfmt", "TPT1msa"], walls=False, np_=np_, dz=0.05)
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    x0 = o.get_x()
+    g = o.objective()
+    mu0, lng0, _, _ = dft.split(x0)
+    mu, lng, psi, _ = dft.split(g)
+    assert rel(mu, mu0) < 1e-8
+    assert rel(lng, lng0) < 1e-8
+    assert np.max(np.abs(psi)) < 1e-9
+
+
 def test_bulk_fixed_point_fmt_msa():
     ds = small_slit(models=["ideal", "TPT1mfmt", "TPT1msa"], walls=False)
     dft = descriptor(ds)
