@@ -32,7 +32,7 @@
 
 #include "common.cuh"
 
-// SDFT_FFT_GEN selects the transform passes this build carries: 0 for
+// SDFT_FFT_GEN selects the transform passes a translation unit carries: 0 for
 // power-of-two M, 1 for a general M (see kernels.cuh)
 #ifndef SDFT_FFT_GEN
 #error "define SDFT_FFT_GEN (0: power-of-two FFT lengths, 1: general lengths) before including fft.cuh"
@@ -99,7 +99,7 @@ __device__ __forceinline__ FftCtxT<float2> make_fft32(double2* z, const DReq& r)
 
 // The loops below come in two instantiations: G = false for power-of-two M
 // (bit reversal, shifts), G = true for a general M (digit-reversal table,
-// divisions); the entry points instantiate the one of this build.
+// divisions); the entry points instantiate the one SDFT_FFT_GEN selects.
 
 // buffer slot of natural complex index m
 template <bool G, class C>

@@ -65,6 +65,16 @@ struct Node {
     return nullptr;
   }
   bool has(const std::string& k) const { return get(k) != nullptr; }
+  // a repeated key keeps its first position and takes the last value, as
+  // YAML.jl's and PyYAML's mapping constructors do
+  void put(const std::string& k, Node v) {
+    for (auto& kv : map)
+      if (kv.first == k) {
+        kv.second = std::move(v);
+        return;
+      }
+    map.emplace_back(k, std::move(v));
+  }
 };
 
 bool match_digits(const std::string& s, size_t& i, bool underscores) {
@@ -120,9 +130,12 @@ double parse_number(std::string s) {
   if (s == ".inf" || s == ".Inf" || s == ".INF" || s == "+.inf" || s == "+.Inf" || s == "+.INF") return INFINITY;
   if (s == "-.inf" || s == "-.Inf" || s == "-.INF") return -INFINITY;
   if (s == ".nan" || s == ".NaN" || s == ".NAN") return NAN;
-  size_t pos = 0;
-  const double v = std::stod(s, &pos);
-  if (pos != s.size()) fail("not a number: " + s);
+  // strtod keeps an underflow (subnormal or zero) and an overflow (infinity),
+  // as parse(Float64, s) does
+  const char* b = s.c_str();
+  char* e = nullptr;
+  const double v = std::strtod(b, &e);
+  if (s.empty() || std::isspace((unsigned char)s[0]) || e != b + s.size()) fail("not a number: " + s);
   return v;
 }
 
@@ -142,7 +155,7 @@ double as_float(const Node& n) {
 bool is_float_node(const Node& n) { return n.kind == Node::Scalar && !n.quoted && is_float_text(n.text); }
 int as_int(const Node& n) {
   const double v = as_float(n);
-  if (v != std::floor(v)) fail("not an integer: " + n.text);
+  if (!(v == std::floor(v)) || v < INT32_MIN || v > INT32_MAX) fail("not an integer: " + n.text);
   return (int)v;
 }
 // Python truthiness of the loaded value (bool(entry.get(key, False)))
@@ -153,6 +166,13 @@ bool truthy(const Node* n) {
   if (!n->quoted && is_bool_text(n->text, &b)) return b;
   if (!n->quoted && (is_int_text(n->text) || is_float_text(n->text))) return parse_number(n->text) != 0.0;
   return !n->text.empty();
+}
+// the entries a `for x in v` loop visits in Julia: a sequence's items, or a
+// scalar itself
+std::vector<Node> listed(const Node& n) {
+  if (n.kind == Node::Seq) return n.seq;
+  if (n.kind == Node::Scalar) return {n};
+  fail("expected a list");
 }
 std::string as_str(const Node& n) {
   if (n.kind != Node::Scalar) fail("expected a scalar");
@@ -218,6 +238,9 @@ Node make_scalar(const std::string& raw) {
     }
     n.text = body;
   } else {
+    // YAML reserves these indicators at the start of a plain scalar (tags,
+    // anchors, aliases, block scalars, directives, @ and `)
+    if (std::strchr("!&*|>%@`", t[0])) fail("a plain scalar cannot start with '" + t.substr(0, 1) + "'");
     n.text = t;
   }
   return n;
@@ -265,7 +288,7 @@ struct Flow {
         if (i >= s.size() || s[i] != ':') fail("line " + std::to_string(line) + ": expected : in a flow mapping");
         i++;
         Node v = value_or_null();
-        n.map.emplace_back(key, std::move(v));
+        n.put(key, std::move(v));
         ws();
         if (i < s.size() && s[i] == ',') {
           i++;
@@ -323,25 +346,34 @@ Node parse_inline(const std::string& text, int line) {
   }
   if (!t.empty() && (t[0] == '|' || t[0] == '>' || t[0] == '&' || t[0] == '*' || t[0] == '!'))
     fail("line " + std::to_string(line) + ": block scalars, anchors, aliases and tags are not supported");
+  if (t == "-" || t.rfind("- ", 0) == 0) fail("line " + std::to_string(line) + ": a sequence entry after a key on its line");
   return make_scalar(t);
 }
 
 // position of the ': ' (or final ':') that separates a block mapping key from its value
 size_t key_colon(const std::string& t) {
-  char q = 0;
-  int depth = 0;
-  for (size_t i = 0; i < t.size(); i++) {
-    const char c = t[i];
-    if (q) {
-      if (c == q) q = 0;
-      continue;
+  // a block key is a quoted scalar or a plain scalar; inside a plain key,
+  // brackets and quotes are ordinary characters.  A line that opens a flow
+  // collection is a value (flow collections as keys are not read).
+  if (!t.empty() && (t[0] == '[' || t[0] == '{')) return std::string::npos;
+  size_t i = 0;
+  if (!t.empty() && (t[0] == '\'' || t[0] == '"')) {
+    const char q = t[0];
+    for (i = 1; i < t.size(); i++) {
+      if (q == '"' && t[i] == '\\') {
+        i++;
+      } else if (t[i] == q) {
+        if (q == '\'' && i + 1 < t.size() && t[i + 1] == '\'') {
+          i++;  // '' inside a single-quoted scalar
+        } else {
+          break;
+        }
+      }
     }
-    if (c == '\'' || c == '"') q = c;
-    else if (c == '[' || c == '{') depth++;
-    else if (c == ']' || c == '}') depth--;
-    else if (c == ':' && depth == 0 && (i + 1 == t.size() || t[i + 1] == ' ' || t[i + 1] == '\t'))
-      return i;
+    if (i >= t.size()) return std::string::npos;
   }
+  for (; i < t.size(); i++)
+    if (t[i] == ':' && (i + 1 == t.size() || t[i + 1] == ' ' || t[i + 1] == '\t')) return i;
   return std::string::npos;
 }
 
@@ -399,17 +431,25 @@ struct Block {
       } else if (i < L.size() && L[i].indent == indent && (L[i].text == "-" || L[i].text.rfind("- ", 0) == 0)) {
         v = seq(indent);  // a sequence may sit at its key's indentation
       }
-      for (const auto& kv : n.map)
-        if (kv.first == key) fail("line " + std::to_string(ln) + ": duplicate key " + key);
-      n.map.emplace_back(key, std::move(v));
+      n.put(key, std::move(v));
     }
     if (i < L.size() && L[i].indent > indent) fail("line " + std::to_string(L[i].number) + ": unexpected indentation");
     return n;
   }
 };
 
-// bracket depth of a line outside quotes (flow collections may span lines)
-int flow_depth(const std::string& t) {
+// bracket depth a line leaves open (flow collections may span lines), counted
+// from a flow collection that opens the line's value; brackets inside a plain
+// scalar are text
+int flow_depth(std::string t) {
+  while (t == "-" || t.rfind("- ", 0) == 0) t = trim(t.substr(1));
+  if (t.empty()) return 0;
+  if (t[0] != '[' && t[0] != '{') {
+    const size_t c = key_colon(t);
+    if (c == std::string::npos) return 0;
+    t = trim(t.substr(c + 1));
+    if (t.empty() || (t[0] != '[' && t[0] != '{')) return 0;
+  }
   int d = 0;
   char q = 0;
   for (char c : t) {
@@ -446,7 +486,7 @@ Node load_yaml(const std::string& text) {
     line = strip_comment(line);
     std::string t = trim(line);
     if (t.empty() || t == "---" || t == "...") continue;
-    if (t.rfind("%", 0) == 0) continue;  // directives
+    if (line.rfind("%", 0) == 0) continue;  // directives (column 0 only)
     int ind = 0;
     while (ind < (int)line.size() && line[ind] == ' ') ind++;
     while (flow_depth(t) > 0 && k + 1 < raw.size()) {  // a flow collection continued on the next lines
@@ -818,9 +858,8 @@ std::vector<double> assign_delta_muH(const std::vector<double>* valences, const 
                                      const std::map<std::string, std::vector<std::string>>& families,
                                      std::vector<Reaction>& rx, const std::vector<std::string>& names,
                                      const std::vector<double>& densities, std::vector<double>& pS, const Constants& c) {
-  std::map<std::string, int> name_to_index;
-  for (size_t i = 0; i < names.size(); i++)
-    if (!name_to_index.count(names[i])) name_to_index[names[i]] = (int)i;
+  std::map<std::string, int> name_to_index;  // a repeated name maps to its last entry, as a Julia Dict does
+  for (size_t i = 0; i < names.size(); i++) name_to_index[names[i]] = (int)i;
   auto idx_of = [&](const std::string& s) {
     auto it = name_to_index.find(s);
     if (it == name_to_index.end()) fail("species " + s + " is not defined in the species list");
@@ -1026,7 +1065,7 @@ MolSys molecular_system(const Node& ds) {
   for (const auto& name : m.monomers) {
     const Node* md = mdata ? mdata->get(name) : nullptr;
     if (!md) fail("Species " + name + " listed in used_monomers not found in dataset[\"monomers\"]");
-    if (md->kind != Node::Map) continue;
+    if (md->kind != Node::Map) fail("the properties of monomer " + name + " must be a mapping");
     for (const auto& kv : md->map) {
       if (kv.second.kind == Node::Map) continue;
       auto& v = props[kv.first + "s"];
@@ -1314,6 +1353,9 @@ struct Residual {
     std::vector<double> qr(m.species.size());
     for (size_t i = 0; i < qr.size(); i++) qr[i] = m.charge[i] * b.rho_species[i];
     res.push_back(-np_sum(qr.data(), qr.size()));
+    // the driver subtracts the residual from the unknowns (AndersonResidual.jl:27-138)
+    if (res.size() != n)
+      fail("bulk state: " + std::to_string(res.size()) + " equations for " + std::to_string(n) + " unknowns");
     return res;
   }
 };
@@ -1476,13 +1518,23 @@ double numv(const std::map<std::string, double>& n, const char* k, double d) {
   return it == n.end() ? d : it->second;
 }
 
+// Int(x) of AndersonMixing.jl:74-79: a finite integral value, or an error.
+// max_iters beyond the int32 range of sdft_numerics is clamped (a count that
+// large is never reached); anderm must fit.
+int32_t numerics_int(const std::map<std::string, double>& n, const char* key, int32_t def, bool clamp) {
+  const double v = numv(n, key, def);
+  if (!std::isfinite(v) || v != std::floor(v) || (!clamp && (v < INT32_MIN || v > INT32_MAX)))
+    fail(std::string("numerical.") + key + " must be an integer");
+  return (int32_t)std::max<double>(INT32_MIN, std::min<double>(INT32_MAX, v));
+}
+
 // AndersonResidual.jl:27-138 (restated driver)
 Bulk solve_bulk_reference(MolSys& m, BulkSys& bs, const std::map<std::string, double>& num, int cap) {
   Bulk b = initialize_densities(m);
-  const long max_iters = (long)numv(num, "max_iters", 100000);
+  const long max_iters = numerics_int(num, "max_iters", 100000, true);
   const double damping = numv(num, "damping", 0.1), mix_max = numv(num, "mixing_max", 0.1);
   const double switch_mix = numv(num, "switch_mix", 1e-4), tole = numv(num, "tole", 1e-6);
-  const int mm = (int)numv(num, "anderm", 5);
+  const int mm = numerics_int(num, "anderm", 5, false);
   std::vector<char> adjustable(m.adjustable);
   Residual R(m, bs);
   std::vector<double> Xk = R.initial(b);
@@ -1585,6 +1637,9 @@ Bulk solve_bulk(MolSys& m, const Node* numerical) {
   build_bulk_sys(m, bs);
   const auto num = bulk_numerics(numerical);
   const std::vector<double> charge0 = m.charge;
+  // zeros(n, anderm) of the history (AndersonResidual.jl) needs anderm >= 1
+  if (numerics_int(num, "anderm", 5, false) < 1) fail("numerical.anderm must be at least 1");
+  numerics_int(num, "max_iters", 100000, true);
   try {
     return solve_bulk_reference(m, bs, num, 3000);
   } catch (const BulkDiverged&) {
@@ -1645,23 +1700,24 @@ Slit geometry_system(const Node& ds) {
       const Node& d = kv.second;
       if (kv.first == "hard_walls") {
         const Node* dd = d.get("dims");
-        if (!dd) fail("Missing 'dims' key in external_field[:hard_walls].");
-        for (const Node& x : dd->seq) {
+        if (!dd || dd->kind == Node::Null) fail("Missing 'dims' key in external_field[:hard_walls].");
+        for (const Node& x : listed(*dd)) {
           if (as_int(x) != 1) fail("Invalid dimension index: " + as_str(x));
           s.hard = true;
         }
       } else if (kv.first == "charged_walls") {
-        const Node* dd = d.get("dims");
-        if (!dd) fail("Please specify the dimensions using 'dims: [i, j, ...]'.");
+        const Node* dp = d.get("dims");
+        if (!dp || dp->kind == Node::Null) fail("Please specify the dimensions using 'dims: [i, j, ...]'.");
+        const std::vector<Node> dd = listed(*dp);
         const Node* ch = d.get("charge");
         if (!ch) fail("Please specify wall charges under 'charge'.");
         std::vector<const Node*> rows;
         if (!ch->seq.empty() && ch->seq[0].kind != Node::Seq) rows.push_back(ch);
         else
           for (const Node& r : ch->seq) rows.push_back(&r);
-        if (rows.size() != dd->seq.size()) fail("Mismatch: number of charge entries does not match dims.");
-        for (size_t i = 0; i < dd->seq.size(); i++) {
-          if (as_int(dd->seq[i]) != 1) fail("Invalid dimension index in dims");
+        if (rows.size() != dd.size()) fail("Mismatch: number of charge entries does not match dims.");
+        for (size_t i = 0; i < dd.size(); i++) {
+          if (as_int(dd[i]) != 1) fail("Invalid dimension index in dims");
           if (rows[i]->seq.size() < 2) fail("wall charges need two values");
           s.charged = true;
           s.q[0] = as_float(rows[i]->seq[0]);
@@ -1743,8 +1799,8 @@ sdft_numerics numerics_of(const Node& ds) {
     if (num->kind == Node::Map)
       for (const auto& kv : num->map) n[kv.first] = as_float(kv.second);
   sdft_numerics o;
-  o.max_iters = (int32_t)numv(n, "max_iters", 100000);
-  o.anderm = (int32_t)numv(n, "anderm", 5);
+  o.max_iters = numerics_int(n, "max_iters", 100000, true);
+  o.anderm = numerics_int(n, "anderm", 5, false);
   o.damping = numv(n, "damping", 0.5);
   o.mixing_max = numv(n, "mixing_max", 1.0);
   o.switch_tole = numv(n, "switch_tole", 1e-3);

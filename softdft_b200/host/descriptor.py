@@ -20,6 +20,7 @@ import numpy as np
 from .geometry import CartesianGrid, julia_round
 from .ilst import BulkState
 from .molsys import MolecularSystem
+from .yamlio import numerics_int
 
 ABI_VERSION = 2
 FUNC_BITS = {"mfmt": 0x1, "TPT1mfmt": 0x2, "msa": 0x4, "TPT1msa": 0x8}
@@ -80,8 +81,8 @@ class Numerics(C.Structure):
 def numerics_from_dict(num: dict) -> Numerics:
     """Defaults of `src/NonlinearSolvers/fixed_point/AndersonMixing.jl:74-79`."""
     return Numerics(
-        max_iters=int(num.get("max_iters", 100000)),
-        anderm=int(num.get("anderm", 5)),
+        max_iters=numerics_int(num, "max_iters", 100000, True),
+        anderm=numerics_int(num, "anderm", 5, False),
         damping=float(num.get("damping", 0.5)),
         mixing_max=float(num.get("mixing_max", 1.0)),
         switch_tole=float(num.get("switch_tole", 1e-3)),

@@ -45,6 +45,16 @@ class CartesianGrid:
         return (self.NP + 2 * self.offset) * (2 if self.mirrored else 1)
 
 
+def _listed(v) -> list:
+    """The entries a Julia `for x in v` loop visits: a list's items, or a
+    scalar itself."""
+    if isinstance(v, (list, tuple)):
+        return list(v)
+    if isinstance(v, dict):
+        raise ValueError("expected a list")
+    return [v]
+
+
 def geometry_system(dataset: dict) -> CartesianGrid:
     geom = dataset.get("geometry")
     if geom is None:
@@ -71,7 +81,7 @@ def geometry_system(dataset: dict) -> CartesianGrid:
             d = desc.get("dims") if isinstance(desc, dict) else None
             if d is None:
                 raise ValueError("Missing 'dims' key in external_field[:hard_walls].")
-            for dim in d:
+            for dim in _listed(d):
                 if int(dim) != 1:
                     raise ValueError(f"Invalid dimension index: {dim}")
                 g.hard_walls = [0.0, H]
@@ -82,6 +92,7 @@ def geometry_system(dataset: dict) -> CartesianGrid:
             ch = desc.get("charge")
             if ch is None:
                 raise ValueError("Please specify wall charges under 'charge'.")
+            d = _listed(d)
             if len(ch) > 0 and not isinstance(ch[0], (list, tuple)):
                 ch = [ch]
             if len(ch) != len(d):

@@ -25,6 +25,7 @@ import numpy as np
 
 from .lsqr import lsqr_inplace
 from .molsys import LOG10, MolecularSystem, concentration_to_density
+from .yamlio import numerics_int
 
 PI = math.pi
 SUPPORTED_MODELS = ("ideal", "mfmt", "TPT1mfmt", "msa", "TPT1msa", "coul")
@@ -736,6 +737,11 @@ def solve_bulk(ms: MolecularSystem, numerical: dict, cap: int = 3000) -> BulkSta
         if m not in SUPPORTED_MODELS:
             raise NotImplementedError(f"Unknown or unsupported model(s): {m}")
     charge0 = list(ms.species_charge)
+    num = _bulk_numerics(numerical)
+    # zeros(n, anderm) of the history (AndersonResidual.jl) needs anderm >= 1
+    if numerics_int(num, "anderm", 5, False) < 1:
+        raise ValueError("numerical.anderm must be at least 1")
+    numerics_int(num, "max_iters", 100000, True)
     try:
         return _solve_bulk_reference(ms, numerical, cap)
     except (BulkDiverged, ValueError, OverflowError, FloatingPointError, ZeroDivisionError):
@@ -811,12 +817,12 @@ def _solve_bulk_robust(ms: MolecularSystem, numerical: dict) -> BulkState:
 def _solve_bulk_reference(ms: MolecularSystem, numerical: dict, cap: int) -> BulkState:
     bulk = initialize_densities(ms)
     num = _bulk_numerics(numerical)
-    max_iters = int(num.get("max_iters", 100000))
+    max_iters = numerics_int(num, "max_iters", 100000, True)
     damping = num.get("damping", 0.1)
     mix_max = num.get("mixing_max", 0.1)
     switch_mix = num.get("switch_mix", 1e-4)
     tole = num.get("tole", 1e-6)
-    m = int(num.get("anderm", 5))
+    m = numerics_int(num, "anderm", 5, False)
     adjustable = list(ms.adjustable)
     Xk, unflat = _initial_solution(ms, bulk)
     n = Xk.size

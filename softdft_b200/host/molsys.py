@@ -488,7 +488,9 @@ def process_monomers(used: Dict[str, int], dataset: dict) -> Dict[str, List[floa
     for name, idx in sorted(used.items(), key=lambda kv: kv[1]):
         if name not in data:
             raise ValueError(f"Species {name} listed in used_monomers not found in dataset[\"monomers\"]")
-        for key, value in (data[name] or {}).items():
+        if not isinstance(data[name], dict):
+            raise ValueError(f"the properties of monomer {name} must be a mapping")
+        for key, value in data[name].items():
             if isinstance(value, dict):
                 continue  # nested properties are unused on the solve path
             pk = str(key) + "s"

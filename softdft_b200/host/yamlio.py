@@ -7,6 +7,7 @@ YAML 1.2 float form is added here.
 """
 from __future__ import annotations
 
+import math
 import re
 
 import yaml
@@ -48,3 +49,14 @@ def as_float(v) -> float:
     if isinstance(v, (int, float)):
         return float(v)
     return float(str(v))
+
+
+def numerics_int(num: dict, key: str, default: int, clamp: bool) -> int:
+    """Int(x) of `src/NonlinearSolvers/fixed_point/AndersonMixing.jl:74-79`: a
+    finite integral value, or an error.  max_iters beyond the int32 field is
+    clamped (a count that large is never reached); anderm must fit."""
+    v = float(num.get(key, default))
+    lo, hi = -2 ** 31, 2 ** 31 - 1
+    if not math.isfinite(v) or v != math.floor(v) or (not clamp and not lo <= v <= hi):
+        raise ValueError(f"numerical.{key} must be an integer")
+    return int(min(max(v, lo), hi))

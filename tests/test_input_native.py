@@ -83,6 +83,9 @@ CASES = {
     "brush_50": _dump(workloads.grafted_brush(2048, 0.02, 50, 0.05, 4.5, 7.0, 0.1)),
     "odd_grid_charged": _dump(workloads.weak_acid_slit(1001, 0.02, 20, 4.5, 6.0, 0.05, 0.25, wall_charge=-0.05)),
     "dense_300": _dump(workloads.weak_acid_slit(4096, 0.02, 300, 4.5, 3.0, 0.001, 0.4)),
+    # a repeated species name: name lookups take its last entry, as the
+    # reference's Dict does (assign_delta_muH.jl:67)
+    "repeated_species": YAML.replace('  - sequence: "Y"\n    pSpecies: 6.0', '  - sequence: "Y"\n  - sequence: "Y"\n    pSpecies: 6.0'),
     "branched": _dump(_branched("AA(AA)AA")),
     "branched_repeat": _dump(_branched("A(AB)2A")),
 }
@@ -134,6 +137,29 @@ model: [ideal, TPT1mfmt, TPT1msa]
     _compare(text)
 
 
+def test_repeated_keys_take_the_last_value():
+    """YAML.jl and PyYAML keep the last value of a repeated key; so does the
+    library's reader, in block and flow mappings alike."""
+    text = YAML.replace("  tole: 1e-6\n", "  tole: 1e-6\n  tole: 1e-7\n")
+    text = text.replace("A: {diameter: 1.0, valence: 0.0}", "A: {diameter: 0.9, valence: 0.0, diameter: 1.0}")
+    text += "numerical: {damping: 0.01, tole: 1e-5, mixing_max: 0.001, tole: 1e-6, anderm: 4}\n"
+    assert yamlio.load_text(text)["numerical"] == {"damping": 0.01, "tole": 1e-6, "mixing_max": 0.001, "anderm": 4}
+    _compare(text)
+    num = native.Input(text).numerics()
+    assert (num.tole, num.anderm) == (1e-6, 4)
+
+
+def test_plain_keys_may_hold_brackets_and_quotes():
+    """In block context a plain scalar key may contain ], } and quotes; such a
+    key is read as text (here an unknown monomer property, which both hosts
+    ignore)."""
+    text = YAML.replace("  a: {diameter: 1.0, valence: -1.0}",
+                        "  a:\n    diameter: 1.0\n    valence: -1.0\n    note]s: 1\n    it's: 2\n    'x: y': 3")
+    d = yamlio.load_text(text)["monomers"]["a"]
+    assert d == {"diameter": 1.0, "valence": -1.0, "note]s": 1, "it's": 2, "x: y": 3}
+    _compare(text)
+
+
 def test_errors_carry_the_reference_messages():
     bad = YAML.split("species:")[0] + "model: [ideal]\n"
     with pytest.raises(native.SdftError) as e:
@@ -152,11 +178,13 @@ def test_errors_carry_the_reference_messages():
 
 
 @pytest.mark.parametrize("text,why", [
-    ("a: 1\na: 2\nspecies: []\n", "duplicate key"),
     ("geometry:\n\tcoordinate_system: Cartesian\n", "tabs in indentation"),
     ("base: &b {x: 1}\nother: *b\n", "anchors"),
     ("note: |\n  text\n", "block scalars"),
     ("geometry: {coordinate_system: Cartesian\n", "flow"),
+    ("geometry:\n  !external_field: 1\n", "cannot start with '!'"),
+    ("monomers: {A: {%diameter: 1.0}}\n", "cannot start with '%'"),
+    ("procedure: - iDFT\n", "sequence entry after a key"),
 ])
 def test_yaml_subset_refuses_what_it_does_not_read(text, why):
     with pytest.raises(native.SdftError) as e:
@@ -171,3 +199,37 @@ def test_slit_sizes_out_of_range_are_refused(dims, bw):
     with pytest.raises(native.SdftError) as e:
         native.Input(text)
     assert e.value.code == 2
+
+
+def _refused_by_both(text, why):
+    with pytest.raises(Exception):
+        setup_request(yamlio.load_text(text))
+    with pytest.raises(native.SdftError) as e:
+        native.Input(text)
+    assert why in str(e.value), str(e.value)
+
+
+@pytest.mark.parametrize("old,new,why", [
+    ("    hard_walls:\n      dims: [1]", "    hard_walls:\n      dims:", "Missing 'dims' key"),
+    ("  A: {diameter: 1.0, valence: 0.0}", "  A: 1.0", "must be a mapping"),
+    ("  tole: 1e-6", "  tole: 1e-6\n  anderm: 2.5", "anderm must be an integer"),
+    ("  tole: 1e-6", "  tole: 1e-6\n  anderm: 0", "anderm must be at least 1"),
+    ("  tole: 1e-6", "  tole: 1e-6\n  max_iters: .nan", "max_iters must be an integer"),
+])
+def test_malformed_sections_are_refused_by_both_hosts(old, new, why):
+    """Inputs on which the reference raises (a wall list that is null, a
+    monomer whose properties are a number, a non-integral or empty Anderson
+    depth: Int(x) and zeros(n, anderm) of AndersonMixing.jl) are refused by
+    both hosts, not read as something else."""
+    assert old in YAML
+    _refused_by_both(YAML.replace(old, new), why)
+
+
+def test_scalar_dims_and_extreme_numbers_read_as_the_reference_reads_them():
+    """`for dim in 1` visits 1 in Julia, so `dims: 1` is the list [1]; a
+    subnormal literal parses to a subnormal float (parse(Float64, ...))."""
+    text = YAML.replace("    hard_walls:\n      dims: [1]", "    hard_walls:\n      dims: 1")
+    text = text.replace("  tole: 1e-6", "  tole: 1e-6\n  mixed_switch: 1e-320")
+    assert text != YAML
+    _compare(text)
+    assert native.Input(text).numerics().mixed_switch == 1e-320
