@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <new>
+#include <stdexcept>
 #include <cstdio>
 #include <cstring>
 #include <deque>
@@ -189,6 +191,8 @@ static void fft_digit_slots(int M, const std::vector<int>& rad, std::vector<int>
 // padded to the even stride NP + 1 (the pad point lies beyond the grid)
 static int plan_grid(int Pt, Plan& pl) {
   if (Pt < 16) return set_err(SDFT_ERR_UNSUPPORTED, "the device solve needs NP >= 16 (got " + std::to_string(Pt) + ")");
+  if (Pt > (1 << 20))  // far above the one-CTA limit below; keeps NP + 1 and the sizes in range
+    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(Pt) + " needs more shared memory than a CTA has");
   const bool odd = (Pt & 1) != 0;
   const int P = odd ? Pt + 1 : Pt;
   const int Mf = odd ? Pt : Pt / 2;
@@ -213,8 +217,13 @@ int plan_species(const sdft_system_desc* d, Plan& pl) {
   if (d->nb < 1 || d->nb > kMaxBeads) return set_err(SDFT_ERR_UNSUPPORTED, "bead types must be in [1, 32]");
   if (d->mb < 0 || d->mb > kMaxBonds) return set_err(SDFT_ERR_UNSUPPORTED, "bond types must be in [0, 64]");
   if (d->n_species < 1 || d->n_species > 16) return set_err(SDFT_ERR_UNSUPPORTED, "species must be in [1, 16]");
-  if (d->bin_width <= 0) return set_err(SDFT_ERR_ARG, "bin_width must be positive");
+  if (!(d->bin_width > 0) || !std::isfinite(d->bin_width)) return set_err(SDFT_ERR_ARG, "bin_width must be positive and finite");
+  if (!std::isfinite(d->length)) return set_err(SDFT_ERR_ARG, "length must be finite");
   if (d->functionals & ~0xFu) return set_err(SDFT_ERR_ARG, "unknown functional bits");
+  for (int j = 0; j < d->nb; j++)
+    if (!std::isfinite(d->diameter[j])) return set_err(SDFT_ERR_ARG, "bead diameters must be finite");
+  for (int u = 0; u < 2 * d->mb; u++)  // the wall and bond tables index diameters by these
+    if (d->bond_types[u] < 0 || d->bond_types[u] >= d->nb) return set_err(SDFT_ERR_ARG, "bond_types entry out of range");
   pl.NB = d->nb;
   pl.MB = d->mb;
   pl.NS = d->n_species;
@@ -745,7 +754,7 @@ extern "C" void sdft_numerics_default(sdft_numerics* o) {
   o->mixed_switch = 0.0;
 }
 
-extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
+int request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
   if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
   *out = nullptr;
   if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
@@ -799,6 +808,17 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
   }
   *out = q;
   return SDFT_OK;
+}
+
+// host tables are sized by the descriptor; a failed host allocation is a status, not an exception across the C ABI
+extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
+  try {
+    return request_create(d, precision, out);
+  } catch (const std::bad_alloc&) {
+    return set_err(SDFT_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_err(SDFT_ERR_ARG, e.what());
+  }
 }
 
 extern "C" int sdft_request_destroy(sdft_handle h) {
@@ -1308,7 +1328,8 @@ int noalloc_scratch_address(void** out) {
 }
 }  // namespace
 
-extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x_dev, double* g_dev, void* stream_ptr) {
+namespace {
+int objective_noalloc(const sdft_system_desc* d, const double* x_dev, double* g_dev, void* stream_ptr) {
   if (!d || !x_dev || !g_dev) return set_err(SDFT_ERR_ARG, "null argument");
   if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
   Plan pl;
@@ -1340,4 +1361,15 @@ extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x
   CUDA_TRY(cudaStreamSynchronize(stream));
   if (st == ST_NORM) return set_err(SDFT_ERR_NORM, "Normalization error: lambda <= 0 or not finite");
   return SDFT_OK;
+}
+}  // namespace
+
+extern "C" int sdft_objective_noalloc(const sdft_system_desc* d, const double* x_dev, double* g_dev, void* stream_ptr) {
+  try {
+    return objective_noalloc(d, x_dev, g_dev, stream_ptr);
+  } catch (const std::bad_alloc&) {
+    return set_err(SDFT_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_err(SDFT_ERR_ARG, e.what());
+  }
 }

@@ -68,3 +68,33 @@ def test_branch_point_beyond_the_reference_arrays_is_refused(seq):
     """Three children of one segment with two states: the reference's
     other-children index (parent_propagators.jl:150) leaves its array."""
     _refused(_branched(seq), "index out of range")
+
+
+def _create_mutated(mutate):
+    dft = setup_request(small_slit())
+    d = dft.descriptor.desc
+    mutate(d)
+    h = C.c_void_p()
+    rc = native.lib().sdft_request_create(C.byref(d), 0, C.byref(h))
+    return rc, native.lib().sdft_last_error().decode()
+
+
+def _set_item(arr, i, v):
+    arr[i] = v
+
+
+@pytest.mark.parametrize("mutate,code,why", [
+    (lambda d: setattr(d, "bin_width", float("nan")), 2, "bin_width must be positive and finite"),
+    (lambda d: setattr(d, "bin_width", float("inf")), 2, "bin_width must be positive and finite"),
+    (lambda d: setattr(d, "length", float("-inf")), 2, "length must be finite"),
+    (lambda d: _set_item(d.diameter, 0, float("nan")), 2, "bead diameters must be finite"),
+    (lambda d: _set_item(d.bond_types, 1, 99), 2, "bond_types entry out of range"),
+    (lambda d: _set_item(d.bond_types, 0, -1), 2, "bond_types entry out of range"),
+    (lambda d: setattr(d, "np", 2 ** 31 - 1), 3, "needs more shared memory than a CTA has"),
+])
+def test_descriptor_values_that_would_misindex_are_refused(mutate, code, why):
+    """Values that the host tables or kernels would turn into indices (a grid
+    spacing, a wall position, a diameter, a bond's bead types, NP + 1) are
+    checked before anything is sized from them."""
+    rc, msg = _create_mutated(mutate)
+    assert rc == code and why in msg, (rc, msg)
