@@ -46,7 +46,7 @@ typedef enum sdft_status {
   SDFT_ERR_ARG = 2,          /* invalid descriptor or argument */
   SDFT_ERR_UNSUPPORTED = 3,  /* feature outside the device solve */
   SDFT_ERR_CUDA = 4,         /* CUDA runtime error or no device */
-  SDFT_ERR_OOM = 5,          /* device memory exhausted / admission refused */
+  SDFT_ERR_OOM = 5,          /* device or host memory exhausted / admission refused */
   SDFT_ERR_NORM = 6,         /* chain normalisation lambda <= 0 or not finite */
   SDFT_ERR_NONFINITE = 7,    /* NaN/Inf in the fixed-point residual */
   SDFT_ERR_TIMEOUT = 8       /* a bounded device wait gave up */
