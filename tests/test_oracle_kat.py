@@ -8,7 +8,10 @@ vectors and cannot run here, so these physics identities are the anchor):
   the bulk segment density;
 * ideal dissociation: the B-state fraction is 1/(1 + 10^(pKa - pH));
 * the k-space weights carry the analytic integrals at k = 0 (n3 of a uniform
-  density is rho*pi*sigma^3/6).
+  density is rho*pi*sigma^3/6);
+* contact-value theorem: at a hard wall the contact density of a hard-sphere
+  fluid equals its bulk pressure (contact_value_theorem.jl:5-20 against
+  eval_pressure.jl:10-25), up to a discretisation error of order dz^2.
 """
 import math
 
@@ -16,6 +19,8 @@ import numpy as np
 import pytest
 
 from oracle.oracle import OracleSystem
+from softdft_b200.host.descriptor import numerics_from_dict
+from softdft_b200.output import contact_value_theorem_arrays
 from tests.helpers import descriptor, rel, small_slit
 
 
@@ -142,3 +147,35 @@ def test_bulk_fixed_point_long_chain_renormalised():
     segs, beads, _ = o.densities()
     d = dft.descriptor
     assert rel(beads.reshape(d.nb, d.np_)[:, d.np_ // 2], dft.bulk_system.bulk.rho_beads) < 1e-8
+
+
+def _hard_sphere_slit(np_, dz, eta):
+    return {"procedure": "iDFT",
+            "geometry": {"coordinate_system": "Cartesian", "dimensions": [(np_ - 1) * dz], "bin_width": [dz],
+                         "external_field": {"hard_walls": {"dims": [1]}}},
+            "species": [{"sequence": "S", "density": eta * 6.0 / math.pi}],
+            "monomers": {"S": {"diameter": 1.0, "valence": 0.0}},
+            "numerical": {"tole": 1e-10, "damping": 0.1, "mixing_max": 0.5, "anderm": 5},
+            "model": ["ideal", "mfmt"]}
+
+
+def test_contact_value_theorem_hard_spheres():
+    """A 10-sigma slit of hard spheres at packing fraction 0.2: the contact
+    density at each wall equals the bulk pressure to 2e-4 at dz = 0.02, and
+    the error falls fourfold with each halving of dz."""
+    errors = []
+    for np_, dz in ((512, 0.02), (1023, 0.01), (2047, 0.005)):
+        ds = _hard_sphere_slit(np_, dz, 0.2)
+        dft = descriptor(ds)
+        o = OracleSystem(dft.descriptor)
+        it, err, _, _ = o.solve(numerics_from_dict(ds["numerical"]))
+        assert err < 1e-10, (np_, it, err)
+        _, beads, _ = o.densities()
+        P = dft.descriptor.desc.np
+        cvt = contact_value_theorem_arrays(beads.reshape(-1, P).T, dft.bulk_system.molsys, dft.geometry)
+        p_bulk = dft.bulk_system.bulk.pressure
+        errors.append(np.abs(cvt - p_bulk) / p_bulk)
+    errors = np.array(errors)
+    assert np.all(errors[0] < 2e-4)
+    ratios = errors[:-1] / errors[1:]
+    assert np.all((ratios > 3.5) & (ratios < 4.5)), ratios
