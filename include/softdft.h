@@ -248,7 +248,10 @@ int sdft_bulk_eval(const sdft_bulk_system* sys, const double* rho_species, const
  * the 1D slit with its fixed segments, restated in C++.
  * sdft_input_from_yaml: parses the text and builds the descriptor; errors come
  *   back as SDFT_ERR_ARG / SDFT_ERR_UNSUPPORTED with the reference's message in
- *   sdft_last_error().  Host only.
+ *   sdft_last_error().  Host only.  The reader takes the YAML the reference's
+ *   inputs use (block and flow collections, plain and quoted scalars, comments,
+ *   YAML.jl's exponent floats); a repeated key takes its last value, as in
+ *   YAML.jl; tags, anchors, aliases and block scalars are refused with the line.
  * sdft_input_descriptor: the descriptor for sdft_request_create; it stays valid
  *   until sdft_input_destroy.
  * sdft_input_numerics: the numerical section with the defaults of
