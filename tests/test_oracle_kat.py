@@ -11,7 +11,10 @@ vectors and cannot run here, so these physics identities are the anchor):
   density is rho*pi*sigma^3/6);
 * contact-value theorem: at a hard wall the contact density of a hard-sphere
   fluid equals its bulk pressure (contact_value_theorem.jl:5-20 against
-  eval_pressure.jl:10-25), up to a discretisation error of order dz^2.
+  eval_pressure.jl:10-25), up to a discretisation error of order dz^2;
+* electroneutrality: in a converged slit with charged walls the fluid's
+  trapezoid-weighted charge cancels the wall charge (the PsiC Newton step of
+  neutrality_shift.jl balances them).
 """
 import math
 
@@ -179,3 +182,21 @@ def test_contact_value_theorem_hard_spheres():
     assert np.all(errors[0] < 2e-4)
     ratios = errors[:-1] / errors[1:]
     assert np.all((ratios > 3.5) & (ratios < 4.5)), ratios
+
+
+def test_charged_slit_is_neutral():
+    """A weak-acid slit between walls of charge -0.05 each, solved to 1e-8: the
+    fluid carries +0.1 to within 1e-7 relative."""
+    ds = small_slit(np_=128, dz=0.05, wall_charge=-0.05)
+    ds["numerical"]["max_iters"] = 20000
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    it, err, _, _ = o.solve(numerics_from_dict(ds["numerical"]))
+    assert err < 1e-8, (it, err)
+    _, beads, _ = o.densities()
+    _, trapez = o.fields()
+    P = dft.descriptor.desc.np
+    z = np.asarray(dft.bulk_system.molsys.valences)
+    q_fluid = float((beads.reshape(-1, P).T * trapez.reshape(-1, P).T * z[None, :]).sum() * dft.geometry.bin_width)
+    q_walls = -0.05 - 0.05
+    assert abs(q_fluid + q_walls) < 1e-7 * abs(q_walls), q_fluid
