@@ -12,6 +12,9 @@ vectors and cannot run here, so these physics identities are the anchor):
 * contact-value theorem: at a hard wall the contact density of a hard-sphere
   fluid equals its bulk pressure (contact_value_theorem.jl:5-20 against
   eval_pressure.jl:10-25), up to a discretisation error of order dz^2;
+* grand potential: in a wall-free box at the bulk state, Omega
+  (grand_potential.jl:4-28) is -P_bulk times the box volume NP*dz, P_bulk from
+  the independent bulk formula (eval_pressure.jl:10-25);
 * electroneutrality: in a converged slit with charged walls the fluid's
   trapezoid-weighted charge cancels the wall charge (the PsiC Newton step of
   neutrality_shift.jl balances them).
@@ -200,3 +203,14 @@ def test_charged_slit_is_neutral():
     q_fluid = float((beads.reshape(-1, P).T * trapez.reshape(-1, P).T * z[None, :]).sum() * dft.geometry.bin_width)
     q_walls = -0.05 - 0.05
     assert abs(q_fluid + q_walls) < 1e-7 * abs(q_walls), q_fluid
+
+
+@pytest.mark.parametrize("models", [["ideal"], ["ideal", "mfmt", "msa"], ["ideal", "TPT1mfmt", "TPT1msa"]])
+def test_bulk_grand_potential_is_minus_pressure_volume(models):
+    ds = small_slit(models=models, walls=False)
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    o.objective()
+    volume = dft.descriptor.desc.np * dft.geometry.bin_width
+    p_bulk = dft.bulk_system.bulk.pressure
+    assert abs(o.grand_potential() + p_bulk * volume) < 1e-12 * p_bulk * volume
