@@ -12,6 +12,10 @@ vectors and cannot run here, so these physics identities are the anchor):
 * contact-value theorem: at a hard wall the contact density of a hard-sphere
   fluid equals its bulk pressure (contact_value_theorem.jl:5-20 against
   eval_pressure.jl:10-25), up to a discretisation error of order dz^2;
+* segment-resolved bulk state: in a wall-free box at the bulk state every
+  segment's state densities (chain ends and ionisation split included) equal
+  the bulk iLST segment densities at every grid point, and the species counts
+  (num_species.jl:1-38) are rho_u times the box volume;
 * grand potential: in a wall-free box at the bulk state, Omega
   (grand_potential.jl:4-28) is -P_bulk times the box volume NP*dz, P_bulk from
   the independent bulk formula (eval_pressure.jl:10-25);
@@ -214,3 +218,20 @@ def test_bulk_grand_potential_is_minus_pressure_volume(models):
     volume = dft.descriptor.desc.np * dft.geometry.bin_width
     p_bulk = dft.bulk_system.bulk.pressure
     assert abs(o.grand_potential() + p_bulk * volume) < 1e-12 * p_bulk * volume
+
+
+def test_bulk_segment_states_and_species_counts():
+    ds = small_slit(models=["ideal", "TPT1mfmt", "TPT1msa"], walls=False)
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    o.objective()
+    d = dft.descriptor.desc
+    bulk = dft.bulk_system.bulk
+    volume = d.np * dft.geometry.bin_width
+    assert rel(o.num_species(), np.asarray(bulk.rho_species) * volume) < 1e-13
+    segs, _, _ = o.densities()
+    for u in range(d.n_species):
+        S, N = d.species[u].max_states, d.species[u].n_seg
+        profile = segs[u].reshape(N, S, d.np).transpose(1, 0, 2)  # (state, segment, K)
+        expected = np.asarray(bulk.rho_segments[u])[:, :, None]     # (state, segment)
+        assert np.max(np.abs(profile - expected)) < 1e-13 * np.max(np.abs(expected)), u
