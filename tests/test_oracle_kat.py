@@ -29,6 +29,7 @@ import numpy as np
 import pytest
 
 from oracle.oracle import OracleSystem
+from softdft_b200 import workloads
 from softdft_b200.host.descriptor import numerics_from_dict
 from softdft_b200.output import contact_value_theorem_arrays
 from tests.helpers import descriptor, rel, small_slit
@@ -220,18 +221,31 @@ def test_bulk_grand_potential_is_minus_pressure_volume(models):
     assert abs(o.grand_potential() + p_bulk * volume) < 1e-12 * p_bulk * volume
 
 
-def test_bulk_segment_states_and_species_counts():
-    ds = small_slit(models=["ideal", "TPT1mfmt", "TPT1msa"], walls=False)
-    dft = descriptor(ds)
+def _bulk_box(name):
+    if name == "weak_acid":
+        return small_slit(models=["ideal", "TPT1mfmt", "TPT1msa"], walls=False)
+    if name == "diblock_200":
+        ds = workloads.diblock_slit(256)
+        ds["geometry"]["external_field"] = {}
+        return ds
+    ds = small_slit(models=["ideal"], walls=False)
+    ds["species"][0]["sequence"] = "AA(AA)AA"
+    return ds
+
+
+# tolerance: a 200-segment chain multiplies 200 convolved propagators
+@pytest.mark.parametrize("name,tol", [("weak_acid", 1e-13), ("diblock_200", 1e-9), ("branched_ideal", 1e-13)])
+def test_bulk_segment_states_and_species_counts(name, tol):
+    dft = descriptor(_bulk_box(name))
     o = OracleSystem(dft.descriptor)
     o.objective()
     d = dft.descriptor.desc
     bulk = dft.bulk_system.bulk
     volume = d.np * dft.geometry.bin_width
-    assert rel(o.num_species(), np.asarray(bulk.rho_species) * volume) < 1e-13
+    assert rel(o.num_species(), np.asarray(bulk.rho_species) * volume) < tol
     segs, _, _ = o.densities()
     for u in range(d.n_species):
         S, N = d.species[u].max_states, d.species[u].n_seg
         profile = segs[u].reshape(N, S, d.np).transpose(1, 0, 2)  # (state, segment, K)
         expected = np.asarray(bulk.rho_segments[u])[:, :, None]     # (state, segment)
-        assert np.max(np.abs(profile - expected)) < 1e-13 * np.max(np.abs(expected)), u
+        assert np.max(np.abs(profile - expected)) < tol * np.max(np.abs(expected)), u
