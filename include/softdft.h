@@ -49,7 +49,8 @@ typedef enum sdft_status {
   SDFT_ERR_OOM = 5,          /* device or host memory exhausted / admission refused */
   SDFT_ERR_NORM = 6,         /* chain normalisation lambda <= 0 or not finite */
   SDFT_ERR_NONFINITE = 7,    /* NaN/Inf in the fixed-point residual */
-  SDFT_ERR_TIMEOUT = 8       /* a bounded device wait gave up */
+  SDFT_ERR_TIMEOUT = 8       /* reserved: no call of this version waits on the device
+                                without a bound, so none returns it */
 } sdft_status;
 
 /* functional set (bitmask): the `model:` list of input.yaml minus `ideal`;
@@ -149,6 +150,43 @@ int sdft_objective(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, d
 
 /* Anderson-mixing solve from the current state; x is updated in place. */
 int sdft_solve(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err);
+
+/* Solver state of a request: what the Anderson driver carries from one
+ * iteration to the next in solver_function(::AndersonMixing, ...)
+ * (AndersonMixing.jl:80-168): the iteration count, the Picard flag, the last
+ * max-norm residual, the LSQR warm start `lambdas` (:88, :142) and the ring
+ * buffers X and G of depth m (:81-84; G holds the residuals G(x) - x).  The
+ * reference keeps these in locals of one call; here they persist in the request
+ * so that a solve can stop and continue (checkpoint / resume), move to another
+ * handle of the same system, or start from a given history. */
+typedef struct sdft_solver_state {
+  int32_t anderm;                /* depth m of the ring buffers */
+  int32_t iter;                  /* iterations done (0: fresh) */
+  int32_t use_picard;            /* 1 while the Picard phase lasts */
+  int32_t reserved;              /* 0 */
+  double err;                    /* max-norm residual of the last iteration */
+  double lambdas[15];            /* LSQR coefficients of the last Anderson step (anderm - 1 used) */
+} sdft_solver_state;
+
+/* Read / replace the solver state.  hist_x and hist_g hold anderm columns of
+ * n_unknowns doubles (ring slot c at offset c * n_unknowns, each column in the
+ * layout mu_ex_K | lng_K | Psi | PsiC of sdft_get_state); either may be NULL
+ * (set: zero columns).  Before any solve the state is fresh (iter 0). */
+int sdft_get_solver_state(sdft_handle h, sdft_solver_state* st, double* hist_x, double* hist_g);
+int sdft_set_solver_state(sdft_handle h, const sdft_solver_state* st, const double* hist_x, const double* hist_g);
+/* Continue the Anderson solve from the stored solver state (the end of the last
+ * solve, or sdft_set_solver_state) up to num->max_iters iterations in total;
+ * num->anderm must equal the state's.  sdft_solve starts from a fresh state,
+ * as a call of solver_function does. */
+int sdft_solve_resume(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err);
+/* One iteration of the Anderson driver with G(x) given by the caller (the
+ * layout of sdft_objective's outputs) instead of evaluated on the device: the
+ * loop body of AndersonMixing.jl:98-160 after `cur = objective_function(...)`.
+ * It updates x and the solver state; *err receives the max-norm residual
+ * |G(x) - x| of this iteration.  A caller that evaluates its own objective can
+ * drive the device mixer with it, as solver_function takes any objective. */
+int sdft_anderson_step(sdft_handle h, const sdft_numerics* num, const double* g_mu_ex_K, const double* g_lng_K,
+                       const double* g_Psi, const double* g_PsiC, double* err);
 
 /* Densities of the last G(x) evaluation.  rho_segments: array of n_species host
  * pointers (entries may be NULL).  Any argument may be NULL. */
@@ -279,8 +317,10 @@ int sdft_input_destroy(sdft_input* in);
  *    loading the library holds until the process exits.  A system whose working
  *    set exceeds it is rejected with SDFT_ERR_ARG and a message giving both sizes
  *    (the plain slit, NP = 1024 with a 20-segment chain, needs about 3 MB).
- *  - The first call on a device looks up the array's device address; make that
- *    first call before any stream capture.
+ *  - Every call looks up the array's address in the current device's context
+ *    (cudaGetSymbolAddress), uploads the system's tables from host memory and
+ *    waits for its stream, so it cannot be called on a stream that is being
+ *    captured into a CUDA graph.
  *  - All calls share the array and it keeps the last call's contents; each call
  *    clears the part it uses.  Calls that overlap on the GPU (other streams or
  *    host threads) race on it.

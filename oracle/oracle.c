@@ -200,6 +200,14 @@ struct oracle_sys {
   fft_plan plan;
   /* scratch */
   double *nai, *wtb, *dphi, *lngK, *wtrho;
+  /* Anderson driver state kept between calls (checkpoint / resume): the ring
+     buffers X (unknowns) and G (residuals G(x) - x) of depth hm, the
+     iteration count, the Picard flag, the last residual and the LSQR warm start */
+  double *hX, *hG;
+  int hm;
+  int32_t s_iter, s_use_picard;
+  double s_err;
+  double s_lam[64];
 };
 
 #define IDX_MU(o, K, j) ((size_t)(j) * (o)->NP + (K))
@@ -348,6 +356,7 @@ void oracle_destroy(oracle_sys* o) {
   free(o->surf_hat); free(o->f_hat); free(o->w_bond); free(o->w_fmt); free(o->w_msa);
   free(o->w_coul); free(o->filter); free(o->nai); free(o->wtb); free(o->dphi); free(o->lngK);
   free(o->wtrho);
+  free(o->hX); free(o->hG);
   fft_plan_free(&o->plan);
   free(o);
 }
@@ -1565,80 +1574,198 @@ static void lsqr(const double* A, int64_t m, int nc, const double* b, double* x,
   }
 }
 
-/* solver_function(::AndersonMixing, ...) (AndersonMixing.jl:56-169) */
-int oracle_solve_trace(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double* err_out,
-                       double* trace, int32_t trace_len) {
-  int64_t n = o->n;
-  int m = num->anderm;
-  if (m < 2 || m > 60) return fail(SDFT_ERR_ARG, "anderm must be in [2, 60]");
-  double *X = calloc((size_t)n * m, sizeof(double)), *G = calloc((size_t)n * m, sizeof(double));
-  double *Xk = malloc(sizeof(double) * n), *Gk = malloc(sizeof(double) * n), *cur = malloc(sizeof(double) * n);
-  double *tX = calloc((size_t)n * (m - 1), sizeof(double)), *tG = calloc((size_t)n * (m - 1), sizeof(double));
-  double *rhs = malloc(sizeof(double) * n), *u = malloc(sizeof(double) * n), *tmpm = malloc(sizeof(double) * n);
-  double lambdas[64] = {0};
-  if (!X || !G || !Xk || !Gk || !cur || !tX || !tG || !rhs || !u || !tmpm) {
-    free(X); free(G); free(Xk); free(Gk); free(cur); free(tX); free(tG); free(rhs); free(u); free(tmpm);
+/* ring buffers of depth m, reallocated when m changes; 0 or an error status */
+static int anderson_buffers(oracle_sys* o, int m) {
+  if (o->hm == m && o->hX && o->hG) return SDFT_OK;
+  free(o->hX); free(o->hG);
+  o->hX = calloc((size_t)o->n * m, sizeof(double));
+  o->hG = calloc((size_t)o->n * m, sizeof(double));
+  o->hm = m;
+  if (!o->hX || !o->hG) {
+    free(o->hX); free(o->hG);
+    o->hX = o->hG = NULL;
+    o->hm = 0;
     return fail(SDFT_ERR_OOM, "out of memory");
   }
-  double err = 1.0;
-  int iter = 0, use_picard = 1, rc = SDFT_OK;
-  while (iter < num->max_iters) {
-    iter++;
-    rc = oracle_objective(o, cur);
-    if (rc) break;
-    int col = (iter - 1) % m;
-    memcpy(Xk, o->x, sizeof(double) * n);
-    double mx = 0.0;
-    int finite = 1;
-    for (int64_t k = 0; k < n; k++) {
-      Gk[k] = cur[k] - Xk[k];
-      X[(size_t)col * n + k] = Xk[k];
-      G[(size_t)col * n + k] = Gk[k];
-      double a = fabs(Gk[k]);
-      if (!(a == a) || a == INFINITY) finite = 0;
-      if (a > mx) mx = a;
-    }
-    if (!finite) { rc = fail(SDFT_ERR_NONFINITE, "non-finite fixed-point residual"); break; }
-    err = mx > 1e-20 ? mx : 1e-20;
-    if (trace && iter <= trace_len) trace[iter - 1] = err;
-    double amix = fmin(num->mixing_max, num->damping / err);
-    if (iter < m || (err > num->switch_tole && use_picard)) {
-      double c1 = 1.0 - amix, c2 = amix;
-      for (int64_t k = 0; k < n; k++) o->x[k] = c1 * o->x[k] + c2 * cur[k];
-    } else {
-      use_picard = 0;
-      int i = 0;
-      for (int j = 0; j < m; j++) {
-        if (j == col) continue;
-        for (int64_t k = 0; k < n; k++) {
-          tX[(size_t)i * n + k] = X[(size_t)j * n + k] - Xk[k];
-          tG[(size_t)i * n + k] = G[(size_t)j * n + k] - Gk[k];
-        }
-        i++;
-      }
-      for (int64_t k = 0; k < n; k++) rhs[k] = -Gk[k];
-      lsqr(tG, n, m - 1, rhs, lambdas, u, tmpm);
-      for (int64_t k = 0; k < n; k++) {
-        double sx = 0.0, sg = 0.0;
-        for (int c = 0; c < m - 1; c++) {
-          sx += tX[(size_t)c * n + k] * lambdas[c];
-          sg += tG[(size_t)c * n + k] * lambdas[c];
-        }
-        double r = Xk[k] + sx + amix * (Gk[k] + sg);
-        o->x[k] = 0.0 * Xk[k] + 1.0 * r;
-      }
-    }
-    if (err < num->tole) break;
+  return SDFT_OK;
+}
+
+static void anderson_reset(oracle_sys* o) {
+  o->s_iter = 0;
+  o->s_use_picard = 1;
+  o->s_err = 1.0;
+  memset(o->s_lam, 0, sizeof(o->s_lam));
+}
+
+/* One pass of the loop body of solver_function(::AndersonMixing, ...)
+ * (AndersonMixing.jl:98-160) with cur = G(x) already evaluated: ring-buffer
+ * column col = mod(iter - 1, m) (:102), residual, amix (:112-114), Picard step
+ * (:123-125) or the least-squares step (:127-145).  Returns 0, or
+ * SDFT_ERR_NONFINITE. */
+static int anderson_update(oracle_sys* o, const sdft_numerics* num, const double* cur, double* tX, double* tG,
+                           double* Xk, double* Gk, double* rhs, double* u, double* tmpm) {
+  const int64_t n = o->n;
+  const int m = o->hm;
+  const int iter = ++o->s_iter;
+  const int col = (iter - 1) % m;
+  double* X = o->hX;
+  double* G = o->hG;
+  memcpy(Xk, o->x, sizeof(double) * n);
+  double mx = 0.0;
+  int finite = 1;
+  for (int64_t k = 0; k < n; k++) {
+    Gk[k] = cur[k] - Xk[k];
+    X[(size_t)col * n + k] = Xk[k];
+    G[(size_t)col * n + k] = Gk[k];
+    double a = fabs(Gk[k]);
+    if (!(a == a) || a == INFINITY) finite = 0;
+    if (a > mx) mx = a;
   }
-  *iters = iter;
-  *err_out = err;
-  free(X); free(G); free(Xk); free(Gk); free(cur); free(tX); free(tG); free(rhs); free(u); free(tmpm);
+  if (!finite) {
+    o->s_err = mx;
+    return fail(SDFT_ERR_NONFINITE, "non-finite fixed-point residual");
+  }
+  double err = mx > 1e-20 ? mx : 1e-20;
+  o->s_err = err;
+  double amix = fmin(num->mixing_max, num->damping / err);
+  if (iter < m || (err > num->switch_tole && o->s_use_picard)) {
+    double c1 = 1.0 - amix, c2 = amix;
+    for (int64_t k = 0; k < n; k++) o->x[k] = c1 * o->x[k] + c2 * cur[k];
+  } else {
+    o->s_use_picard = 0;
+    int i = 0;
+    for (int j = 0; j < m; j++) {
+      if (j == col) continue;
+      for (int64_t k = 0; k < n; k++) {
+        tX[(size_t)i * n + k] = X[(size_t)j * n + k] - Xk[k];
+        tG[(size_t)i * n + k] = G[(size_t)j * n + k] - Gk[k];
+      }
+      i++;
+    }
+    for (int64_t k = 0; k < n; k++) rhs[k] = -Gk[k];
+    lsqr(tG, n, m - 1, rhs, o->s_lam, u, tmpm);
+    for (int64_t k = 0; k < n; k++) {
+      double sx = 0.0, sg = 0.0;
+      for (int c = 0; c < m - 1; c++) {
+        sx += tX[(size_t)c * n + k] * o->s_lam[c];
+        sg += tG[(size_t)c * n + k] * o->s_lam[c];
+      }
+      double r = Xk[k] + sx + amix * (Gk[k] + sg);
+      o->x[k] = 0.0 * Xk[k] + 1.0 * r;
+    }
+  }
+  return SDFT_OK;
+}
+
+/* work vectors of one Anderson update */
+typedef struct {
+  double *cur, *tX, *tG, *Xk, *Gk, *rhs, *u, *tmpm;
+} anderson_work;
+
+static void work_free(anderson_work* w) {
+  free(w->cur); free(w->tX); free(w->tG); free(w->Xk); free(w->Gk); free(w->rhs); free(w->u); free(w->tmpm);
+}
+
+static int work_alloc(anderson_work* w, int64_t n, int m) {
+  w->cur = malloc(sizeof(double) * n);
+  w->tX = calloc((size_t)n * (m - 1), sizeof(double));
+  w->tG = calloc((size_t)n * (m - 1), sizeof(double));
+  w->Xk = malloc(sizeof(double) * n);
+  w->Gk = malloc(sizeof(double) * n);
+  w->rhs = malloc(sizeof(double) * n);
+  w->u = malloc(sizeof(double) * n);
+  w->tmpm = malloc(sizeof(double) * n);
+  if (!w->cur || !w->tX || !w->tG || !w->Xk || !w->Gk || !w->rhs || !w->u || !w->tmpm) {
+    work_free(w);
+    return fail(SDFT_ERR_OOM, "out of memory");
+  }
+  return SDFT_OK;
+}
+
+/* solver_function(::AndersonMixing, ...) (AndersonMixing.jl:56-169), continuing
+ * from the state in o (iteration count, Picard flag, ring buffers, warm start) */
+static int solve_loop(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double* err_out, double* trace,
+                      int32_t trace_len) {
+  int m = num->anderm;
+  if (m < 2 || m > 60) return fail(SDFT_ERR_ARG, "anderm must be in [2, 60]");
+  if (o->hm != m) return fail(SDFT_ERR_ARG, "anderm differs from the solver state's");
+  anderson_work w;
+  int rc = work_alloc(&w, o->n, m);
   if (rc) return rc;
-  return (err < num->tole) ? SDFT_OK : SDFT_MAX_ITERS;
+  while (o->s_iter < num->max_iters) {
+    rc = oracle_objective(o, w.cur);
+    if (rc) break;
+    rc = anderson_update(o, num, w.cur, w.tX, w.tG, w.Xk, w.Gk, w.rhs, w.u, w.tmpm);
+    if (rc) break;
+    if (trace && o->s_iter <= trace_len) trace[o->s_iter - 1] = o->s_err;
+    if (o->s_err < num->tole) break;
+  }
+  *iters = o->s_iter;
+  *err_out = o->s_err;
+  work_free(&w);
+  if (rc) return rc;
+  return (o->s_err < num->tole) ? SDFT_OK : SDFT_MAX_ITERS;
+}
+
+int oracle_solve_trace(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double* err_out,
+                       double* trace, int32_t trace_len) {
+  int m = num->anderm;
+  if (m < 2 || m > 60) return fail(SDFT_ERR_ARG, "anderm must be in [2, 60]");
+  int rc = anderson_buffers(o, m);
+  if (rc) return rc;
+  memset(o->hX, 0, sizeof(double) * (size_t)o->n * m);
+  memset(o->hG, 0, sizeof(double) * (size_t)o->n * m);
+  anderson_reset(o);
+  return solve_loop(o, num, iters, err_out, trace, trace_len);
 }
 
 int oracle_solve(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double* err) {
   return oracle_solve_trace(o, num, iters, err, NULL, 0);
+}
+
+int oracle_solve_resume(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double* err) {
+  if (!o->hX) return fail(SDFT_ERR_ARG, "no solver state to resume");
+  return solve_loop(o, num, iters, err, NULL, 0);
+}
+
+int oracle_get_solver_state(const oracle_sys* o, sdft_solver_state* st, double* hist_x, double* hist_g) {
+  if (!o->hX) return fail(SDFT_ERR_ARG, "no solver state");
+  memset(st, 0, sizeof(*st));
+  st->anderm = o->hm;
+  st->iter = o->s_iter;
+  st->use_picard = o->s_use_picard;
+  st->err = o->s_err;
+  for (int c = 0; c < o->hm - 1 && c < 15; c++) st->lambdas[c] = o->s_lam[c];
+  if (hist_x) memcpy(hist_x, o->hX, sizeof(double) * (size_t)o->n * o->hm);
+  if (hist_g) memcpy(hist_g, o->hG, sizeof(double) * (size_t)o->n * o->hm);
+  return SDFT_OK;
+}
+
+int oracle_set_solver_state(oracle_sys* o, const sdft_solver_state* st, const double* hist_x, const double* hist_g) {
+  if (st->anderm < 2 || st->anderm > 16) return fail(SDFT_ERR_ARG, "anderm must be in [2, 16]");
+  int rc = anderson_buffers(o, st->anderm);
+  if (rc) return rc;
+  anderson_reset(o);
+  o->s_iter = st->iter;
+  o->s_use_picard = st->use_picard;
+  o->s_err = st->err;
+  for (int c = 0; c < st->anderm - 1; c++) o->s_lam[c] = st->lambdas[c];
+  size_t bytes = sizeof(double) * (size_t)o->n * st->anderm;
+  if (hist_x) memcpy(o->hX, hist_x, bytes); else memset(o->hX, 0, bytes);
+  if (hist_g) memcpy(o->hG, hist_g, bytes); else memset(o->hG, 0, bytes);
+  return SDFT_OK;
+}
+
+int oracle_anderson_step(oracle_sys* o, const sdft_numerics* num, const double* g, double* err) {
+  if (!o->hX || o->hm != num->anderm) return fail(SDFT_ERR_ARG, "anderm differs from the solver state's");
+  anderson_work w;
+  int rc = work_alloc(&w, o->n, num->anderm);
+  if (rc) return rc;
+  memcpy(w.cur, g, sizeof(double) * o->n);
+  rc = anderson_update(o, num, w.cur, w.tX, w.tG, w.Xk, w.Gk, w.rhs, w.u, w.tmpm);
+  *err = o->s_err;
+  work_free(&w);
+  return rc;
 }
 
 int oracle_get_densities(const oracle_sys* o, double* const* rho_segments, double* rho_beads, double* rho_bonds) {

@@ -41,6 +41,15 @@ int oracle_solve(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double
 int oracle_solve_trace(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double* err,
                        double* err_trace, int32_t trace_len);
 
+/* Anderson driver state (sdft_solver_state of softdft.h; hist_x / hist_g hold
+ * anderm columns of n_unknowns in the flattening of x): read it after a solve,
+ * set it to seed one, continue a solve from it, or take one driver iteration
+ * with a given G(x) instead of evaluating it */
+int oracle_get_solver_state(const oracle_sys* o, sdft_solver_state* st, double* hist_x, double* hist_g);
+int oracle_set_solver_state(oracle_sys* o, const sdft_solver_state* st, const double* hist_x, const double* hist_g);
+int oracle_solve_resume(oracle_sys* o, const sdft_numerics* num, int32_t* iters, double* err);
+int oracle_anderson_step(oracle_sys* o, const sdft_numerics* num, const double* g, double* err);
+
 int oracle_get_densities(const oracle_sys* o, double* const* rho_segments, double* rho_beads,
                          double* rho_bonds);
 int oracle_grand_potential(oracle_sys* o, double* omega);

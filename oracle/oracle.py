@@ -12,7 +12,7 @@ import subprocess
 
 import numpy as np
 
-from softdft_b200.host.descriptor import Descriptor, Numerics
+from softdft_b200.host.descriptor import Descriptor, Numerics, SolverState
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -48,6 +48,10 @@ def lib():
         L.oracle_get_fields.argtypes = [vp, vp, vp]
         L.oracle_solve_many.argtypes = [vp, C.c_int32, vp, vp, vp, vp, C.c_int32]
         L.oracle_max_threads.restype = C.c_int
+        L.oracle_get_solver_state.argtypes = [vp, vp, vp, vp]
+        L.oracle_set_solver_state.argtypes = [vp, vp, vp, vp]
+        L.oracle_solve_resume.argtypes = [vp, vp, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        L.oracle_anderson_step.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
         _LIB = L
     return _LIB
 
@@ -107,6 +111,32 @@ class OracleSystem:
         tr = np.zeros(max(trace_len, 1))
         rc = _check(lib().oracle_solve_trace(self.h, C.byref(num), C.byref(it), C.byref(err), _p(tr), trace_len))
         return int(it.value), float(err.value), rc, tr[: min(trace_len, it.value)]
+
+    def solve_resume(self, num: Numerics):
+        it = C.c_int32()
+        err = C.c_double()
+        rc = _check(lib().oracle_solve_resume(self.h, C.byref(num), C.byref(it), C.byref(err)))
+        return int(it.value), float(err.value), rc
+
+    def solver_state(self):
+        st = SolverState()
+        _check(lib().oracle_get_solver_state(self.h, C.byref(st), None, None))
+        hx = np.zeros(st.anderm * self.n)
+        hg = np.zeros(st.anderm * self.n)
+        _check(lib().oracle_get_solver_state(self.h, C.byref(st), _p(hx), _p(hg)))
+        return st, hx.reshape(st.anderm, self.n), hg.reshape(st.anderm, self.n)
+
+    def set_solver_state(self, st: SolverState, hist_x=None, hist_g=None) -> None:
+        hx = None if hist_x is None else np.ascontiguousarray(hist_x, dtype=np.float64).ravel()
+        hg = None if hist_g is None else np.ascontiguousarray(hist_g, dtype=np.float64).ravel()
+        _check(lib().oracle_set_solver_state(self.h, C.byref(st), _p(hx) if hx is not None else None,
+                                             _p(hg) if hg is not None else None))
+
+    def anderson_step(self, num: Numerics, g: np.ndarray) -> float:
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        err = C.c_double()
+        _check(lib().oracle_anderson_step(self.h, C.byref(num), _p(g), C.byref(err)))
+        return float(err.value)
 
     def densities(self):
         d = self.d

@@ -141,12 +141,16 @@ def iDFT(input_file: str, precision: int = desc_mod.PREC_FP64, directory: Option
     return eval_inhomogeneous(dft, directory)
 
 
-def densities(dft: IsingDFT):
-    """rho_segments (list of (NP, S_u, N_u)), rho_beads_K (NP, NB), rho_bonds_K (NP, 2, MB)."""
-    d = dft.descriptor
-    segs, beads, bonds = dft.handle().densities()
+def shape_densities(d, segs, beads, bonds):
+    """Flat density arrays in the ABI's column-major order -> rho_segments (list
+    of (NP, S_u, N_u)), rho_beads_K (NP, NB), rho_bonds_K (NP, 2, MB)."""
     segs = [s.reshape((d.np_, d.max_states[u], d.n_seg[u]), order="F") for u, s in enumerate(segs)]
     return segs, beads.reshape((d.np_, d.nb), order="F"), bonds.reshape((d.np_, 2, d.mb), order="F")
+
+
+def densities(dft: IsingDFT):
+    """rho_segments (list of (NP, S_u, N_u)), rho_beads_K (NP, NB), rho_bonds_K (NP, 2, MB)."""
+    return shape_densities(dft.descriptor, *dft.handle().densities())
 
 
 def grand_potential(dft: IsingDFT) -> float:
@@ -160,7 +164,13 @@ def get_num_species(dft: IsingDFT) -> np.ndarray:
 def state_fractions(dft: IsingDFT):
     """Per species with multi-state segments: per-segment state fractions and
     their average over dissociating segments (write_total_state_fractions)."""
-    segs, _, _ = densities(dft)
+    return state_fractions_of(dft, densities(dft)[0])
+
+
+def state_fractions_of(dft: IsingDFT, segs):
+    """state_fractions for given segment densities (list of (NP, S_u, N_u)):
+    the degree of dissociation of degree_of_dissociation.jl:1-78, a plain sum
+    over the grid per (segment, state) normalised over the segment's states."""
     out = {}
     for u, cfg in enumerate(dft.bulk_system.molsys.configurations):
         fam = cfg.state_family

@@ -524,12 +524,22 @@ def _pac_branches(branches, kind, ds_init, max_steps, num, pH_range, corrector_t
                 if not ok(dft) or abs(f) <= corrector_tol * used[b] or last:
                     done[b] = (dft, it + 1, ok(dft) and abs(f) <= corrector_tol * used[b], f)
                     continue
+                # a pH turning point has t_pH = 0: the constraint cannot move pH
+                # there, so the branch's corrector stops as failed
+                flat = abs(t[-1]) <= 1e-12 * max(float(np.max(np.abs(t))), 1e-300)
                 if len(hist[b]) == 1:
                     # the reference's constraint update: pH = pH_k + (dS - t_x . (x - x_k)) / t_pH
-                    lam[b] = lam[b] - f / t[-1]
+                    new_lam = lam[b] - f / t[-1] if not flat else float("nan")
                 else:
                     (l0, f0), (l1, f1) = hist[b][-2], hist[b][-1]
-                    lam[b] = l1 - f1 * (l1 - l0) / (f1 - f0) if f1 != f0 else l1 - f1 / t[-1]
+                    if f1 != f0:
+                        new_lam = l1 - f1 * (l1 - l0) / (f1 - f0)
+                    else:
+                        new_lam = l1 - f1 / t[-1] if not flat else float("nan")
+                if not np.isfinite(new_lam):
+                    done[b] = (dft, it + 1, False, f)
+                    continue
+                lam[b] = new_lam
                 xstart[b] = x
                 dft.handle().close()
                 nxt.append(b)

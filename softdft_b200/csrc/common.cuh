@@ -253,6 +253,8 @@ cudaError_t launch_objective_pow2(const DReq* reqs, int n, size_t smem, cudaStre
 cudaError_t launch_solve_pow2(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, int max_chunk, int n, size_t smem,
                               cudaStream_t s);
 cudaError_t launch_omega_pow2(const DReq* reqs, double* out, size_t smem, cudaStream_t s);
+cudaError_t launch_anderson_pow2(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, cudaStream_t s);
+cudaError_t launch_anderson_gen(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, cudaStream_t s);
 cudaError_t launch_objective_gen(const DReq* reqs, int n, size_t smem, cudaStream_t s);
 cudaError_t launch_solve_gen(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, int max_chunk, int n, size_t smem,
                              cudaStream_t s);

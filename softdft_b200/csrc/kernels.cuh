@@ -94,6 +94,28 @@ extern "C" __global__ void __launch_bounds__(kThreads, 3)
   }
 }
 
+// one iteration of the Anderson driver with r.g = G(x) supplied by the caller
+extern "C" __global__ void __launch_bounds__(kThreads) SDFT_KNAME(sdft_k_anderson)(const DReq* reqs, SolveSlot* slots,
+                                                                                  SolveCfg cfg) {
+  extern __shared__ double smem[];
+  const DReq& r = reqs[blockIdx.x];
+  SolveSlot* sl = &slots[blockIdx.x];
+  if (r.gen != SDFT_FFT_GEN) return;
+  AndersonState st;
+  st.use_picard = sl->use_picard;
+  for (int c = 0; c < kMaxAnderson; c++) st.lam[c] = sl->lam[c];
+  const int iter = sl->iter + 1;
+  double err = sl->err;
+  const int s = anderson_step(r, cfg, iter, st, smem, &err);
+  if (threadIdx.x == 0) {
+    sl->iter = iter;
+    sl->status = s;
+    sl->use_picard = st.use_picard;
+    sl->err = err;
+    for (int c = 0; c < kMaxAnderson; c++) sl->lam[c] = st.lam[c];
+  }
+}
+
 extern "C" __global__ void __launch_bounds__(kThreads) SDFT_KNAME(sdft_k_omega)(const DReq* reqs, double* out) {
   extern __shared__ double smem[];
   const DReq& r = reqs[blockIdx.x];
@@ -122,6 +144,11 @@ cudaError_t SDFT_KLAUNCH(launch_solve)(const DReq* reqs, SolveSlot* slots, Solve
   cudaError_t e = allow_smem((const void*)SDFT_KNAME(sdft_k_solve), smem);
   if (e != cudaSuccess) return e;
   SDFT_KNAME(sdft_k_solve)<<<n, kThreads, smem, s>>>(reqs, slots, cfg, max_chunk);
+  return cudaGetLastError();
+}
+
+cudaError_t SDFT_KLAUNCH(launch_anderson)(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, cudaStream_t s) {
+  SDFT_KNAME(sdft_k_anderson)<<<1, kThreads, sizeof(double) * kRedDoubles, s>>>(reqs, slots, cfg);
   return cudaGetLastError();
 }
 

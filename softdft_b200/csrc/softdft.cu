@@ -728,7 +728,21 @@ struct sdft_request {
   DReq* dreq = nullptr;
   SolveSlot* dslot = nullptr;
   double* dout = nullptr;  // omega + num species
+  // solver state after the last solve (checkpoint / resume): iteration count,
+  // Picard flag, residual and LSQR warm start; the ring buffers stay in hx / hg
+  SolveSlot slot{};
+  int slot_m = 0;  // depth of the ring buffers in use (0: fresh)
 };
+
+// the state of a solve that has not started (AndersonMixing.jl:80-90)
+static SolveSlot fresh_slot() {
+  SolveSlot s{};
+  s.iter = 0;
+  s.status = ST_RUNNING;
+  s.use_picard = 1;
+  s.err = 1.0;
+  return s;
+}
 
 extern "C" int32_t sdft_abi_version(void) { return SDFT_ABI_VERSION; }
 extern "C" const char* sdft_last_error(void) { return g_err.c_str(); }
@@ -967,9 +981,14 @@ static int validate_numerics(const sdft_numerics* num) {
 }
 
 // chunked persistent solve of a batch of requests that share one stream
-static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32_t* iters, double* errs, int32_t* status) {
+static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32_t* iters, double* errs, int32_t* status,
+                     bool resume = false) {
   int rc = validate_numerics(num);
   if (rc) return rc;
+  if (resume)
+    for (int i = 0; i < n; i++)
+      if (hs[i]->slot_m != 0 && hs[i]->slot_m != num->anderm)
+        return set_err(SDFT_ERR_ARG, "anderm differs from the solver state's");
   cudaStream_t stream = hs[0]->stream;
   size_t sm = 0;
   bool any_pow2 = false, any_gen = false;
@@ -977,19 +996,33 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
     sm = std::max(sm, smem_bytes(hs[i]->M));
     (hs[i]->h.gen ? any_gen : any_pow2) = true;
   }
-  DReq* dreqs = nullptr;
-  SolveSlot* dslots = nullptr;
-  CUDA_TRY(cudaMallocAsync(&dreqs, sizeof(DReq) * n, stream));
-  CUDA_TRY(cudaMallocAsync(&dslots, sizeof(SolveSlot) * n, stream));
+  // device arrays and events of this batch, released on every return path
+  struct BatchRes {
+    cudaStream_t stream;
+    DReq* dreqs = nullptr;
+    SolveSlot* dslots = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~BatchRes() {
+      if (dreqs) cudaFreeAsync(dreqs, stream);
+      if (dslots) cudaFreeAsync(dslots, stream);
+      if (ev0) cudaEventDestroy(ev0);
+      if (ev1) cudaEventDestroy(ev1);
+      if (dreqs || dslots) cudaStreamSynchronize(stream);
+    }
+  } res{stream};
+  CUDA_TRY(cudaMallocAsync(&res.dreqs, sizeof(DReq) * n, stream));
+  CUDA_TRY(cudaMallocAsync(&res.dslots, sizeof(SolveSlot) * n, stream));
+  DReq* const dreqs = res.dreqs;
+  SolveSlot* const dslots = res.dslots;
   std::vector<DReq> hreq(n);
   std::vector<SolveSlot> slots(n);
   for (int i = 0; i < n; i++) {
     hreq[i] = hs[i]->h;
-    SolveSlot s{};
-    s.iter = 0;
-    s.status = ST_RUNNING;
-    s.use_picard = 1;
-    s.err = 1.0;
+    SolveSlot s = fresh_slot();
+    if (resume && hs[i]->slot_m) {
+      s = hs[i]->slot;
+      s.status = ST_RUNNING;
+    }
     slots[i] = s;
   }
   // requests on other streams must be idle before the batch stream uses them
@@ -1008,9 +1041,9 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
   // bounded launches: each runs at most `chunk` iterations per request, the
   // host re-launches until every request has converged, failed or hit max_iters
   const int chunk = 1024;
-  cudaEvent_t ev0, ev1;
-  CUDA_TRY(cudaEventCreate(&ev0));
-  CUDA_TRY(cudaEventCreate(&ev1));
+  CUDA_TRY(cudaEventCreate(&res.ev0));
+  CUDA_TRY(cudaEventCreate(&res.ev1));
+  cudaEvent_t const ev0 = res.ev0, ev1 = res.ev1;
   double dev_ms = 0.0;
   int launches = 0;
   for (;;) {
@@ -1026,17 +1059,14 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
     for (int i = 0; i < n; i++) running |= slots[i].status == ST_RUNNING;
     if (!running) break;
   }
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
   g_batch_ms = dev_ms;
   g_batch_launches = launches;
   g_batch_latency.assign(n, 0.0);
   for (int i = 0; i < n; i++) g_batch_latency[i] = (double)(slots[i].t1 - slots[i].t0) * 1e-6;
-  cudaFreeAsync(dreqs, stream);
-  cudaFreeAsync(dslots, stream);
-  CUDA_TRY(cudaStreamSynchronize(stream));
   int worst = SDFT_OK;
   for (int i = 0; i < n; i++) {
+    hs[i]->slot = slots[i];
+    hs[i]->slot_m = num->anderm;
     if (iters) iters[i] = slots[i].iter;
     if (errs) errs[i] = slots[i].err;
     int r = slots[i].status == ST_OK ? SDFT_OK
@@ -1049,17 +1079,129 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
   return worst;
 }
 
-extern "C" int sdft_solve(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err) {
+static int solve_one(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err, bool resume) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
   int32_t it = 0, st = 0;
   double e = 0.0;
-  int rc = run_batch(&h, 1, num, &it, &e, &st);
+  int rc = run_batch(&h, 1, num, &it, &e, &st, resume);
+  if (rc == SDFT_ERR_ARG || rc == SDFT_ERR_UNSUPPORTED) return rc;
   if (iters) *iters = it;
   if (err) *err = e;
   if (rc == SDFT_ERR_CUDA) return rc;
   if (st == SDFT_ERR_NORM) return set_err(SDFT_ERR_NORM, "Normalization error: lambda <= 0 or not finite");
   if (st == SDFT_ERR_NONFINITE) return set_err(SDFT_ERR_NONFINITE, "non-finite fixed-point residual");
   return st;
+}
+
+extern "C" int sdft_solve(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err) {
+  return solve_one(h, num, iters, err, false);
+}
+
+extern "C" int sdft_solve_resume(sdft_handle h, const sdft_numerics* num, int32_t* iters, double* err) {
+  return solve_one(h, num, iters, err, true);
+}
+
+// one caller-layout vector (mu_ex_K | lng_K | Psi | PsiC, NPt points per row)
+// to or from a device vector of stride NP
+static int vec_in(sdft_handle h, double* dv, const double* src) {
+  const size_t P = h->NP, Pt = h->NPt, rows = (size_t)h->NB + 2 * h->MB + 1;
+  CUDA_TRY(rows_copy(h, dv, src, rows, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(dv + P * rows, src + Pt * rows, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  return SDFT_OK;
+}
+static int vec_out(sdft_handle h, const double* dv, double* dst) {
+  const size_t P = h->NP, Pt = h->NPt, rows = (size_t)h->NB + 2 * h->MB + 1;
+  CUDA_TRY(rows_copy(h, dst, dv, rows, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpyAsync(dst + Pt * rows, dv + P * rows, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_get_solver_state(sdft_handle h, sdft_solver_state* st, double* hist_x, double* hist_g) {
+  if (!h || !st) return set_err(SDFT_ERR_ARG, "null argument");
+  const SolveSlot& s = h->slot_m ? h->slot : fresh_slot();
+  std::memset(st, 0, sizeof(*st));
+  st->anderm = h->slot_m;
+  st->iter = s.iter;
+  st->use_picard = s.use_picard;
+  st->err = s.err;
+  for (int c = 0; c + 1 < h->slot_m && c < 15; c++) st->lambdas[c] = s.lam[c];
+  for (int c = 0; c < h->slot_m; c++) {
+    if (hist_x) {
+      int rc = vec_out(h, h->h.hx + (size_t)c * h->n, hist_x + (size_t)c * h->n_caller);
+      if (rc) return rc;
+    }
+    if (hist_g) {
+      int rc = vec_out(h, h->h.hg + (size_t)c * h->n, hist_g + (size_t)c * h->n_caller);
+      if (rc) return rc;
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_set_solver_state(sdft_handle h, const sdft_solver_state* st, const double* hist_x,
+                                     const double* hist_g) {
+  if (!h || !st) return set_err(SDFT_ERR_ARG, "null argument");
+  if (st->anderm < 2 || st->anderm > kMaxAnderson) return set_err(SDFT_ERR_ARG, "anderm must be in [2, 16]");
+  if (st->iter < 0) return set_err(SDFT_ERR_ARG, "negative iteration count");
+  SolveSlot s = fresh_slot();
+  s.iter = st->iter;
+  s.use_picard = st->use_picard ? 1 : 0;
+  s.err = st->err;
+  for (int c = 0; c + 1 < st->anderm; c++) s.lam[c] = st->lambdas[c];
+  // the columns hold stride-NP vectors; the pad point of odd grids stays 0
+  CUDA_TRY(cudaMemsetAsync(h->h.hx, 0, sizeof(double) * (size_t)kMaxAnderson * h->n, h->stream));
+  CUDA_TRY(cudaMemsetAsync(h->h.hg, 0, sizeof(double) * (size_t)kMaxAnderson * h->n, h->stream));
+  for (int c = 0; c < st->anderm; c++) {
+    if (hist_x) {
+      int rc = vec_in(h, h->h.hx + (size_t)c * h->n, hist_x + (size_t)c * h->n_caller);
+      if (rc) return rc;
+    }
+    if (hist_g) {
+      int rc = vec_in(h, h->h.hg + (size_t)c * h->n, hist_g + (size_t)c * h->n_caller);
+      if (rc) return rc;
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->slot = s;
+  h->slot_m = st->anderm;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_anderson_step(sdft_handle h, const sdft_numerics* num, const double* g_mu_ex_K,
+                                  const double* g_lng_K, const double* g_Psi, const double* g_PsiC, double* err) {
+  if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  int rc = validate_numerics(num);
+  if (rc) return rc;
+  if (!g_mu_ex_K || (h->MB && !g_lng_K) || !g_Psi || !g_PsiC) return set_err(SDFT_ERR_ARG, "null G(x) component");
+  if (h->slot_m != 0 && h->slot_m != num->anderm) return set_err(SDFT_ERR_ARG, "anderm differs from the solver state's");
+  const size_t P = h->NP;
+  double* g = h->h.g;
+  const cudaMemcpyKind H2D = cudaMemcpyHostToDevice;
+  CUDA_TRY(rows_copy(h, g, g_mu_ex_K, h->NB, H2D));
+  if (h->MB) CUDA_TRY(rows_copy(h, g + P * h->NB, g_lng_K, 2 * h->MB, H2D));
+  CUDA_TRY(rows_copy(h, g + P * (h->NB + 2 * h->MB), g_Psi, 1, H2D));
+  CUDA_TRY(cudaMemcpyAsync(g + P * (h->NB + 2 * h->MB + 1), g_PsiC, sizeof(double), H2D, h->stream));
+  SolveSlot s = h->slot_m ? h->slot : fresh_slot();
+  s.status = ST_RUNNING;
+  CUDA_TRY(cudaMemcpyAsync(h->dslot, &s, sizeof(SolveSlot), H2D, h->stream));
+  SolveCfg cfg;
+  cfg.max_iters = num->max_iters;
+  cfg.anderm = num->anderm;
+  cfg.damping = num->damping;
+  cfg.mixing_max = num->mixing_max;
+  cfg.switch_tole = num->switch_tole;
+  cfg.tole = num->tole;
+  cfg.mixed_switch = mixed_switch(num);
+  CUDA_TRY(h->h.gen ? launch_anderson_gen(h->dreq, h->dslot, cfg, h->stream)
+                    : launch_anderson_pow2(h->dreq, h->dslot, cfg, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(&s, h->dslot, sizeof(SolveSlot), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->slot = s;
+  h->slot_m = num->anderm;
+  if (err) *err = s.err;
+  if (s.status == ST_NONFINITE) return set_err(SDFT_ERR_NONFINITE, "non-finite fixed-point residual");
+  return SDFT_OK;
 }
 
 extern "C" int sdft_solve_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32_t* iters, double* errs,
@@ -1301,29 +1443,18 @@ extern "C" int sdft_num_species(sdft_handle h, double* num_species) {
 // device arrays.  The array exists on every GPU that loads the library, until
 // the process exits.
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 static __device__ __align__(256) unsigned char sdft_noalloc_scratch[SDFT_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-std::mutex g_noalloc_mu;
-constexpr int kNoAllocMaxDevices = 64;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
-
-// device address of the scratch array on the current device, looked up once per device
+// device address of the scratch array in the current device's context, looked
+// up on every call: a cached address would dangle after cudaDeviceReset (the
+// module, and the array with it, is loaded again at another address)
 int noalloc_scratch_address(void** out) {
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return set_err(SDFT_ERR_CUDA, "device index out of range");
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, sdft_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return set_err(SDFT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_noalloc_addr[dev] = p;
-  }
-  *out = g_noalloc_addr[dev];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, sdft_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return set_err(SDFT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  *out = p;
   return SDFT_OK;
 }
 }  // namespace

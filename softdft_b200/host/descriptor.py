@@ -78,6 +78,18 @@ class Numerics(C.Structure):
     ]
 
 
+class SolverState(C.Structure):
+    """sdft_solver_state: the Anderson driver's state between iterations."""
+    _fields_ = [
+        ("anderm", C.c_int32),
+        ("iter", C.c_int32),
+        ("use_picard", C.c_int32),
+        ("reserved", C.c_int32),
+        ("err", C.c_double),
+        ("lambdas", C.c_double * 15),
+    ]
+
+
 def numerics_from_dict(num: dict) -> Numerics:
     """Defaults of `src/NonlinearSolvers/fixed_point/AndersonMixing.jl:74-79`."""
     return Numerics(

@@ -659,7 +659,14 @@ def eval_bulk_state_native(ms: MolecularSystem, bulk: BulkState) -> None:
     bulk.Xi[:] = xi
 
 
+# False keeps the bulk evaluation in numpy (no shared library loaded), e.g. for
+# a CPU-only process that times the oracle
+USE_NATIVE_BULK = True
+
+
 def _use_native() -> bool:
+    if not USE_NATIVE_BULK:
+        return False
     from .. import native
     return native.library_present()
 

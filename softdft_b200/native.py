@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .host.descriptor import Descriptor, Numerics
+from .host.descriptor import Descriptor, Numerics, SolverState
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsoftdft.so")
@@ -28,7 +28,8 @@ EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_num
            "sdft_num_species", "sdft_solve_batch", "sdft_last_batch_stats", "sdft_server_create",
            "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll", "sdft_bulk_eval",
            "sdft_grid_supported", "sdft_input_from_yaml", "sdft_input_descriptor", "sdft_input_numerics",
-           "sdft_input_bulk_stats", "sdft_input_destroy"]
+           "sdft_input_bulk_stats", "sdft_input_destroy", "sdft_get_solver_state", "sdft_set_solver_state",
+           "sdft_solve_resume", "sdft_anderson_step"]
 
 
 class SdftError(RuntimeError):
@@ -79,6 +80,10 @@ def lib():
         L.sdft_server_submit.argtypes = [vp, vp, C.c_int64]
         L.sdft_server_step.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.sdft_server_poll.argtypes = [vp, vp, vp, vp, vp, vp, C.c_int32, C.POINTER(C.c_int32)]
+        L.sdft_get_solver_state.argtypes = [vp, vp, vp, vp]
+        L.sdft_set_solver_state.argtypes = [vp, vp, vp, vp]
+        L.sdft_solve_resume.argtypes = [vp, vp, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        L.sdft_anderson_step.argtypes = [vp, vp, vp, vp, vp, vp, C.POINTER(C.c_double)]
         _LIB = L
     return _LIB
 
@@ -150,6 +155,42 @@ class DeviceSystem:
         err = C.c_double()
         rc = _check(lib().sdft_solve(self.h, C.byref(num), C.byref(it), C.byref(err)))
         return int(it.value), float(err.value), rc
+
+    def solve_resume(self, num: Numerics):
+        """Continue the solve from the stored solver state (sdft_solve_resume)."""
+        it = C.c_int32()
+        err = C.c_double()
+        rc = _check(lib().sdft_solve_resume(self.h, C.byref(num), C.byref(it), C.byref(err)))
+        return int(it.value), float(err.value), rc
+
+    def solver_state(self):
+        """(SolverState, hist_x, hist_g): the driver's scalars and ring buffers
+        (anderm columns of n unknowns each)."""
+        st = SolverState()
+        _check(lib().sdft_get_solver_state(self.h, C.byref(st), None, None))
+        m = st.anderm
+        hx = np.zeros(max(m, 1) * self.n)
+        hg = np.zeros(max(m, 1) * self.n)
+        _check(lib().sdft_get_solver_state(self.h, C.byref(st), _p(hx), _p(hg)))
+        return st, hx[: m * self.n].reshape(m, self.n), hg[: m * self.n].reshape(m, self.n)
+
+    def set_solver_state(self, st: SolverState, hist_x=None, hist_g=None) -> None:
+        hx = None if hist_x is None else np.ascontiguousarray(hist_x, dtype=np.float64).ravel()
+        hg = None if hist_g is None else np.ascontiguousarray(hist_g, dtype=np.float64).ravel()
+        for a in (hx, hg):
+            if a is not None and a.size != st.anderm * self.n:
+                raise ValueError("history must hold anderm columns of n unknowns")
+        _check(lib().sdft_set_solver_state(self.h, C.byref(st), _p(hx), _p(hg)))
+
+    def anderson_step(self, num: Numerics, g: np.ndarray) -> float:
+        """One driver iteration with the caller's G(x) (sdft_anderson_step);
+        returns the max-norm residual of the iteration."""
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        mu, lng, psi, psic = (np.ascontiguousarray(a) for a in self._split(g))
+        err = C.c_double()
+        _check(lib().sdft_anderson_step(self.h, C.byref(num), _p(mu), _p(lng) if lng.size else None, _p(psi),
+                                        _p(psic), C.byref(err)))
+        return float(err.value)
 
     def densities(self):
         d = self.d

@@ -40,6 +40,8 @@ def _diblock_small():
 
 
 CASES["diblock_small"] = _diblock_small()
+# the benchmarked request: NP = 1024, 20-segment weak polyacid, TPT1 FMT + MSA
+CASES["plain_slit"] = workloads.plain_slit()
 # 200-segment diblock in a 10-sigma slit: renormalised propagators
 CASES["long_diblock"] = workloads.diblock_slit(1024)
 # grid sizes that exercise every FFT pass mix (log2 M = 10, 11, 12, 13: radix-8

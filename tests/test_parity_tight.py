@@ -1,0 +1,249 @@
+"""Plain-form parity of converged states and of single Anderson steps, device
+vs the CPU oracle, through the C ABI.
+
+* Converged states at tole 5e-12 (the FP64 residual floor of these solves lies
+  between 5e-13 and 3e-12, depending on the trajectory).  The bead density
+  profiles, grand potential, chains per species and the degree of
+  dissociation alpha agree to 1e-10 relative.  Segment and bond-end profiles
+  resolve directions of the fixed point that the residual pins only loosely:
+  a small residual pins the fixed point to |(I - J)^-1| times the residual,
+  and changing the map itself by 1e-14 relative (the level at which the
+  device's DCT-space transforms and the oracle's mirrored complex FFTs differ)
+  moves the oracle's own converged segment profiles by up to ~1e-9 on these
+  slits (1.5e-10 on the plain slit, where the device sits 1.6e-10 away).  So
+  segment and bond-end profiles are held to 1e-10, or to ten times the
+  oracle's spread against itself (started from x0 (1 + 1e-15 noise), and solved
+  with G(x) (1 + 1e-14 noise); one random draw each, so the spread is itself a
+  noisy estimate: the device-to-spread ratios measured on B200 range from 0.04
+  to 7.5) where that spread is larger; every figure is printed.
+* Anderson steps from an identical history: the oracle runs the Picard phase,
+  its solver state (ring buffers, warm start, counters) is copied into the
+  device handle, and both take the same driver iteration with the same G(x)
+  (sdft_anderson_step / oracle_anderson_step), so only the arithmetic order of
+  the LSQR sweeps differs.  The ring buffers and the residual come out bit for
+  bit.  The first least-squares problems are nearly singular (|lambda| up to
+  6e7 on the acid slit), so x moves with rounding: the device's step is held to
+  100 times the oracle's own spread when its history is perturbed in the last
+  bit.
+* Checkpoint / resume: a solve stopped, saved and resumed (on the same or on
+  another handle) equals the uninterrupted solve bit for bit.
+"""
+import copy
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleSystem
+from softdft_b200 import native, workloads
+from softdft_b200.api import shape_densities, state_fractions_of
+from softdft_b200.host.descriptor import SolverState, numerics_from_dict
+from tests.helpers import descriptor, rel
+from tests.test_gpu_parity import CASES
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = {
+    "plain_slit": workloads.plain_slit(),
+    "acid_salt": CASES["acid_salt"],
+    "charged_walls": CASES["charged_walls"],
+    "mfmt_msa": CASES["mfmt_msa"],
+    "brush": CASES["brush"],
+    "brush_600": CASES["brush_600"],
+    "brush_999": CASES["brush_999"],
+    "branched_brush": CASES["branched_brush"],
+    "branched_acid_mix5e-4": CASES["branched_acid_mix5e-4"],
+}
+TOL_STATE = 1e-10
+STRICT = ("beads", "omega", "num_species", "alpha")   # held to TOL_STATE
+RESOLVED = ("segments", "bonds")                       # held to max(TOL_STATE, 10 x the oracle's spread)
+
+
+def _tight(ds):
+    ds = copy.deepcopy(ds)
+    ds["numerical"]["tole"] = 5e-12
+    ds["numerical"]["max_iters"] = 10000
+    return ds
+
+
+def _results(dft, sysm):
+    d = dft.descriptor
+    segs, beads, bonds = shape_densities(d, *sysm.densities())
+    return {"segs": segs, "beads": beads, "bonds": bonds, "omega": sysm.grand_potential(),
+            "num": sysm.num_species(), "alpha": state_fractions_of(dft, segs)}
+
+
+def _diffs(a, b):
+    """Relative differences of result dicts a against b (max-norm relative for
+    arrays, |a - b| / |b| for Omega, largest difference for alpha)."""
+    out = {
+        "beads": rel(a["beads"], b["beads"]),
+        "segments": max(rel(x, y) for x, y in zip(a["segs"], b["segs"])),
+        "bonds": rel(a["bonds"], b["bonds"]) if b["bonds"].size else 0.0,
+        "omega": abs(a["omega"] - b["omega"]) / abs(b["omega"]),
+        "num_species": rel(a["num"], b["num"]),
+        "alpha": 0.0,
+    }
+    for sp, y in b["alpha"].items():
+        x = a["alpha"][sp]
+        out["alpha"] = max(out["alpha"], rel(x["avg"], y["avg"]),
+                           max(rel(rx, ry) for (_, rx), (_, ry) in zip(x["segments"], y["segments"])))
+    return out
+
+
+def _oracle_map_perturbed(dft, num, eps):
+    """The oracle's Anderson solve of the map G(x) (1 + eps noise), one driver
+    iteration per oracle_anderson_step."""
+    o = OracleSystem(dft.descriptor)
+    o.set_solver_state(SolverState(anderm=num.anderm, iter=0, use_picard=1, err=1.0))
+    noise = 1.0 + eps * np.random.default_rng(13).standard_normal(o.n)
+    err = np.inf
+    for it in range(num.max_iters):
+        err = o.anderson_step(num, o.objective() * noise)
+        if err < num.tole:
+            break
+    return it + 1, err, 0 if err < num.tole else 1, o
+
+
+@pytest.fixture(scope="module")
+def oracle_tight():
+    """Every case solved on the oracle at tole 5e-12 three times, on parallel
+    host threads (the oracle's C calls release the GIL): as is, from
+    x0 (1 + 1e-15 noise), and with G(x) (1 + 1e-14 noise).  Returns the first
+    solve and the larger spread of the other two against it."""
+    def run(job):
+        name, kind = job
+        ds = _tight(TIGHT[name])
+        dft = descriptor(ds)
+        num = numerics_from_dict(ds["numerical"])
+        if kind == "map":
+            it, err, rc, o = _oracle_map_perturbed(dft, num, 1e-14)
+        else:
+            o = OracleSystem(dft.descriptor)
+            if kind == "x0":
+                x0 = o.get_x()
+                o.set_x(x0 * (1.0 + 1e-15 * np.random.default_rng(11).standard_normal(x0.size)))
+            it, err, rc, _ = o.solve(num)
+        return (name, kind), (it, err, rc, _results(dft, o))
+
+    jobs = [(n, k) for n in sorted(TIGHT) for k in ("plain", "x0", "map")]
+    with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        done = dict(ex.map(run, jobs))
+    out = {}
+    for n in TIGHT:
+        it, err, rc, ro = done[(n, "plain")]
+        spread = {}
+        for k in ("x0", "map"):
+            it2, err2, rc2, ro2 = done[(n, k)]
+            assert rc == 0 and rc2 == 0, (n, k, it, err, it2, err2)
+            for q, v in _diffs(ro2, ro).items():
+                spread[q] = max(spread.get(q, 0.0), v)
+        out[n] = (it, err, rc, ro, spread)
+    return out
+
+
+def _pointwise(a, b, floor=1e-12):
+    """max |a - b| / |b| over the points where |b| > floor * max|b|."""
+    a, b = np.asarray(a).ravel(), np.asarray(b).ravel()
+    m = np.abs(b) > floor * np.max(np.abs(b))
+    return float(np.max(np.abs(a[m] - b[m]) / np.abs(b[m]))) if m.any() else 0.0
+
+
+@pytest.mark.parametrize("name", sorted(TIGHT))
+def test_converged_state_tight(name, oracle_tight):
+    ds = _tight(TIGHT[name])
+    dft = descriptor(ds)
+    g = native.DeviceSystem(dft.descriptor)
+    it_g, err_g, rc_g = g.solve(numerics_from_dict(ds["numerical"]))
+    it_o, err_o, rc_o, ro, spread = oracle_tight[name]
+    assert rc_o == 0 and rc_g == 0, (it_o, err_o, it_g, err_g)
+    rg = _results(dft, g)
+    diffs = _diffs(rg, ro)
+    diffs["beads_pointwise"] = _pointwise(rg["beads"], ro["beads"])
+    print(f"\n{name}: iterations device {it_g} oracle {it_o}\n  device vs oracle: " +
+          ", ".join(f"{k} {v:.2e}" for k, v in diffs.items()) +
+          "\n  oracle spread:    " + ", ".join(f"{k} {v:.2e}" for k, v in spread.items()))
+    for k in STRICT:
+        assert diffs[k] < TOL_STATE, (k, diffs[k])
+    for k in RESOLVED:
+        assert diffs[k] < max(TOL_STATE, 10.0 * spread[k]), (k, diffs[k], spread[k])
+    g.close()
+
+
+def _oracle_after_picard(ds, k):
+    """Oracle after k driver iterations: (oracle, its state, history, x, G(x))."""
+    dft = descriptor(ds)
+    o = OracleSystem(dft.descriptor)
+    o.solve(numerics_from_dict(dict(ds["numerical"], max_iters=k)))
+    st, hx, hg = o.solver_state()
+    x = o.get_x()
+    return dft, o, st, hx, hg, x
+
+
+@pytest.mark.parametrize("name", ["plain_slit", "acid_salt", "brush"])
+def test_anderson_steps_from_identical_history(name):
+    """The first Anderson steps (LSQR on the ring buffers, warm-started) from
+    the oracle's own history and G(x)."""
+    ds = TIGHT[name]
+    m = int(ds["numerical"].get("anderm", 5))
+    num = numerics_from_dict(dict(ds["numerical"], max_iters=100000))
+    dft, o, st, hx, hg, x = _oracle_after_picard(ds, m - 1)
+    assert st.use_picard == 1 and st.iter == m - 1
+    d = native.DeviceSystem(dft.descriptor)
+    rng = np.random.default_rng(3)
+    for step in range(4):
+        g = o.objective()
+        d.set_x(x)
+        d.set_solver_state(st, hx, hg)
+        err_d = d.anderson_step(num, g)
+        # the oracle's spread: the same step from its history perturbed in the last bit
+        o2 = OracleSystem(dft.descriptor)
+        o2.set_x(x)
+        o2.set_solver_state(st, hx, hg * (1.0 + 2.220446049250313e-16 * rng.choice([-1.0, 1.0], hg.shape)))
+        o2.anderson_step(num, g)
+        err_o = o.anderson_step(num, g)
+        assert err_d == err_o
+        st_d, hx_d, hg_d = d.solver_state()
+        st2, _, _ = o2.solver_state()
+        st, hx, hg = o.solver_state()
+        assert st.use_picard == 0 and st_d.use_picard == 0 and st_d.iter == st.iter == m + step
+        assert np.array_equal(hx_d, hx) and np.array_equal(hg_d, hg)
+        x = o.get_x()
+        lam_o, lam_d, lam_2 = (np.array(s_.lambdas[: m - 1]) for s_ in (st, st_d, st2))
+        dx, dx_self = rel(d.get_x(), x), rel(o2.get_x(), x)
+        dl, dl_self = rel(lam_d, lam_o), rel(lam_2, lam_o)
+        print(f"\n{name} step {m + step}: |lambda| {np.max(np.abs(lam_o)):.3e}; device vs oracle: x {dx:.2e}, "
+              f"lambdas {dl:.2e}; oracle vs its last-bit perturbation: x {dx_self:.2e}, lambdas {dl_self:.2e}")
+        assert dx <= 100.0 * dx_self + 1e-13, (dx, dx_self)
+        assert dl <= 100.0 * dl_self + 1e-13, (dl, dl_self)
+        o2.close()
+    d.close()
+
+
+def test_checkpoint_resume_equals_uninterrupted():
+    ds = CASES["acid_salt"]
+    num60 = numerics_from_dict(dict(ds["numerical"], max_iters=60))
+    num25 = numerics_from_dict(dict(ds["numerical"], max_iters=25))
+    dft = descriptor(ds)
+    whole = native.DeviceSystem(dft.descriptor)
+    whole.solve(num60)
+    # the same handle: stop at 25, resume to 60
+    a = native.DeviceSystem(dft.descriptor)
+    it, _, rc = a.solve(num25)
+    assert it == 25 and rc == native.SDFT_MAX_ITERS
+    st, hx, hg = a.solver_state()
+    it, _, _ = a.solve_resume(num60)
+    assert it == 60
+    assert rel(a.get_x(), whole.get_x()) == 0.0
+    # another handle of the same system seeded with the checkpoint
+    b = native.DeviceSystem(dft.descriptor)
+    c = native.DeviceSystem(dft.descriptor)
+    c.solve(num25)
+    x25 = c.get_x()
+    b.set_x(x25)
+    b.set_solver_state(st, hx, hg)
+    it, _, _ = b.solve_resume(num60)
+    assert it == 60
+    assert rel(b.get_x(), whole.get_x()) == 0.0
+    for h in (whole, a, b, c):
+        h.close()
