@@ -57,11 +57,13 @@ def parse():
                     help="profiling case: only batched solves capped at --max-iters, one short line out")
     ap.add_argument("--max-iters", type=int, default=0)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--workload", default="plain", choices=["plain", "uneven"],
                     help="uneven: a seeded batch of slits of different grids and chains in one launch sequence")
     ap.add_argument("--uneven-n", type=int, default=148)
     ap.add_argument("--uneven-np", type=str, default="1024,4096", help="log-uniform grid range (powers of two)")
     ap.add_argument("--uneven-chain", type=str, default="10,60", help="uniform chain-length range")
+    ap.add_argument("--uneven-dump", type=str, default="", help="write per-request status and iterations (JSON)")
     ap.add_argument("--serve-requests", type=int, default=1500)
     ap.add_argument("--serve-rate", type=float, default=100.0, help="offered requests/s of the serving stream")
     ap.add_argument("--serve-iters", type=int, default=25, help="Anderson iterations per server launch")
@@ -337,6 +339,40 @@ def serving_family(n_points: int, seed: int):
     return pts
 
 
+class StreamBackend:
+    """The continuous-batching server fed with prepared requests: each arrival
+    builds its request on the host (sdft_request_prepare: descriptor checks,
+    grid fields, weights), the server places it on the device when free HBM
+    allows, and each completion reads the request's bead densities back and
+    destroys it, returning its memory for the queue."""
+
+    def __init__(self, native, srv, descs):
+        import numpy as np
+
+        self.native, self.srv, self.descs = native, srv, descs
+        self.held = {}
+        self.np = np
+        self.d2h_bytes = 0
+
+    def submit(self, point: int, tag: int):
+        s = self.native.DeviceSystem(self.descs[point], prepare=True)
+        self.held[tag] = s
+        self.srv.submit(s, tag)
+
+    def step(self, iters: int):
+        return self.srv.step(iters)
+
+    def poll(self):
+        out = self.srv.poll()
+        for tag, *_ in out:
+            s = self.held.pop(tag)
+            beads = self.np.zeros(s.d.np_ * s.d.nb)
+            self.native.lib().sdft_get_densities(s.h, None, self.native._p(beads), None)
+            self.d2h_bytes += beads.nbytes
+            s.close()
+        return out
+
+
 def run_serving(native, slots: int, n_requests: int, rate: float, iters_per_step: int, seed: int = 7):
     import numpy as np
 
@@ -355,21 +391,23 @@ def run_serving(native, slots: int, n_requests: int, rate: float, iters_per_step
     dropped = len(pts) - len(kept)
     pts = kept
     rng = np.random.default_rng(seed + 1)
-    pick = rng.integers(0, len(pts), size=n_requests)
-    requests = [native.DeviceSystem(pts[k][1].descriptor) for k in pick]
+    pick = [int(k) for k in rng.integers(0, len(pts), size=n_requests)]
     arrivals = poisson_arrivals(n_requests, rate, seed + 2)
     srv = native.Server(num, max_slots=slots)
-    res = serve_stream(srv, requests, arrivals, iters_per_step)
+    backend = StreamBackend(native, srv, [dft.descriptor for _, dft in pts])
+    res = serve_stream(backend, pick, arrivals, iters_per_step)
     srv.close()
-    for r in requests:
-        r.close()
     ok = int(np.sum(res["status"] == 0))
     return {"requests": n_requests, "converged": ok, "offered_rate": rate, "solves_per_s": res["solves_per_s"],
             "p50_ms": res["p50_ms"], "p99_ms": res["p99_ms"], "slots": slots, "iters_per_step": iters_per_step,
             "launches": res["steps"], "distinct_points": len(pts), "points_left_out": dropped,
             "iterations": {"min": int(res["iters"].min()), "max": int(res["iters"].max()),
                            "mean": float(res["iters"].mean())},
-            "mix": "NP=1024 weak-polyacid slits, pH U(5,9), salt log-U(0.01,0.3) M, N U{10..30}, FP64"}
+            "admission": "by free device memory (requests prepared on the host at arrival, placed at admission, "
+                         "destroyed after their densities are read)",
+            "latency_covers": "host request build, queueing, device placement, solve, density readback",
+            "mix": "NP=1024 weak-polyacid slits, pH U(5,9), salt log-U(0.01,0.3) M, N U{10..30}, FP64; bulk "
+                   "state per distinct point computed once"}
 
 
 def run_uneven(args):
@@ -413,6 +451,11 @@ def run_uneven(args):
                         "frac": alg / (ms / 1000.0) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None},
            "gpu_launches": launches, "clocks": clk}
     print(json.dumps(out), flush=True)
+    if args.uneven_dump:
+        with open(args.uneven_dump, "w") as fh:
+            json.dump({"seed": 3, "np_range": [lo, hi], "chain_range": [nlo, nhi], "n": len(systems),
+                       "status": status.tolist(), "iters": iters.tolist(), "errs": errs.tolist(),
+                       "np": [int(d.NP) for d in dfts]}, fh)
     for s_ in systems:
         s_.close()
 
@@ -434,15 +477,9 @@ def run_ours(args, ws, rank, local):
     check = rank == 0 and ws == 1 and not args.no_cpu_baseline
     tight_ds = copy.deepcopy(ds)
     tight_ds["numerical"].update(tole=5e-12, max_iters=10000)
-    tight = None
-    if check:  # the oracle's 5e-12 solves run on host threads while the device works
-        tight = TightOracle(tight_ds)
-        tight2 = TightOracle(tight_ds, perturb=True)
-        tight.start()
-        tight2.start()
-    import torch
-    sms = torch.cuda.get_device_properties(local if ws > 1 else 0).multi_processor_count
-    B = args.batch if args.batch > 0 else 3 * sms  # the solve kernel keeps three CTAs per SM
+    probe = native.DeviceSystem(dft.descriptor)
+    B = args.batch if args.batch > 0 else probe.resident()  # one wave: resident solve CTAs per SM x SMs
+    probe.close()
     systems = [native.DeviceSystem(dft.descriptor) for _ in range(B)]
     x0 = systems[0].get_x()
     n = x0.size
@@ -506,6 +543,23 @@ def run_ours(args, ws, rank, local):
     if prof and prof.get("workload") == name:
         traffic = prof["dram_bytes_per_request_iteration"] * it_sum / max(launches, 1)
     lat = np.asarray(lat_all)
+    # the same batch in mixed precision (SDFT_PREC_MIXED: FP32 convolutions and
+    # propagator storage in the Anderson phase above the switch, FP64 otherwise)
+    mixed = None
+    if not args.no_mixed:
+        msys = [native.DeviceSystem(dft.descriptor, precision=1) for _ in range(B)]
+        native.solve_batch(msys, num)  # warm-up
+        for s_ in msys:
+            s_.set_x(x0)
+        m_it, _, m_st = native.solve_batch(msys, num)
+        m_ms, _, _ = native.last_batch_stats(B)
+        mixed = {"value": ws * B / (m_ms / 1000.0) if ws == 1 else None, "unit": "solves/s", "ms_per_step": m_ms,
+                 "converged": int(np.sum(m_st == 0)), "iterations": {"min": int(m_it.min()), "max": int(m_it.max())},
+                 "form": "FP32 chain convolutions and propagator storage while the residual is above 1e-2 in the "
+                         "Anderson phase, FP64 otherwise"}
+        for s_ in msys[1:]:
+            s_.close()
+        mixed_probe = msys[0]
     serving = None
     if not args.no_serving:
         serving = run_serving(native, B, args.serve_requests, args.serve_rate, args.serve_iters)
@@ -533,12 +587,23 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if mixed is not None:
+        out["mixed"] = mixed
     if check:
         # the device state of the timed request (tole 1e-8) and a device solve at
-        # tole 5e-12, each against the oracle's state of the same request
+        # tole 5e-12, each against the oracle's state of the same request; the
+        # oracle's 5e-12 solves run on host threads before the timed CPU baseline
+        tight = TightOracle(tight_ds)
+        tight2 = TightOracle(tight_ds, perturb=True)
+        tight.start()
+        tight2.start()
+        tight.join()
+        tight2.join()
         base, ora, it_ora = cpu_baseline(dft, num, args.cpu_threads, keep=True)
         out["cpu_baseline"] = base
         err8 = state_error(dft, systems[0], ora, int(iters_all[-1][0]), it_ora)
+        if mixed is not None:
+            out["mixed"]["oracle_error"] = state_error(dft, mixed_probe, ora, int(m_it[0]), it_ora)
         tdft, tora, tit, trc = (tight.join(), tight.out)[1]
         tdev = native.DeviceSystem(tdft.descriptor)
         tit_dev, _, trc_dev = tdev.solve(numerics_from_dict(tight_ds["numerical"]))
@@ -559,6 +624,8 @@ def run_ours(args, ws, rank, local):
     for s in systems:
         s.close()
     plain.close()
+    if mixed is not None:
+        mixed_probe.close()
 
 
 def main():

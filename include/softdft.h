@@ -129,8 +129,19 @@ void sdft_numerics_default(sdft_numerics* out);
  * (src/iDFT/setup/setup_steps/process_guess.jl:5-54) on the device. */
 int sdft_request_create(const sdft_system_desc* desc, int32_t precision, sdft_handle* out);
 int sdft_request_destroy(sdft_handle h);
+/* A request without device memory yet: the descriptor is validated and the
+ * host tables are built as by sdft_request_create, and the handle keeps them;
+ * the device memory (sdft_request_sizes' device_bytes) is taken when the
+ * request is first used, or by a server when it admits the request.  No
+ * reference counterpart (the reference holds one system per process). */
+int sdft_request_prepare(const sdft_system_desc* desc, int32_t precision, sdft_handle* out);
 /* sizes: n = NP*(NB + 2*MB + 1) + 1 (Anderson vector length) */
 int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* device_bytes);
+/* How many requests of this one's shape (grid, transform buffers) the device
+ * runs at once: resident solve CTAs per SM times the SM count.  A batch or a
+ * server of that many requests fills the GPU in one wave.  No reference
+ * counterpart. */
+int sdft_request_resident(sdft_handle h, int32_t* per_device);
 /* SDFT_OK when the device solve runs a grid of np points, else
  * SDFT_ERR_UNSUPPORTED with the reason in sdft_last_error().  No reference
  * counterpart (FFTW plans any length): the device transform takes np >= 16
@@ -218,7 +229,13 @@ int sdft_last_batch_stats(double* device_ms, int32_t* launches, double* latency_
  *   max_slots requests are active at a time and, when max_bytes > 0, the sum of
  *   their device footprints (sdft_request_sizes) stays within max_bytes.
  * sdft_server_submit: queue a request (it starts from its current state); the
- *   handle must stay alive until its completion has been polled.
+ *   handle must stay alive until its completion has been polled.  A prepared
+ *   request (sdft_request_prepare) is placed on the device only at admission,
+ *   and only while the device's free memory less the server's reserve covers
+ *   it: admission then follows the free HBM.  A finished request keeps its
+ *   device memory until the caller destroys the handle, so a stream driver
+ *   reads each result and destroys the request to make room for the queue.
+ * sdft_server_set_reserve: device bytes that admission leaves free (default 0).
  * sdft_server_step: admit queued requests (first in, first out), run every
  *   active request for at most `iters` Anderson iterations in one launch, retire
  *   the finished ones; returns the counts still active and still queued.
@@ -231,6 +248,7 @@ int sdft_server_submit(sdft_server_t server, sdft_handle h, int64_t tag);
 int sdft_server_step(sdft_server_t server, int32_t iters, int32_t* active, int32_t* queued);
 int sdft_server_poll(sdft_server_t server, int64_t* tags, int32_t* status, int32_t* iters, double* errs,
                      double* device_ms, int32_t max, int32_t* n);
+int sdft_server_set_reserve(sdft_server_t server, int64_t reserve_bytes);
 
 /* ---- bulk (iLST) state evaluation on the host --------------------------------
  * One evaluation of the bulk residual's expensive steps, for the host solve of
@@ -311,7 +329,8 @@ int sdft_input_destroy(sdft_input* in);
  * reserved once at start-up) or because they cannot afford the implicit device
  * synchronisation a cudaMalloc may cause while other work is in flight.
  *  - x_dev, g_dev: the caller's device arrays of n = NP*(NB+2*MB+1)+1 doubles in
- *    the layout of sdft_objective (x read, G(x) written).
+ *    the layout of sdft_objective (x read, G(x) written); g_dev 16-byte aligned
+ *    (as cudaMalloc returns), x_dev 8-byte aligned, else SDFT_ERR_ARG.
  *  - Every other array (grid fields, weights, propagators, densities, spectra)
  *    lives in one static device array of SDFT_NOALLOC_SCRATCH_BYTES that each GPU
  *    loading the library holds until the process exits.  A system whose working

@@ -26,6 +26,80 @@ struct AndersonState {
 // columns j != col of the history, ascending
 __device__ __forceinline__ int hist_col(int c, int col) { return c < col ? c : c + 1; }
 
+// One sweep over q of  w_q = a_q . v + coef * u_q  (a_q[c] = G_hist[j_c][q] - g_k[q]),
+// storing w, and accumulating ||w||^2 (acc[NC]) and A^T w (acc[c]).  Element
+// pairs move as 16-byte loads (every history column starts on a 256-byte
+// boundary; the last element of an odd n is handled alone) and each thread
+// keeps U pairs in flight, every load of a round issued before the first use;
+// the history columns, g_k and u are distinct arrays.
+template <int NC>
+__device__ __forceinline__ void lsqr_pass(const double* __restrict__ gk, const double* const* hc, double* __restrict__ u,
+                                          long long n, int nc, const double* v, double coef, double* acc) {
+  constexpr int U = 2;  // element pairs in flight per thread (more spill at the 128-register cap)
+  const long long n2 = n >> 1;
+  const double2* __restrict__ gk2 = reinterpret_cast<const double2*>(gk);
+  double2* __restrict__ u2 = reinterpret_cast<double2*>(u);
+  const int bd = blockDim.x;
+  for (long long p0 = threadIdx.x; p0 < n2; p0 += U * bd) {
+    double2 g[U], uu[U], h[U][NC];
+    bool on[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const long long pk = p0 + (long long)k * bd;
+      on[k] = pk < n2;
+      if (!on[k]) continue;
+      g[k] = __ldcg(gk2 + pk);
+      uu[k] = __ldcg(u2 + pk);
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        if (c < nc) h[k][c] = __ldcg(reinterpret_cast<const double2*>(hc[c]) + pk);
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      if (!on[k]) continue;
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const double gq = e ? g[k].y : g[k].x;
+        const double uq = e ? uu[k].y : uu[k].x;
+        double aq[NC];
+        double av = 0.0;
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          if (c < nc) {
+            aq[c] = (e ? h[k][c].y : h[k][c].x) - gq;
+            av += aq[c] * v[c];
+          }
+        const double wq = coef * uq + av;
+        if (e) uu[k].y = wq;
+        else uu[k].x = wq;
+        acc[NC] += wq * wq;
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          if (c < nc) acc[c] += aq[c] * wq;
+      }
+      __stcg(u2 + p0 + (long long)k * bd, uu[k]);
+    }
+  }
+  if ((n & 1) && threadIdx.x == 0) {  // the last element of an odd length
+    const long long q = n - 1;
+    const double gq = gk[q];
+    double aq[NC];
+    double av = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) {
+        aq[c] = hc[c][q] - gq;
+        av += aq[c] * v[c];
+      }
+    const double wq = coef * u[q] + av;
+    u[q] = wq;
+    acc[NC] += wq * wq;
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) acc[c] += aq[c] * wq;
+  }
+}
+
 // One sweep over the history serves each LSQR iteration: the next vector
 // w = A v - alpha u is stored unnormalised (u_true = uscale * u_stored) while
 // ||w||^2 and A^T w are accumulated in the same pass; A^T u_{i+1} = A^T w / beta
@@ -34,11 +108,11 @@ __device__ __forceinline__ int hist_col(int c, int col) { return c < col ? c : c
 // compile time so that the per-thread column values stay in registers.
 template <int NC>
 __device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, double* lam, double* red) {
-  const long long n = r.n;
-  const double* gk = r.hg + (size_t)col * n;
+  const long long n = r.n, hs = r.hstride;
+  const double* gk = r.hg + (size_t)col * hs;
   const double* hc[NC];
 #pragma unroll
-  for (int c = 0; c < NC; c++) hc[c] = c < nc ? r.hg + (size_t)hist_col(c, col) * n : gk;
+  for (int c = 0; c < NC; c++) hc[c] = c < nc ? r.hg + (size_t)hist_col(c, col) * hs : gk;
   double* u = r.lsq_u;
   const double eps = 2.220446049250313e-16;
   const double atol = sqrt(eps), btol = sqrt(eps), conlim = 1.0 / sqrt(eps);
@@ -101,23 +175,7 @@ __device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, d
     const double coef = alpha * uscale;
 #pragma unroll
     for (int c = 0; c <= NC; c++) acc[c] = 0.0;
-    for (long long q = threadIdx.x; q < n; q += blockDim.x) {
-      const double gq = gk[q];
-      double aq[NC];
-      double av = 0.0;
-#pragma unroll
-      for (int c = 0; c < NC; c++)
-        if (c < nc) {
-          aq[c] = hc[c][q] - gq;
-          av += aq[c] * v[c];
-        }
-      const double wq = -coef * u[q] + av;
-      u[q] = wq;
-      acc[NC] += wq * wq;
-#pragma unroll
-      for (int c = 0; c < NC; c++)
-        if (c < nc) acc[c] += aq[c] * wq;
-    }
+    lsqr_pass<NC>(gk, hc, u, n, nc, v, -coef, acc);
     block_sum_vec<NC + 1>(acc, NC + 1, red);
     beta = sqrt(acc[NC]);
     if (beta > 0) {
@@ -192,20 +250,95 @@ __device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* 
   else lsqr_sweep_device<kMaxAnderson - 1>(r, nc, col, lam, red);
 }
 
+// x <- X_k + dX lambda + amix (g_k + dG lambda) over element pairs (AndersonMixing.jl:144),
+// the sums over the history columns j != col in ascending order as the reference's
+// matrix-vector products; NC bounds the column count so that the column values stay
+// in registers
+template <int NC>
+__device__ __noinline__ void anderson_mix(const DReq& r, int nc, int col, const double* lam, double amix) {
+  const long long n = r.n, hs = r.hstride, n2 = n >> 1;
+  const double* __restrict__ hxc = r.hx + (size_t)col * hs;
+  const double* __restrict__ hgc = r.hg + (size_t)col * hs;
+  const double* hxj[NC];
+  const double* hgj[NC];
+  double lm[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
+    const int j = c < nc ? hist_col(c, col) : col;
+    hxj[c] = r.hx + (size_t)j * hs;
+    hgj[c] = r.hg + (size_t)j * hs;
+    lm[c] = c < nc ? lam[c] : 0.0;
+  }
+  double* __restrict__ x = r.x;
+  auto mix = [&](double xq, double gq, const double* hxq, const double* hgq) {
+    double sx = 0.0, sg = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) {
+        sx += (hxq[c] - xq) * lm[c];
+        sg += (hgq[c] - gq) * lm[c];
+      }
+    return xq + sx + amix * (gq + sg);
+  };
+  for (long long p = threadIdx.x; p < n2; p += blockDim.x) {
+    const double2 xk = __ldcg(reinterpret_cast<const double2*>(hxc) + p);
+    const double2 gk = __ldcg(reinterpret_cast<const double2*>(hgc) + p);
+    double2 hx2[NC], hg2[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) {
+        hx2[c] = __ldcg(reinterpret_cast<const double2*>(hxj[c]) + p);
+        hg2[c] = __ldcg(reinterpret_cast<const double2*>(hgj[c]) + p);
+      }
+    double ax[NC], ag[NC], bx[NC], bg[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      ax[c] = c < nc ? hx2[c].x : 0.0;
+      ag[c] = c < nc ? hg2[c].x : 0.0;
+      bx[c] = c < nc ? hx2[c].y : 0.0;
+      bg[c] = c < nc ? hg2[c].y : 0.0;
+    }
+    __stcg(reinterpret_cast<double2*>(x) + p, make_double2(mix(xk.x, gk.x, ax, ag), mix(xk.y, gk.y, bx, bg)));
+  }
+  if ((n & 1) && threadIdx.x == 0) {  // the last element of an odd length
+    const long long q = n - 1;
+    double ax[NC], ag[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      ax[c] = c < nc ? hxj[c][q] : 0.0;
+      ag[c] = c < nc ? hgj[c][q] : 0.0;
+    }
+    x[q] = mix(hxc[q], hgc[q], ax, ag);
+  }
+}
+
 // One Anderson update after r.g = G(x).  Returns ST_RUNNING, ST_OK (converged
 // after this update) or ST_NONFINITE.
 __device__ int anderson_step(const DReq& r, const SolveCfg& cfg, int iter, AndersonState& st, double* red,
                              double* err_out) {
-  const long long n = r.n;
+  const long long n = r.n, hs = r.hstride, n2 = n >> 1;
   const int m = cfg.anderm;
   const int col = (iter - 1) % m;
-  double* hxc = r.hx + (size_t)col * n;
-  double* hgc = r.hg + (size_t)col * n;
+  double* __restrict__ hxc = r.hx + (size_t)col * hs;
+  double* __restrict__ hgc = r.hg + (size_t)col * hs;
+  const double* __restrict__ xv = r.x;
+  const double* __restrict__ gv = r.g;
   double mx = 0.0;
   int bad = 0;
-  for (long long q = threadIdx.x; q < n; q += blockDim.x) {
-    const double xq = r.x[q];
-    const double gq = r.g[q] - xq;
+  // ring-buffer column col: x and G(x) - x (AndersonMixing.jl:102-111), element pairs
+  for (long long p = threadIdx.x; p < n2; p += blockDim.x) {
+    const double2 xq = __ldcg(reinterpret_cast<const double2*>(xv) + p);
+    const double2 g2 = __ldcg(reinterpret_cast<const double2*>(gv) + p);
+    const double2 gq = make_double2(g2.x - xq.x, g2.y - xq.y);
+    __stcg(reinterpret_cast<double2*>(hxc) + p, xq);
+    __stcg(reinterpret_cast<double2*>(hgc) + p, gq);
+    const double a0 = fabs(gq.x), a1 = fabs(gq.y);
+    if (!isfinite(a0) || !isfinite(a1)) bad = 1;
+    mx = fmax(mx, fmax(a0, a1));
+  }
+  if ((n & 1) && threadIdx.x == 0) {
+    const long long q = n - 1;
+    const double xq = xv[q], gq = gv[q] - xq;
     hxc[q] = xq;
     hgc[q] = gq;
     const double a = fabs(gq);
@@ -223,21 +356,20 @@ __device__ int anderson_step(const DReq& r, const SolveCfg& cfg, int iter, Ander
   const double amix = fmin(cfg.mixing_max, cfg.damping / err);
   if (iter < m || (err > cfg.switch_tole && st.use_picard)) {
     const double c1 = 1.0 - amix, c2 = amix;
-    for (long long q = threadIdx.x; q < n; q += blockDim.x) r.x[q] = c1 * r.x[q] + c2 * r.g[q];
+    double* __restrict__ x = r.x;
+    for (long long p = threadIdx.x; p < n2; p += blockDim.x) {
+      const double2 xq = __ldcg(reinterpret_cast<const double2*>(x) + p);
+      const double2 gq = __ldcg(reinterpret_cast<const double2*>(gv) + p);
+      __stcg(reinterpret_cast<double2*>(x) + p, make_double2(c1 * xq.x + c2 * gq.x, c1 * xq.y + c2 * gq.y));
+    }
+    if ((n & 1) && threadIdx.x == 0) x[n - 1] = c1 * x[n - 1] + c2 * gv[n - 1];
   } else {
     st.use_picard = 0;
     lsqr_device(r, m, col, st.lam, red);
     const int nc = m - 1;
-    for (long long q = threadIdx.x; q < n; q += blockDim.x) {
-      const double xq = hxc[q], gq = hgc[q];
-      double sx = 0.0, sg = 0.0;
-      for (int c = 0; c < nc; c++) {
-        const int j = hist_col(c, col);
-        sx += (r.hx[(size_t)j * n + q] - xq) * st.lam[c];
-        sg += (r.hg[(size_t)j * n + q] - gq) * st.lam[c];
-      }
-      r.x[q] = xq + sx + amix * (gq + sg);
-    }
+    if (nc <= 4) anderson_mix<4>(r, nc, col, st.lam, amix);
+    else if (nc <= 9) anderson_mix<9>(r, nc, col, st.lam, amix);
+    else anderson_mix<kMaxAnderson - 1>(r, nc, col, st.lam, amix);
   }
   __syncthreads();
   return err < cfg.tole ? ST_OK : ST_RUNNING;

@@ -15,12 +15,15 @@
 
 namespace sdft {
 
-constexpr int kThreads = 256;        // CTA size of the solve kernels
+#ifndef SDFT_THREADS
+#define SDFT_THREADS 256
+#endif
+constexpr int kThreads = SDFT_THREADS;  // CTA size of the solve kernels
 constexpr int kMaxStates = 4;        // per-segment state families the device supports
 constexpr int kMaxBeads = 32;        // bead types
 constexpr int kMaxBonds = 64;        // bond types
 constexpr int kMaxAnderson = 16;     // Anderson depth m
-constexpr int kMaxTB = 4;            // transforms in flight per CTA
+constexpr int kMaxTB = 8;            // transforms in flight per CTA
 constexpr int kMaxRadices = 24;      // stages of a general-length FFT
 constexpr int kMaxGenRadix = 61;     // largest prime factor of a general-length FFT
 constexpr double kPi = 3.14159265358979323846;
@@ -82,6 +85,7 @@ struct DReq {
   int prec;           // 0: FP64; 1: FP32 propagators while the residual is above the switch
   double dz, lB, total_charge;
   long long n;        // Anderson unknowns
+  long long hstride;  // column stride of the Anderson histories: n rounded up to 32 (256-byte columns)
   // per-bead / per-bond constants
   const double* sig;  // [NB]
   const double* z;    // [NB]
@@ -206,6 +210,26 @@ __device__ __forceinline__ double block_max(double v, double* red) {
   return t;
 }
 
+// the maxima of two values over the CTA (one barrier pair)
+__device__ __forceinline__ void block_max2(double* a, double* b, double* red) {
+  double x = warp_max(*a), y = warp_max(*b);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    red[w] = x;
+    red[32 + w] = y;
+  }
+  __syncthreads();
+  x = red[0];
+  y = red[32];
+  for (int i = 1; i < nw; i++) {
+    x = fmax(x, red[i]);
+    y = fmax(y, red[32 + i]);
+  }
+  *a = x;
+  *b = y;
+}
+
 // k sums at once (k <= 16): vals[k] in/out
 template <int KMAX>
 __device__ __forceinline__ void block_sum_vec(double* vals, int k, double* red) {
@@ -242,6 +266,14 @@ struct SolveSlot {       // per-request solver state kept across launches
 };
 
 constexpr int kRedDoubles = 1024;              // reduction scratch ahead of the transform buffers
+// Occupancy target of the solve kernel: CTAs resident per SM.  It sets the
+// register cap (65536 / (256 CTAs)) through __launch_bounds__ and the shared
+// memory each CTA may use for transform buffers (an SM holds 228 KB).
+#ifndef SDFT_SOLVE_CTAS
+#define SDFT_SOLVE_CTAS 2
+#endif
+constexpr int kSolveCtasPerSm = SDFT_SOLVE_CTAS;
+constexpr size_t kTransformBudget = kSolveCtasPerSm >= 3 ? 64 * 1024 : 96 * 1024;
 constexpr size_t kMaxSmemBytes = 227 * 1024;   // dynamic shared memory a CTA may opt into
 
 // ---- kernel launches ----
@@ -254,6 +286,8 @@ cudaError_t launch_solve_pow2(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, 
                               cudaStream_t s);
 cudaError_t launch_omega_pow2(const DReq* reqs, double* out, size_t smem, cudaStream_t s);
 cudaError_t launch_anderson_pow2(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, cudaStream_t s);
+cudaError_t occupancy_solve_pow2(size_t smem, int* ctas_per_sm);
+cudaError_t occupancy_solve_gen(size_t smem, int* ctas_per_sm);
 cudaError_t launch_anderson_gen(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, cudaStream_t s);
 cudaError_t launch_objective_gen(const DReq* reqs, int n, size_t smem, cudaStream_t s);
 cudaError_t launch_solve_gen(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, int max_chunk, int n, size_t smem,

@@ -156,6 +156,10 @@ __device__ __forceinline__ void store_b(const FftCtx& c, int nT, double scale, S
 __device__ __forceinline__ double2 ldcg2(const double* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
 __device__ __forceinline__ void stcg2(double* p, double2 v) { __stcg(reinterpret_cast<double2*>(p), v); }
 __device__ __forceinline__ float2 ldcg2(const float* p) { return __ldcg(reinterpret_cast<const float2*>(p)); }
+// L1-cached pair loads (ld.global.ca) for arrays that one CTA reads repeatedly
+// after writing them earlier in the same kernel: the SM's L1 sees its own writes
+__device__ __forceinline__ double2 ldca2(const double* p) { return __ldca(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ float2 ldca2(const float* p) { return __ldca(reinterpret_cast<const float2*>(p)); }
 __device__ __forceinline__ void stcg2(float* p, float2 v) { __stcg(reinterpret_cast<float2*>(p), v); }
 
 template <bool G, class C, class V>
@@ -1022,6 +1026,227 @@ __device__ __forceinline__ void dct2_convolve_b2(const FftCtxT<C>& c, int nT, F2
     }
   }
   dct2_convolve_b2_impl<(SDFT_FFT_GEN != 0)>(c, nT, f2, wgt, pre2, put2);
+}
+
+// ---- grid-pair-major convolution driver (even P) ------------------------------
+// The same convolution of nT transforms, with load and store phases organised
+// by grid-point pair instead of by transform: loadkp(kp, put) issues every load
+// that pair kp needs for all nT transforms before it calls put(t, (f_K, f_K+1));
+// storekp(kp, get) receives get(t) = (y_K, y_K+1) for every transform.  A
+// thread owns the same pairs in both phases, so whatever the store phase keeps
+// per pair (a running maximum, sums over transforms) needs no exchange, and the
+// loads of all nT transforms are in flight together.
+template <bool GEN, class C, class LK, class W, class SK>
+__device__ __forceinline__ void dct2_convolve_kpair_impl(const FftCtxT<C>& c, int nT, LK loadkp, W wgt, SK storekp) {
+  using R = typename Cx<C>::R;
+  const int P = c.P, M = c.M, H = c.H;
+  __syncthreads();
+  for (int kp = threadIdx.x; kp < M; kp += blockDim.x)
+    loadkp(kp, [&](int t, double2 v) { put_pair<GEN>(c, t, kp, v); });
+  fft_fwd_b(c, nT);
+  SDFT_PAIR_LOOP(c, nT)
+  if (k == 0) {
+    const C dM = __ldg(&c.twD[M]);
+    R c0, cM;
+    zero_forward(zb[0], dM, &c0, &cM);
+    zb[0] = zero_inverse(c0 * (R)wgt(t, 0), cM * (R)wgt(t, M), dM);
+    if (!(M & 1)) {
+      const C dh = __ldg(&c.twD[H]);
+      R ch, cPh;
+      mid_forward(zb[fpad(H)], dh, &ch, &cPh);
+      zb[fpad(H)] = mid_inverse(ch * (R)wgt(t, H), cPh * (R)wgt(t, P - H), dh);
+    }
+  } else {
+    const R w0 = (R)wgt(t, k), w1 = (R)wgt(t, P - k), w2 = (R)wgt(t, M - k), w3 = (R)wgt(t, M + k);
+    const C wk = __ldg(&c.twP[k]), dk = __ldg(&c.twD[k]), dk2 = __ldg(&c.twD[M - k]);
+    QuadT<R> q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], wk, dk, dk2);
+    q.c0 *= w0;
+    q.c1 *= w1;
+    q.c2 *= w2;
+    q.c3 *= w3;
+    C a, b;
+    pair_inverse(q, wk, dk, dk2, &a, &b);
+    zb[fpad(k)] = a;
+    zb[fpad(M - k)] = b;
+  }
+}
+fft_inv_b(c, nT);
+const R scale = (R)1 / (R)M;
+for (int kp = threadIdx.x; kp < M; kp += blockDim.x)
+  storekp(kp, [&](int t) {
+    C y = get_pair<GEN>(c, t, kp);
+    y.x *= scale;
+    y.y *= scale;
+    return y;
+  });
+__syncthreads();
+}
+
+template <class C, class LK, class W, class SK>
+__device__ __forceinline__ void dct2_convolve_kpair(const FftCtxT<C>& c, int nT, LK loadkp, W wgt, SK storekp) {
+  dct2_convolve_kpair_impl<(SDFT_FFT_GEN != 0)>(c, nT, loadkp, wgt, storekp);
+}
+
+// ---- grid-pair-major forward and inverse transforms (any P) -------------------
+// The batched forward DCT-II and inverse DCT-II with the grid-side phase
+// organised by grid-point pair, as dct2_convolve_kpair: loadkp(kp, put) calls
+// put(t, (f_K, f_K+1)) for every transform t, storekp(kp, get) reads
+// get(t) = (y_K, y_K+1).  Pairs run over kp < ceil(P/2); on an odd grid the last
+// pair's second sample is the pad point beyond the grid (read by loadkp, never
+// transformed, given as 0 by get).  The coefficient side keeps the per-index
+// functors of dct2_forward_b / dct2_inverse_b.
+template <bool GEN, class LK>
+__device__ __forceinline__ void load_kpair(const FftCtx& c, int nT, LK loadkp) {
+  if (GEN && (c.P & 1)) {  // odd P: transforms 2b, 2b+1 are the real and imaginary parts of buffer b
+    const int np = (c.P + 1) >> 1;
+    for (int kp = threadIdx.x; kp < np; kp += blockDim.x) {
+      const bool two = 2 * kp + 1 < c.P;
+      const int s0 = fslot<true>(c, kp), s1 = two ? fslot<true>(c, c.P - 1 - kp) : 0;
+      loadkp(kp, [&](int t, double2 v) {
+        odd_part(c, t, s0) = v.x;
+        if (two) odd_part(c, t, s1) = v.y;
+      });
+      if (nT & 1) {  // a lone last transform has a zero partner
+        odd_part(c, nT, s0) = 0.0;
+        if (two) odd_part(c, nT, s1) = 0.0;
+      }
+    }
+    return;
+  }
+  for (int kp = threadIdx.x; kp < c.M; kp += blockDim.x)
+    loadkp(kp, [&](int t, double2 v) { put_pair<GEN>(c, t, kp, v); });
+}
+
+template <bool GEN, class SK>
+__device__ __forceinline__ void store_kpair(const FftCtx& c, double scale, SK storekp) {
+  if (GEN && (c.P & 1)) {
+    const int np = (c.P + 1) >> 1;
+    for (int kp = threadIdx.x; kp < np; kp += blockDim.x) {
+      const bool two = 2 * kp + 1 < c.P;
+      const int s0 = fslot<true>(c, kp), s1 = two ? fslot<true>(c, c.P - 1 - kp) : 0;
+      storekp(kp, [&](int t) {
+        return make_double2(odd_part(c, t, s0) * scale, two ? odd_part(c, t, s1) * scale : 0.0);
+      });
+    }
+    return;
+  }
+  for (int kp = threadIdx.x; kp < c.M; kp += blockDim.x)
+    storekp(kp, [&](int t) {
+      double2 y = get_pair<GEN>(c, t, kp);
+      y.x *= scale;
+      y.y *= scale;
+      return y;
+    });
+}
+
+// C[q] for q in [0, P): forward DCT-II; emit(t, q, C[q]) as dct2_forward_b
+template <class LK, class E>
+__device__ __forceinline__ void dct2_forward_kp(const FftCtx& c, int nT, LK loadkp, E emit) {
+  constexpr bool GEN = SDFT_FFT_GEN != 0;
+  const int P = c.P, M = c.M, H = c.H;
+  __syncthreads();
+  load_kpair<GEN>(c, nT, loadkp);
+  if (GEN && (P & 1)) {
+    const int cnt = (P + 1) >> 1, nb = (nT + 1) >> 1;
+    fft_fwd_b(c, nb);
+    for (int it = threadIdx.x; it < nb * cnt; it += blockDim.x) {
+      const int b = it / cnt, k = it - b * cnt, t0 = 2 * b, t1 = t0 + 1;
+      const double2* zb = c.z + (size_t)b * c.stride;
+      if (k == 0) {
+        emit(t0, 0, zb[0].x);
+        if (t1 < nT) emit(t1, 0, zb[0].y);
+      } else {
+        double2 V0, V1;
+        odd_unpack(zb[fpad(k)], zb[fpad(P - k)], &V0, &V1);
+        const double2 dk = __ldg(&c.twD[k]), dpk = __ldg(&c.twD[P - k]);
+        double ck, cpk;
+        odd_forward(V0, dk, dpk, &ck, &cpk);
+        emit(t0, k, ck);
+        emit(t0, P - k, cpk);
+        if (t1 < nT) {
+          odd_forward(V1, dk, dpk, &ck, &cpk);
+          emit(t1, k, ck);
+          emit(t1, P - k, cpk);
+        }
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  fft_fwd_b(c, nT);
+  const int lH = c.L - 1, cnt = (M + 1) >> 1;
+  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
+    const int t = item_t<GEN>(it, cnt, lH), k = it - t * cnt;
+    const double2* zb = c.z + (size_t)t * c.stride;
+    if (k == 0) {
+      double c0, cM;
+      zero_forward(zb[0], __ldg(&c.twD[M]), &c0, &cM);
+      emit(t, 0, c0);
+      emit(t, M, cM);
+      if (!(M & 1)) {
+        double ch, cPh;
+        mid_forward(zb[fpad(H)], __ldg(&c.twD[H]), &ch, &cPh);
+        emit(t, H, ch);
+        emit(t, P - H, cPh);
+      }
+    } else {
+      Quad q = pair_forward(zb[fpad(k)], zb[fpad(M - k)], __ldg(&c.twP[k]), __ldg(&c.twD[k]), __ldg(&c.twD[M - k]));
+      emit(t, k, q.c0);
+      emit(t, P - k, q.c1);
+      emit(t, M - k, q.c2);
+      emit(t, M + k, q.c3);
+    }
+  }
+  __syncthreads();
+}
+
+// y_t = iDCT2(E_t), E_t[q] = get(t, q) as dct2_inverse_b; pair-major store
+template <class G, class SK>
+__device__ __forceinline__ void dct2_inverse_kp(const FftCtx& c, int nT, G get, SK storekp) {
+  constexpr bool GEN = SDFT_FFT_GEN != 0;
+  const int P = c.P, M = c.M, H = c.H;
+  __syncthreads();
+  if (GEN && (P & 1)) {
+    const int cnt = (P + 1) >> 1, nb = (nT + 1) >> 1;
+    for (int it = threadIdx.x; it < nb * cnt; it += blockDim.x) {
+      const int b = it / cnt, k = it - b * cnt, t0 = 2 * b, t1 = t0 + 1;
+      double2* zb = c.z + (size_t)b * c.stride;
+      if (k == 0) {
+        zb[0] = make_double2(get(t0, 0), t1 < nT ? get(t1, 0) : 0.0);
+      } else {
+        const double2 dk = __ldg(&c.twD[k]);
+        const double2 W0 = odd_inverse(get(t0, k), get(t0, P - k), dk);
+        const double2 W1 = t1 < nT ? odd_inverse(get(t1, k), get(t1, P - k), dk) : make_double2(0.0, 0.0);
+        odd_pack(W0, W1, &zb[fpad(k)], &zb[fpad(P - k)]);
+      }
+    }
+    fft_inv_b(c, nb);
+    store_kpair<GEN>(c, 1.0 / (double)P, storekp);
+    __syncthreads();
+    return;
+  }
+  const int lH = c.L - 1, cnt = (M + 1) >> 1;
+  for (int it = threadIdx.x; it < nT * cnt; it += blockDim.x) {
+    const int t = item_t<GEN>(it, cnt, lH), k = it - t * cnt;
+    double2* zb = c.z + (size_t)t * c.stride;
+    if (k == 0) {
+      zb[0] = zero_inverse(get(t, 0), get(t, M), __ldg(&c.twD[M]));
+      if (!(M & 1)) zb[fpad(H)] = mid_inverse(get(t, H), get(t, P - H), __ldg(&c.twD[H]));
+    } else {
+      Quad e;
+      e.c0 = get(t, k);
+      e.c1 = get(t, P - k);
+      e.c2 = get(t, M - k);
+      e.c3 = get(t, M + k);
+      double2 a, b;
+      pair_inverse(e, __ldg(&c.twP[k]), __ldg(&c.twD[k]), __ldg(&c.twD[M - k]), &a, &b);
+      zb[fpad(k)] = a;
+      zb[fpad(M - k)] = b;
+    }
+  }
+  fft_inv_b(c, nT);
+  store_kpair<GEN>(c, 1.0 / (double)M, storekp);
+  __syncthreads();
 }
 
 #undef SDFT_PAIR_LOOP

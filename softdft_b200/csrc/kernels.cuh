@@ -53,7 +53,7 @@ extern "C" __global__ void __launch_bounds__(kThreads) SDFT_KNAME(sdft_k_objecti
   if (threadIdx.x == 0) *r.status = ok ? ST_OK : ST_NORM;
 }
 
-extern "C" __global__ void __launch_bounds__(kThreads, 3)
+extern "C" __global__ void __launch_bounds__(kThreads, kSolveCtasPerSm)
     SDFT_KNAME(sdft_k_solve)(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, int max_chunk) {
   extern __shared__ double smem[];
   const DReq& r = reqs[blockIdx.x];
@@ -69,8 +69,10 @@ extern "C" __global__ void __launch_bounds__(kThreads, 3)
   double err = sl->err;
   for (int step = 0; step < max_chunk && iter < cfg.max_iters; step++) {
     iter++;
-    // mixed precision: FP32 propagators while the residual is above the switch
-    if (!objective(r, sh, r.prec == 1 && err > cfg.mixed_switch)) {
+    // mixed precision: FP32 propagators once the driver has left its Picard
+    // phase (the first least-squares history is built from FP64 evaluations)
+    // and while the residual is above the switch
+    if (!objective(r, sh, r.prec == 1 && !st.use_picard && err > cfg.mixed_switch)) {
       status = ST_NORM;
       break;
     }
@@ -145,6 +147,12 @@ cudaError_t SDFT_KLAUNCH(launch_solve)(const DReq* reqs, SolveSlot* slots, Solve
   if (e != cudaSuccess) return e;
   SDFT_KNAME(sdft_k_solve)<<<n, kThreads, smem, s>>>(reqs, slots, cfg, max_chunk);
   return cudaGetLastError();
+}
+
+cudaError_t SDFT_KLAUNCH(occupancy_solve)(size_t smem, int* ctas_per_sm) {
+  cudaError_t e = allow_smem((const void*)SDFT_KNAME(sdft_k_solve), smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, SDFT_KNAME(sdft_k_solve), kThreads, smem);
 }
 
 cudaError_t SDFT_KLAUNCH(launch_anderson)(const DReq* reqs, SolveSlot* slots, SolveCfg cfg, cudaStream_t s) {

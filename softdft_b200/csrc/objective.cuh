@@ -64,10 +64,13 @@ __device__ void stage_lambda(const DReq& r) {
 //          convolution towards the bead at this end, child_propagators.jl:118-133)
 //   Fout = e^{lng_{b,e}/2}                          (the output factor at this end)
 // computed once per evaluation instead of once per (segment, state pair).
-// In an FP32 evaluation the input factors are also written as floats, all
-// divided by one power of two 2^sc that brings their maximum below 1 (e^{-lambda}
-// can exceed the float range far from the solution); sc goes to scal[1] and
-// every convolution step adds it to the carried propagator exponent.
+// In an FP32 evaluation the factors are also written as floats, the input
+// factors divided by one power of two 2^sc and the output factors by one 2^so
+// that bring their maxima below 1 (e^{-lambda} and e^{lng/2} can exceed the
+// float range far from the solution); sc and so go to scal[1] and scal[2], and
+// every FP32 convolution step adds sc + so to the carried propagator exponent
+// (its outputs are the true propagators times 2^-(sc+so); the grafted
+// segment's local sums are shifted to match).
 __device__ void stage_bond_factors(const DReq& r, Shared sh, bool fp32) {
   const int P = r.NP, nbe = 2 * r.MB;
   const double* lng = xs_lng(r, r.x);
@@ -81,16 +84,26 @@ __device__ void stage_bond_factors(const DReq& r, Shared sh, bool fp32) {
     r.fbe[(size_t)nbe * P + idx] = exp(l / 2.0);
     if (K < grid_points(r) && isfinite(fin)) mx = fmax(mx, fin);
   }
+  double mo = 0.0;  // largest output factor e^{lng/2}
+  for (int idx = threadIdx.x; idx < nbe * P; idx += blockDim.x) {
+    const int K = idx - (idx / P) * P;
+    const double fo = r.fbe[(size_t)nbe * P + idx];
+    if (K < grid_points(r) && isfinite(fo)) mo = fmax(mo, fo);
+  }
   for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) r.elam[idx] = exp(-r.lambda[idx]);
   if (fp32 && r.fbe32) {
-    mx = block_max(mx, sh.red);
-    int sc = 0;
+    block_max2(&mx, &mo, sh.red);
+    int sc = 0, so = 0;
     if (mx > 0.0) frexp(mx, &sc);
+    if (mo > 0.0) frexp(mo, &so);
     for (int idx = threadIdx.x; idx < nbe * P; idx += blockDim.x) {
       r.fbe32[idx] = (float)ldexp(r.fbe[idx], -sc);
-      r.fbe32[(size_t)nbe * P + idx] = (float)r.fbe[(size_t)nbe * P + idx];
+      r.fbe32[(size_t)nbe * P + idx] = (float)ldexp(r.fbe[(size_t)nbe * P + idx], -so);
     }
-    if (threadIdx.x == 0) r.scal[1] = (double)sc;
+    if (threadIdx.x == 0) {
+      r.scal[1] = (double)sc;
+      r.scal[2] = (double)so;
+    }
   }
   __syncthreads();
 }
@@ -148,8 +161,8 @@ template <class R>
 __device__ bool chain_child(const DReq& r, const DSpecies& s, Shared sh) {
   const int P = r.NP, S = s.S, N = s.n_seg;
   double* const gC = s.gC;
-  // FP32: the input factors are stored divided by 2^sc (stage_bond_factors)
-  const int sc = sizeof(R) == 4 ? (int)r.scal[1] : 0;
+  // FP32: the factors are stored divided by 2^sc (inputs) and 2^so (outputs), stage_bond_factors
+  const int sc = sizeof(R) == 4 ? (int)r.scal[1] + (int)r.scal[2] : 0;
   bool scaled = false;
   int e_child = 0;  // exponent carried by gC of segment p + 1 (the leaf carries none)
   const double* lng = xs_lng(r, r.x);
@@ -264,8 +277,8 @@ template <class R>
 __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
   const int P = r.NP, S = s.S, N = s.n_seg;
   double* const gP = s.gP;
-  // FP32: the input factors are stored divided by 2^sc (stage_bond_factors)
-  const int sc = sizeof(R) == 4 ? (int)r.scal[1] : 0;
+  // FP32: the factors are stored divided by 2^sc (inputs) and 2^so (outputs), stage_bond_factors
+  const int sc = sizeof(R) == 4 ? (int)r.scal[1] + (int)r.scal[2] : 0;
   bool scaled = false;
   int e_parent = 0;  // exponent carried by gP of segment c - 1 (the root carries none)
   if (threadIdx.x == 0) s.expo[N] = 0;
@@ -373,6 +386,273 @@ __device__ bool chain_parent(const DReq& r, const DSpecies& s, Shared sh) {
     e_parent += e + sc;
     scaled |= (e + sc) != 0;
     if (threadIdx.x == 0) s.expo[N + c] = e_parent;
+  }
+  __syncthreads();
+  return scaled;
+}
+
+// ---------------------------------------------------------------------------
+// Both recursions of a linear chain in one loop (even grids).  The child
+// recursion (child_propagators.jl:118-141) runs from the leaf to the root and
+// the parent recursion (parent_propagators.jl:96-122) from the root to the leaf;
+// neither reads the other, so step t computes gC of segment p = N-2-t and gP of
+// segment c = t+1 together: up to 2 S^2 transforms share each FFT pass, and a
+// chain of N segments takes N-1 steps of passes instead of 2(N-1).  The
+// arithmetic per entry is that of chain_child / chain_parent: input
+// Fin * sum_q g[prev][j][q], the filtered bond-kernel convolution, output
+// |y| Fout / normative, the max-distance mask of grafted species, the grafted
+// segment's local sums, and per-segment power-of-two renormalisation with the
+// same exponent bookkeeping (expo[p] child, expo[N + c] parent).
+// ---------------------------------------------------------------------------
+struct FuseT {             // one transform of a fused chain step (shared memory)
+  const void* fin;         // input bond-end factor (R)
+  const void* fout;        // output bond-end factor (R)
+  const void* src;         // S slots of the previous segment's propagator (R), summed; nullptr: the base case 1
+  const double* w;         // filtered bond kernel in C-space
+  void* out;               // propagator slot written (R)
+  int sweep;               // 0: child recursion, 1: parent recursion
+  int pad;
+};
+constexpr int kFuseOffset = 64;  // FuseT table position in Shared::red (doubles), after the reduction slots
+
+// exponent of the power of two that brings mx into [0.5, 1) when mx leaves
+// [2^-400, 2^400] ([2^-30, 2^30] for FP32 propagator convolutions); else 0
+__device__ __forceinline__ int renorm_exponent(double mx, bool fp32_bounds) {
+  const double lo = fp32_bounds ? 0x1p-30 : 0x1p-400, hi = fp32_bounds ? 0x1p30 : 0x1p400;
+  if (!(mx > 0.0) || !isfinite(mx)) return 0;
+  if (mx >= lo && mx <= hi) return 0;
+  int e;
+  frexp(mx, &e);
+  return e;
+}
+
+template <class T>
+__device__ void rescale_segment(T* a, int count_per_K, int P, int e) {
+  for (int K = threadIdx.x; K < P; K += blockDim.x)
+    for (int q = 0; q < count_per_K; q++) a[(size_t)q * P + K] = (T)ldexp((double)a[(size_t)q * P + K], -e);
+}
+
+template <class R, int SM>
+__device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
+  using R2 = decltype(ldcg2((const R*)nullptr));
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  // propagators are stored in the precision of the step (FP32 in a mixed evaluation)
+  R* const gC = reinterpret_cast<R*>(s.gC);
+  R* const gP = reinterpret_cast<R*>(s.gP);
+  // FP32: the factors are stored divided by 2^sc (inputs) and 2^so (outputs), stage_bond_factors
+  const int sc = sizeof(R) == 4 ? (int)r.scal[1] + (int)r.scal[2] : 0;
+  const bool fp32 = sizeof(R) == 4;
+  const double* lng = xs_lng(r, r.x);
+  const double inv_norm = 1.0 / s.normative;
+  const R* fin = bond_factors(r, (R*)nullptr);
+  const R* fout = fin + (size_t)2 * r.MB * P;
+  FuseT* fd = reinterpret_cast<FuseT*>(sh.red + kFuseOffset);
+  const auto fc = fft_ctx<R>(sh.z, r);
+  bool scaled = false;
+  int eC = 0, eP = 0;  // exponents carried by gC of segment p + 1 and gP of segment c - 1
+  // root base case of the parent recursion: gP[0][i][0] = 1 (only at the graft point when fixed)
+  for (int K = threadIdx.x; K < P; K += blockDim.x)
+    for (int ii = 0; ii < S; ii++)
+      for (int jj = 0; jj < S; jj++)
+        gP[((size_t)ii * S + jj) * P + K] =
+            (R)((jj == 0 && ii < s.nst[0] && (s.fixed < 0 || K == s.fixed)) ? 1.0 : 0.0);
+  if (threadIdx.x == 0) {
+    s.expo[N - 1] = 0;
+    s.expo[N] = 0;
+  }
+  for (int t = 0; t < N - 1; t++) {
+    const int p = N - 2 - t, c = p + 1;  // child recursion: gC[p] from gC[c]
+    const int c2 = t + 1, p2 = t;        // parent recursion: gP[c2] from gP[p2]
+    const bool child_local = p == 0 && s.fixed >= 0;
+    const bool parent_local = p2 == 0 && s.fixed >= 0;
+    const int ncC = s.nst[c], npP = s.nst[p2];
+    const int nC = child_local ? 0 : s.nst[p] * ncC;
+    const int nP = parent_local ? 0 : s.nst[c2] * npP;
+    const int nT = nC + nP;
+    __syncthreads();  // the previous step's table and outputs are complete
+    if (threadIdx.x < nT) {
+      FuseT d;
+      const int q = threadIdx.x;
+      if (q < nC) {  // child pair (ii of p, jj of c)
+        const int ii = q / ncC, jj = q - ii * ncC;
+        const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
+        const int bond = s.bnd[(p * S + ii) * S + jj];
+        const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+        d.fin = fin + (size_t)(bond * 2 + pair_j) * P;
+        d.fout = fout + (size_t)(bond * 2 + pair_i) * P;
+        d.src = c < N - 1 ? gC + ((size_t)(c * S + jj) * S) * P : nullptr;
+        d.w = r.Wbond + (size_t)bond * P;
+        d.out = gC + ((size_t)(p * S + ii) * S + jj) * P;
+        d.sweep = 0;
+      } else {  // parent pair (ii of c2, jj of p2)
+        const int qq = q - nC, ii = qq / npP, jj = qq - ii * npP;
+        const int si = s.states[c2 * S + ii], sj = s.states[p2 * S + jj];
+        const int bond = s.bnd[(p2 * S + jj) * S + ii];
+        const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+        d.fin = fin + (size_t)(bond * 2 + pair_j) * P;
+        d.fout = fout + (size_t)(bond * 2 + pair_i) * P;
+        d.src = gP + ((size_t)(p2 * S + jj) * S) * P;
+        d.w = r.Wbond + (size_t)bond * P;
+        d.out = gP + ((size_t)(c2 * S + ii) * S + jj) * P;
+        d.sweep = 1;
+      }
+      d.pad = 0;
+      fd[q] = d;
+    }
+    double mxC = 0.0, mxP = 0.0;  // largest output of each recursion at this step (this thread)
+    // grafted segment 0 as the child's parent: local sums within sigma_ij (child_propagators.jl:91-116)
+    if (child_local) {
+      const int Kp = s.fixed;
+      for (int pi = 0; pi < s.nst[p] * ncC; pi++) {
+        const int ii = pi / ncC, jj = pi - ii * ncC;
+        const int si = s.states[p * S + ii], sj = s.states[c * S + jj];
+        const int bond = s.bnd[(p * S + ii) * S + jj];
+        const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+        const double* lam_j = r.lambda + (size_t)sj * P;
+        const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
+        const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
+        const double* tr_j = r.trapez + (size_t)sj * P;
+        const R* gcc = (c < N - 1) ? gC + ((size_t)(c * S + jj) * S) * P : nullptr;
+        const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
+        const double Dij2 = Dij * Dij;
+        const double renorm = 2.0 * Dij;
+        const double el = exp(lng_pi[Kp] / 2.0);
+        double acc = 0.0;
+        for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+          const double d2 = dist2_grid(K1, Kp, r.dz);
+          if (d2 <= Dij2) {
+            double f = exp(-lam_j[K1] + lng_pj[K1] / 2.0);
+            if (gcc) {
+              double tq = 0.0;
+              for (int q = 0; q < S; q++) tq += (double)gcc[(size_t)q * P + K1];
+              f *= tq;
+            }
+            double v = fabs(f) * el * r.dz * tr_j[K1] / renorm;
+            if (fabs(d2 - Dij2) <= 1e-6) v /= 2.0;
+            acc += v / s.normative;
+          }
+        }
+        acc = block_sum(acc, sh.red);
+        if (sc) acc = ldexp(acc, -sc);
+        R* out = gC + ((size_t)(p * S + ii) * S + jj) * P;
+        // the max-distance mask of segment 0 keeps only the graft point
+        const double md2 = s.md[p] * s.md[p];
+        for (int K = threadIdx.x; K < P; K += blockDim.x)
+          out[K] = (R)((K == Kp && dist2_grid(K, Kp, r.dz) <= md2) ? acc : 0.0);
+        mxC = fmax(mxC, fabs(acc));
+      }
+    }
+    // grafted segment 0 as the parent: local writes within sigma_ij (parent_propagators.jl:72-94)
+    if (parent_local) {
+      const int Kp = s.fixed;
+      for (int pi = 0; pi < s.nst[c2] * npP; pi++) {
+        const int ii = pi / npP, jj = pi - ii * npP;
+        const int si = s.states[c2 * S + ii], sj = s.states[p2 * S + jj];
+        const int bond = s.bnd[(p2 * S + jj) * S + ii];
+        const int pair_i = si <= sj ? 0 : 1, pair_j = 1 - pair_i;
+        const double* lng_pj = lng + (size_t)(bond * 2 + pair_j) * P;
+        const double* lng_pi = lng + (size_t)(bond * 2 + pair_i) * P;
+        const R* gpp = gP + ((size_t)(p2 * S + jj) * S) * P;
+        const double Dij = (r.sig[si] + r.sig[sj]) / 2.0;
+        const double Dij2 = Dij * Dij;
+        const double renorm = 2.0 * Dij;
+        double tq = 0.0;
+        for (int q = 0; q < S; q++) tq += (double)gpp[(size_t)q * P + Kp];
+        const double f = exp(-r.lambda[(size_t)sj * P + Kp] + lng_pj[Kp] / 2.0) * tq;
+        const double md2 = s.md[c2] * s.md[c2];
+        const double base = jj == 0 ? 1.0 : 0.0;  // the base case left where no bond reaches
+        R* out = gP + ((size_t)(c2 * S + ii) * S + jj) * P;
+        for (int K1 = threadIdx.x; K1 < P; K1 += blockDim.x) {
+          const double d2 = dist2_grid(K1, Kp, r.dz);
+          double v = base;
+          if (d2 <= Dij2) {
+            v = fabs(f) * exp(lng_pi[K1] / 2.0) / renorm / s.normative;
+            if (fabs(d2 - Dij2) <= 1e-6) v /= 2.0;
+            if (sc) v = ldexp(v, -sc);
+          }
+          if (d2 > md2) v = 0.0;
+          out[K1] = (R)v;
+          mxP = fmax(mxP, fabs(v));
+        }
+      }
+    }
+    // the convolutions of both recursions, TB transforms per pass set
+    const double mdC = s.fixed >= 0 ? s.md[p] * s.md[p] : 0.0;
+    const double mdP = s.fixed >= 0 ? s.md[c2] * s.md[c2] : 0.0;
+    for (int g0 = 0; g0 < nT; g0 += r.TB) {
+      const int nb = min(r.TB, nT - g0);
+      dct2_convolve_kpair(
+          fc, nb,
+          [&](int kp, auto put) {
+            const int K = 2 * kp;
+            double2 f[kMaxTB];
+#pragma unroll
+            for (int u = 0; u < kMaxTB; u++)
+              if (u < nb) {
+                const FuseT& d = fd[g0 + u];
+                // the bond-end factors repeat across the two recursions and the
+                // steps of a chain: L1-cached loads
+                const R2 fv = ldca2(reinterpret_cast<const R*>(d.fin) + K);
+                f[u] = make_double2((double)fv.x, (double)fv.y);
+                if (d.src) {
+                  double2 q2 = make_double2(0.0, 0.0);
+#pragma unroll
+                  for (int q = 0; q < SM; q++)
+                    if (q < S) {
+                      const R2 v = ldcg2(reinterpret_cast<const R*>(d.src) + (size_t)q * P + K);
+                      q2.x += v.x;
+                      q2.y += v.y;
+                    }
+                  f[u].x *= q2.x;
+                  f[u].y *= q2.y;
+                }
+              }
+#pragma unroll
+            for (int u = 0; u < kMaxTB; u++)
+              if (u < nb) put(u, f[u]);
+          },
+          [&](int u, int q) { return __ldg(&fd[g0 + u].w[q]); },
+          [&](int kp, auto get) {
+            const int K = 2 * kp;
+            R2 fo[kMaxTB];
+#pragma unroll
+            for (int u = 0; u < kMaxTB; u++)
+              if (u < nb) fo[u] = ldca2(reinterpret_cast<const R*>(fd[g0 + u].fout) + K);
+            const bool cut = s.fixed >= 0;
+#pragma unroll
+            for (int u = 0; u < kMaxTB; u++)
+              if (u < nb) {
+                const FuseT& d = fd[g0 + u];
+                const auto y = get(u);
+                double2 v = make_double2(fabs((double)y.x) * (double)fo[u].x * inv_norm,
+                                         fabs((double)y.y) * (double)fo[u].y * inv_norm);
+                if (cut) {  // max-distance mask (child_propagators.jl:147-157)
+                  const double md2 = d.sweep ? mdP : mdC;
+                  if (dist2_grid(K, s.fixed, r.dz) > md2) v.x = 0.0;
+                  if (dist2_grid(K + 1, s.fixed, r.dz) > md2) v.y = 0.0;
+                }
+                R2 st;
+                st.x = (R)v.x;
+                st.y = (R)v.y;
+                stcg2(reinterpret_cast<R*>(d.out) + K, st);
+                const double m = fmax(fabs(v.x), fabs(v.y));
+                if (d.sweep) mxP = fmax(mxP, m);
+                else mxC = fmax(mxC, m);
+              }
+          });
+    }
+    // per-segment renormalisation of both new segments
+    block_max2(&mxC, &mxP, sh.red);
+    const int ec = renorm_exponent(mxC, fp32), ep = renorm_exponent(mxP, fp32);
+    if (ec) rescale_segment(gC + (size_t)p * S * S * P, S * S, P, ec);
+    if (ep) rescale_segment(gP + (size_t)c2 * S * S * P, S * S, P, ep);
+    eC += ec + sc;
+    eP += ep + sc;
+    scaled |= (ec + sc) != 0 || (ep + sc) != 0;
+    if (threadIdx.x == 0) {
+      s.expo[p] = eC;
+      s.expo[N + c2] = eP;
+    }
   }
   __syncthreads();
   return scaled;
@@ -815,6 +1095,217 @@ __device__ __noinline__ void accumulate_pairs(const DReq& r, const DSpecies& s, 
   __syncthreads();
 }
 
+// accumulate_pairs with its two loops merged: at step (g, ii) the segment
+// density, the bond end 0 of segment g and the bond end 1 of segment g (as the
+// child c = g of the second loop) read the same e^{-lambda}, gP and gC slots, so
+// one pass over the (segment, state) steps serves all three, and each thread
+// carries KP grid-point pairs through the steps together, the loads of the next
+// step issued before the current one is combined.  Every sum runs in the order
+// of accumulate_pairs (a0 and ab over (g, ii), a1 over (c, ii) with c >= 1).
+template <int BR, int ER, class R, int KP>
+__device__ __noinline__ void accumulate_merged(const DReq& r, const DSpecies& s, double norm, bool scaled) {
+  const int P = r.NP, S = s.S, N = s.n_seg;
+  const double pref = norm * exp(s.mu_species);
+  const R* __restrict__ gP = reinterpret_cast<const R*>(s.gP);
+  const R* __restrict__ gC = reinterpret_cast<const R*>(s.gC);
+  const double* __restrict__ elam = r.elam;
+  const int* __restrict__ states = s.states;
+  const int* __restrict__ nst = s.nst;
+  const int* __restrict__ bslot = s.bslot;
+  const int* __restrict__ eslot = s.eslot;
+  auto seg_pref = [&](int g, double* lp, bool* direct) {
+    if (!scaled) {
+      *lp = 0.0;
+      *direct = false;
+      return pref;
+    }
+    *lp = log_prefactor(s, norm, g);
+    *direct = fabs(*lp) > 600.0;
+    return exp(*lp);
+  };
+  const int bd = blockDim.x;
+  for (int kp0 = threadIdx.x; kp0 < P / 2; kp0 += KP * bd) {
+    int Ks[KP];
+    bool on[KP];
+#pragma unroll
+    for (int v = 0; v < KP; v++) {
+      Ks[v] = 2 * (kp0 + v * bd);
+      on[v] = Ks[v] < P;
+    }
+    double2 a0[KP][BR], a1[KP][BR], ab[KP][ER];
+#pragma unroll
+    for (int v = 0; v < KP; v++) {
+#pragma unroll
+      for (int q = 0; q < BR; q++) a0[v][q] = a1[v][q] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < ER; q++) ab[v][q] = make_double2(0.0, 0.0);
+    }
+    auto load = [&](int g, int ii, AccStep* d) {
+      const int si = states[g * S + ii];
+#pragma unroll
+      for (int v = 0; v < KP; v++) {
+        if (!on[v]) continue;
+        const int K = Ks[v];
+        d[v].el = ldcg2(elam + (size_t)si * P + K);
+        if (N > 1) {
+          d[v].p0 = to_d2(ldcg2(gP + ((size_t)(g * S + ii) * S) * P + K));
+          if (S > 1) d[v].p1 = to_d2(ldcg2(gP + ((size_t)(g * S + ii) * S + 1) * P + K));
+        }
+        if (g < N - 1) {
+          d[v].c0 = to_d2(ldcg2(gC + ((size_t)(g * S + ii) * S) * P + K));
+          if (S > 1) d[v].c1 = to_d2(ldcg2(gC + ((size_t)(g * S + ii) * S + 1) * P + K));
+        }
+      }
+    };
+    AccStep cur[KP], nxt[KP];
+    int g = 0, ii = 0;
+    load(0, 0, cur);
+    while (g < N) {
+      int g2 = g, ii2 = ii + 1;
+      if (ii2 == nst[g2]) {
+        g2++;
+        ii2 = 0;
+      }
+      if (g2 < N) load(g2, ii2, nxt);
+      double lp;
+      bool direct;
+      const double elp = seg_pref(g, &lp, &direct);
+      const int si = states[g * S + ii];
+      const int nn = g < N - 1 ? nst[g + 1] : 0;
+      const int b0 = nn > 0 ? bslot[(g * S + ii) * S] : -1;
+      const int b1 = nn > 1 ? bslot[(g * S + ii) * S + 1] : -1;
+      const int e = eslot[g * S + ii];
+      const int np_ = g > 0 ? nst[g - 1] : 0;
+      const int c0s = g > 0 ? bslot[((g - 1) * S) * S + ii] : -1;
+      const int c1s = np_ > 1 ? bslot[((g - 1) * S + 1) * S + ii] : -1;
+#pragma unroll
+      for (int v = 0; v < KP; v++) {
+        if (!on[v]) continue;
+        const int K = Ks[v];
+        const AccStep& d = cur[v];
+        // segment density and bond end 0 (the first loop of accumulate_pairs)
+        double2 sp;
+        if (N > 1) {
+          sp.x = 0.0 + d.p0.x;
+          sp.y = 0.0 + d.p0.y;
+          if (S > 1) {
+            sp.x += d.p1.x;
+            sp.y += d.p1.y;
+          }
+        } else {
+          sp.x = (s.fixed < 0 || K == s.fixed) ? 1.0 : 0.0;
+          sp.y = (s.fixed < 0 || K + 1 == s.fixed) ? 1.0 : 0.0;
+        }
+        double2 base;  // the prefactor times e^{-lambda} at K, K+1
+        if (direct) {
+          base.x = exp(lp - r.lambda[(size_t)si * P + K]);
+          base.y = exp(lp - r.lambda[(size_t)si * P + K + 1]);
+        } else {
+          base.x = elp * d.el.x;
+          base.y = elp * d.el.y;
+        }
+        const double2 contr = direct ? make_double2(base.x * sp.x, base.y * sp.y)
+                                     : make_double2(elp * d.el.x * sp.x, elp * d.el.y * sp.y);
+        double2 temp;
+        if (nn) {
+          temp = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int q = 0; q < BR; q++)
+            if (q == b0) {
+              a0[v][q].x += contr.x * d.c0.x;
+              a0[v][q].y += contr.y * d.c0.y;
+            }
+          temp.x += d.c0.x;
+          temp.y += d.c0.y;
+          if (nn > 1) {
+#pragma unroll
+            for (int q = 0; q < BR; q++)
+              if (q == b1) {
+                a0[v][q].x += contr.x * d.c1.x;
+                a0[v][q].y += contr.y * d.c1.y;
+              }
+            temp.x += d.c1.x;
+            temp.y += d.c1.y;
+          }
+        } else {
+          temp = make_double2(1.0, 1.0);
+        }
+        const double2 val = make_double2(contr.x * temp.x, contr.y * temp.y);
+        stcg2(s.rho_seg + (size_t)(g * S + ii) * P + K, val);
+        if (g == 0 && s.fixed >= 0) {
+#pragma unroll
+          for (int q = 0; q < ER; q++)
+            if (q == e) {
+              if (K == s.fixed) ab[v][q].x += val.x / r.dz / r.trapez[(size_t)si * P + K];
+              if (K + 1 == s.fixed) ab[v][q].y += val.y / r.dz / r.trapez[(size_t)si * P + K + 1];
+            }
+        } else {
+#pragma unroll
+          for (int q = 0; q < ER; q++)
+            if (q == e) {
+              ab[v][q].x += val.x;
+              ab[v][q].y += val.y;
+            }
+        }
+        // bond end 1 of segment g as the child (the second loop of accumulate_pairs)
+        if (g >= 1) {
+          double2 c1v = base;
+          if (g < N - 1) {
+            double2 t = make_double2(0.0 + d.c0.x, 0.0 + d.c0.y);
+            if (S > 1) {
+              t.x += d.c1.x;
+              t.y += d.c1.y;
+            }
+            c1v.x *= t.x;
+            c1v.y *= t.y;
+          }
+#pragma unroll
+          for (int q = 0; q < BR; q++)
+            if (q == c0s) {
+              a1[v][q].x += c1v.x * d.p0.x;
+              a1[v][q].y += c1v.y * d.p0.y;
+            }
+          if (np_ > 1) {
+#pragma unroll
+            for (int q = 0; q < BR; q++)
+              if (q == c1s) {
+                a1[v][q].x += c1v.x * d.p1.x;
+                a1[v][q].y += c1v.y * d.p1.y;
+              }
+          }
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < KP; v++) cur[v] = nxt[v];
+      g = g2;
+      ii = ii2;
+    }
+#pragma unroll
+    for (int v = 0; v < KP; v++) {
+      if (!on[v]) continue;
+      const int K = Ks[v];
+#pragma unroll
+      for (int q = 0; q < BR; q++)
+        if (q < s.nbslot) {
+          const int b = s.bslot_bond[q];
+          double* r0 = r.rho_bonds + (size_t)(b * 2 + 0) * P + K;
+          double* r1 = r.rho_bonds + (size_t)(b * 2 + 1) * P + K;
+          const double2 o0 = ldcg2(r0), o1 = ldcg2(r1);
+          stcg2(r0, make_double2(o0.x + a0[v][q].x, o0.y + a0[v][q].y));
+          stcg2(r1, make_double2(o1.x + a1[v][q].x, o1.y + a1[v][q].y));
+        }
+#pragma unroll
+      for (int q = 0; q < ER; q++)
+        if (q < s.neslot) {
+          double* rb = r.rho_beads + (size_t)s.eslot_bead[q] * P + K;
+          const double2 o = ldcg2(rb);
+          stcg2(rb, make_double2(o.x + ab[v][q].x, o.y + ab[v][q].y));
+        }
+    }
+  }
+  __syncthreads();
+}
+
 // accumulate_densities! for long grids, segment-outer: each (segment, state)
 // step streams its slices over the grid on point pairs, two pairs per round
 // with every load of the round issued first, and adds into rho_bonds /
@@ -992,11 +1483,11 @@ __device__ __forceinline__ bool accumulate_fast(const DReq& r, const DSpecies& s
     return true;
   }
   if (s.S <= 2 && s.nbslot <= 4 && s.neslot <= 2) {
-    accumulate_pairs<4, 2, R>(r, s, norm, scaled);
+    accumulate_merged<4, 2, R, 1>(r, s, norm, scaled);
     return true;
   }
   if (s.S <= 2 && s.nbslot <= 4 && s.neslot <= 4) {
-    accumulate_pairs<4, 4, R>(r, s, norm, scaled);
+    accumulate_merged<4, 4, R, 1>(r, s, norm, scaled);
     return true;
   }
   if (s.nbslot <= 4 && s.neslot <= 4) {
@@ -1332,11 +1823,18 @@ __device__ __noinline__ bool stage_densities(const DReq& r, Shared sh, int* bad_
       continue;
     }
     if (s.n_seg > 1) {
-      scaled |= chain_child<R>(r, s, sh);
-      scaled |= chain_parent<R>(r, s, sh);
+      if (grid_points(r) == P) {  // even grids: both recursions in one loop
+        scaled |= s.S <= 2 ? chain_sweeps<R, 2>(r, s, sh) : chain_sweeps<R, kMaxStates>(r, s, sh);
+      } else {
+        scaled |= chain_child<R>(r, s, sh);
+        scaled |= chain_parent<R>(r, s, sh);
+      }
     }
+    // the even-grid fused sweep stores the propagators in the precision of the
+    // step (FP32 in a mixed evaluation); the odd-grid recursions in FP64
+    const bool f32 = sizeof(R) == 4 && s.n_seg > 1 && grid_points(r) == P;
     double norm;
-    bool ok = chain_norm<double>(r, s, sh, &norm);
+    bool ok = f32 ? chain_norm<float>(r, s, sh, &norm) : chain_norm<double>(r, s, sh, &norm);
     if (!ok) {
       *bad_species = u;
       return false;
@@ -1348,8 +1846,12 @@ __device__ __noinline__ bool stage_densities(const DReq& r, Shared sh, int* bad_
     }
     // the reference's prefactor norm e^{mu - lambda} overflows beyond e^709
     if (fabs(s.mu_species) + (double)(s.n_seg - 1) * fabs(log(s.normative)) > 600.0) scaled = true;
-    if (accumulate_fast<double>(r, s, norm, scaled)) fast_mask |= 1u << u;
-    else chain_accumulate<double>(r, s, norm, scaled);
+    if (f32 ? accumulate_fast<float>(r, s, norm, scaled) : accumulate_fast<double>(r, s, norm, scaled))
+      fast_mask |= 1u << u;
+    else if (f32)
+      chain_accumulate<float>(r, s, norm, scaled);
+    else
+      chain_accumulate<double>(r, s, norm, scaled);
   }
   // update_spatial_structures! for the species accumulated without register slots
   if (fast_mask != (1u << r.NS) - 1u) {
@@ -1381,28 +1883,30 @@ __device__ void stage_rho_hat(const DReq& r, Shared sh) {
   const int P = r.NP;
   const FftCtx fc = make_fft(sh.z, r);
   const int ntot = r.NB + 2 * r.MB;
+  // transform q: bead densities (q < NB) or bond-end densities, times the trapezoid weight of their bead
+  auto rho_of = [&](int q) { return q < r.NB ? r.rho_beads + (size_t)q * P : r.rho_bonds + (size_t)(q - r.NB) * P; };
+  auto tr_of = [&](int q) { return r.trapez + (size_t)(q < r.NB ? q : r.bonds[q - r.NB]) * P; };
   for (int g0 = 0; g0 < ntot; g0 += r.TB) {
     const int nT = min(r.TB, ntot - g0);
-    const double* rho_t[kMaxTB];
-    const double* tr_t[kMaxTB];
-    double* C_t[kMaxTB];
-    for (int t = 0; t < nT; t++) {
-      const int q = g0 + t;
-      if (q < r.NB) {
-        rho_t[t] = r.rho_beads + (size_t)q * P;
-        tr_t[t] = r.trapez + (size_t)q * P;
-        C_t[t] = r.Cb + (size_t)q * P;
-      } else {
-        const int be = q - r.NB;  // bond * 2 + end
-        const int bead = r.bonds[be];
-        rho_t[t] = r.rho_bonds + (size_t)be * P;
-        tr_t[t] = r.trapez + (size_t)bead * P;
-        C_t[t] = r.Cbond + (size_t)be * P;
-      }
-    }
-    dct2_forward_b(
-        fc, nT, [&](int t, int K) { return rho_t[t][K] * tr_t[t][K]; },
-        [&](int t, int q, double v) { C_t[t][q] = v; });
+    dct2_forward_kp(
+        fc, nT,
+        [&](int kp, auto put) {
+          const int K = 2 * kp;
+          double2 a[kMaxTB], b[kMaxTB];
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) {
+              a[u] = ldcg2(rho_of(g0 + u) + K);
+              b[u] = ldcg2(tr_of(g0 + u) + K);
+            }
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) put(u, make_double2(a[u].x * b[u].x, a[u].y * b[u].y));
+        },
+        [&](int t, int q, double v) {
+          const int w = g0 + t;
+          (w < r.NB ? r.Cb + (size_t)w * P : r.Cbond + (size_t)(w - r.NB) * P)[q] = v;
+        });
   }
 }
 
@@ -1444,13 +1948,21 @@ __device__ void fmt_weighted(const DReq& r, Shared sh, bool tpt1) {
   const int ns = 2 * NB;  // (bead j, weight m) -> wd[(2j+m) P]
   for (int g0 = 0; g0 < ns; g0 += r.TB) {
     const int nT = min(r.TB, ns - g0);
-    dct2_inverse_b(
+    dct2_inverse_kp(
         fc, nT,
         [&](int t, int q) {
           const int jm = g0 + t, j = jm >> 1, m = jm & 1;
           return r.Cb[(size_t)j * P + q] * r.Wfmt[((size_t)j * 3 + m) * P + q];
         },
-        [&](int t, int K, double y) { r.wd[(size_t)(g0 + t) * P + K] = fabs(y); });
+        [&](int kp, auto get) {
+          const int K = 2 * kp;
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) {
+              const double2 y = get(u);
+              stcg2(r.wd + (size_t)(g0 + u) * P + K, make_double2(fabs(y.x), fabs(y.y)));
+            }
+        });
   }
   for (int K = threadIdx.x; K < P; K += blockDim.x) {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
@@ -1470,7 +1982,7 @@ __device__ void fmt_weighted(const DReq& r, Shared sh, bool tpt1) {
   // vector weighted densities: odd output of the odd weight; the bead sum is linear
   for (int g0 = 0; g0 < 2; g0 += r.TB) {
     const int nT = min(r.TB, 2 - g0);
-    dct2_inverse_b(
+    dct2_inverse_kp(
         fc, nT,
         [&](int t, int q) {
           if (q == 0) return 0.0;
@@ -1482,20 +1994,36 @@ __device__ void fmt_weighted(const DReq& r, Shared sh, bool tpt1) {
           }
           return s;
         },
-        [&](int t, int K, double y) { (g0 + t == 0 ? nV1 : nV2)[K] = (K & 1) ? y : -y; });
+        [&](int kp, auto get) {
+          const int K = 2 * kp;  // (K even, K + 1 odd): the odd output takes (-y_K, y_K+1)
+#pragma unroll
+          for (int u = 0; u < 2; u++)
+            if (u < nT) {
+              const double2 y = get(u);
+              stcg2((g0 + u == 0 ? nV1 : nV2) + K, make_double2(-y.x, y.y));
+            }
+        });
   }
   // bond weighted densities (TPT1mfmt.jl:106-133)
   if (tpt1) {
     const int nb2 = 2 * MB;
     for (int g0 = 0; g0 < nb2; g0 += r.TB) {
       const int nT = min(r.TB, nb2 - g0);
-      dct2_inverse_b(
+      dct2_inverse_kp(
           fc, nT,
           [&](int t, int q) {
             const int be = g0 + t, i = r.bonds[be];
             return r.Cbond[(size_t)be * P + q] * r.Wfmt[((size_t)i * 3 + 0) * P + q] / (r.sig[i] * r.sig[i]) / kPi;
           },
-          [&](int t, int K, double y) { r.wb[(size_t)(g0 + t) * P + K] = fabs(y); });
+          [&](int kp, auto get) {
+            const int K = 2 * kp;
+#pragma unroll
+            for (int u = 0; u < kMaxTB; u++)
+              if (u < nT) {
+                const double2 y = get(u);
+                stcg2(r.wb + (size_t)(g0 + u) * P + K, make_double2(fabs(y.x), fabs(y.y)));
+              }
+          });
     }
   }
 }
@@ -1561,12 +2089,17 @@ __device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
   }
   for (int g0 = 0; g0 < 6; g0 += r.TB) {
     const int nT = min(r.TB, 6 - g0);
-    dct2_forward_b(
+    dct2_forward_kp(
         fc, nT,
-        [&](int t, int K) {
-          const int q = g0 + t;
-          const double v = D[(size_t)q * P + K];
-          return (q >= 4 && (K & 1)) ? -v : v;
+        [&](int kp, auto put) {
+          const int K = 2 * kp;
+          double2 v[kMaxTB];
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) v[u] = ldcg2(D + (size_t)(g0 + u) * P + K);
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) put(u, g0 + u >= 4 ? make_double2(v[u].x, -v[u].y) : v[u]);  // odd weights: (-1)^K
         },
         [&](int t, int k, double v) {
           const int q = g0 + t;
@@ -1591,8 +2124,18 @@ __device__ void stage_fmt(const DReq& r, Shared sh, bool tpt1) {
   if (tpt1) {
     for (int g0 = 0; g0 < MB; g0 += r.TB) {
       const int nT = min(r.TB, MB - g0);
-      dct2_forward_b(
-          fc, nT, [&](int t, int K) { return lny[(size_t)(g0 + t) * P + K]; },
+      dct2_forward_kp(
+          fc, nT,
+          [&](int kp, auto put) {
+            const int K = 2 * kp;
+            double2 v[kMaxTB];
+#pragma unroll
+            for (int u = 0; u < kMaxTB; u++)
+              if (u < nT) v[u] = ldcg2(lny + (size_t)(g0 + u) * P + K);
+#pragma unroll
+            for (int u = 0; u < kMaxTB; u++)
+              if (u < nT) put(u, v[u]);
+          },
           [&](int t, int k, double c) {
             const int u = g0 + t;
             const int ia = r.bonds[2 * u], ib = r.bonds[2 * u + 1];
@@ -1754,7 +2297,7 @@ __device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
   const int ntot = NB + (tpt1 ? 2 * MB : 0);
   for (int g0 = 0; g0 < ntot; g0 += r.TB) {
     const int nT = min(r.TB, ntot - g0);
-    dct2_inverse_b(
+    dct2_inverse_kp(
         fc, nT,
         [&](int t, int q) {
           const int w = g0 + t;
@@ -1762,10 +2305,15 @@ __device__ void msa_weighted(const DReq& r, Shared sh, bool tpt1) {
           const int be = w - NB;
           return r.Cbond[(size_t)be * P + q] * r.Wmsa[(size_t)r.bonds[be] * P + q];
         },
-        [&](int t, int K, double y) {
-          const int w = g0 + t;
-          if (w < NB) r.wa[(size_t)w * P + K] = fabs(y);
-          else r.wb[(size_t)(w - NB) * P + K] = fabs(y);
+        [&](int kp, auto get) {
+          const int K = 2 * kp;
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) {
+              const int w = g0 + u;
+              const double2 y = get(u);
+              stcg2((w < NB ? r.wa + (size_t)w * P : r.wb + (size_t)(w - NB) * P) + K, make_double2(fabs(y.x), fabs(y.y)));
+            }
         });
   }
 }
@@ -1868,21 +2416,27 @@ __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
   msa_weighted(r, sh, tpt1);
   __syncthreads();
   msa_gamma_pass(r, r.wd);  // wd is free between the FMT stage and the next evaluation
-  // point-wise derivative (TPT1msa.jl:129-156 -> iLST TPT1msa.jl:200-282)
+  // point-wise derivative (TPT1msa.jl:129-156 -> iLST TPT1msa.jl:200-282).  The
+  // per-bead denominators 1 + G sigma_j, their reciprocals and the per-bond
+  // sums of the bond weighted densities are formed once per point; every use
+  // below is the same expression as before, so the values are unchanged.
   const double* sig = r.sig;
   const double* Z = r.z;
   const double lB = r.lB;
   for (int K = threadIdx.x; K < P; K += blockDim.x) {
-    double rho[kMaxBeads], dphi[kMaxBeads];
+    double rho[kMaxBeads], dphi[kMaxBeads], og[kMaxBeads], inv[kMaxBeads];
     for (int j = 0; j < NB; j++) rho[j] = r.wa[(size_t)j * P + K];
     const double G = r.wd[K], eta = r.wd[(size_t)P + K], H = r.wd[(size_t)2 * P + K];
+    for (int j = 0; j < NB; j++) {
+      og[j] = 1.0 + G * sig[j];
+      inv[j] = 1.0 / og[j];
+    }
     double us = 0.0;
-    for (int j = 0; j < NB; j++)
-      us += rho[j] * sig[j] * sig[j] * ((Z[j] - eta * sig[j] * sig[j]) / (1.0 + G * sig[j]) + Z[j]);
+    for (int j = 0; j < NB; j++) us += rho[j] * sig[j] * sig[j] * ((Z[j] - eta * sig[j] * sig[j]) / og[j] + Z[j]);
     us = -kPi / 6 * us;
     for (int j = 0; j < NB; j++)
-      dphi[j] = -lB * (G * (Z[j] * Z[j]) / (1.0 + G * sig[j]) +
-                       eta * sig[j] * ((2.0 * Z[j] - eta * (sig[j] * sig[j])) / (1.0 + G * sig[j]) + eta * (sig[j] * sig[j]) / 3.0) +
+      dphi[j] = -lB * (G * (Z[j] * Z[j]) / og[j] +
+                       eta * sig[j] * ((2.0 * Z[j] - eta * (sig[j] * sig[j])) / og[j] + eta * (sig[j] * sig[j]) / 3.0) +
                        Z[j] * us);
     if (tpt1) {
       double* lngo = r.wc + (size_t)NB * P;
@@ -1895,18 +2449,17 @@ __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
         for (int u = 0; u < MB; u++) {
           const int i = r.bonds[2 * u], j = r.bonds[2 * u + 1];
           const double sij = (sig[i] + sig[j]) / 2.0;
-          const double Xi = (Z[i] - eta * (sig[i] * sig[i])) / (1.0 + G * sig[i]);
-          const double Xj = (Z[j] - eta * (sig[j] * sig[j])) / (1.0 + G * sig[j]);
+          const double Xi = (Z[i] - eta * (sig[i] * sig[i])) / og[i];
+          const double Xj = (Z[j] - eta * (sig[j] * sig[j])) / og[j];
           lngo[(size_t)u * P + K] = -lB / sij * Xi * Xj;
         }
         double dfG = 0.0, dfe = 0.0, deG = 0.0, dHG = 0.0;
         for (int w = 0; w < NB; w++) {
           const double a = Z[w] - eta * sig[w] * sig[w];
-          const double og = 1.0 + G * sig[w];
-          dfG += rho[w] * sig[w] * a * a / og / og / og;
-          dfe += rho[w] * sig[w] * sig[w] * a / og / og;
-          deG += rho[w] * Z[w] * sig[w] * sig[w] / og / og;
-          dHG += rho[w] * sig[w] * sig[w] * sig[w] * sig[w] / og / og;
+          dfG += rho[w] * sig[w] * a * a / og[w] / og[w] / og[w];
+          dfe += rho[w] * sig[w] * sig[w] * a / og[w] / og[w];
+          deG += rho[w] * Z[w] * sig[w] * sig[w] / og[w] / og[w];
+          dHG += rho[w] * sig[w] * sig[w] * sig[w] * sig[w] / og[w] / og[w];
         }
         dfG = -2.0 * kPi * lB * dfG;
         dfe = -2.0 * kPi * lB * dfe;
@@ -1915,25 +2468,25 @@ __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
         dHG = -dHG;
         const double detaG = deG + deH * dHG;
         const double denom = 1.0 / (2.0 * G - dfe * detaG - dfG);
+        double rbu[kMaxBonds];
+        for (int u = 0; u < MB; u++) rbu[u] = r.wb[(size_t)(u * 2) * P + K] + r.wb[(size_t)(u * 2 + 1) * P + K];
         for (int w = 0; w < NB; w++) {
-          const double inv = 1.0 / (1.0 + G * sig[w]);
-          const double Xw = (Z[w] - eta * (sig[w] * sig[w])) * inv;
+          const double Xw = (Z[w] - eta * (sig[w] * sig[w])) * inv[w];
           const double dfr = kPi * lB * (Xw * Xw);
-          const double der = sig[w] / H * Z[w] * inv;
-          const double dHr = (sig[w] * sig[w] * sig[w]) * (inv - 1.0 / 3.0);
+          const double der = sig[w] / H * Z[w] * inv[w];
+          const double dHr = (sig[w] * sig[w] * sig[w]) * (inv[w] - 1.0 / 3.0);
           const double dGr = (dfr + dfe * (der + dfe * deH * dHr)) * denom;
           const double detar = detaG * dGr;
           for (int u = 0; u < MB; u++) {
             const int i = r.bonds[2 * u], j = r.bonds[2 * u + 1];
             const double sij = (sig[i] + sig[j]) / 2.0;
-            const double ii = 1.0 / (1.0 + G * sig[i]);
+            const double ii = inv[i];
             const double Xi = (Z[i] - eta * (sig[i] * sig[i])) * ii;
             const double dXi = -((sig[i] * sig[i]) * ii * detar + sig[i] * Xi * ii * dGr);
-            const double ij = 1.0 / (1.0 + G * sig[j]);
+            const double ij = inv[j];
             const double Xj = (Z[j] - eta * (sig[j] * sig[j])) * ij;
             const double dXj = -((sig[j] * sig[j]) * ij * detar + sig[j] * Xj * ij * dGr);
-            const double rb = r.wb[(size_t)(u * 2) * P + K] + r.wb[(size_t)(u * 2 + 1) * P + K];
-            dphi[w] += rb / 2.0 * lB / sij * (dXi * Xj + Xi * dXj);
+            dphi[w] += rbu[u] / 2.0 * lB / sij * (dXi * Xj + Xi * dXj);
           }
         }
       }
@@ -1944,8 +2497,18 @@ __device__ void stage_msa(const DReq& r, Shared sh, bool tpt1) {
   const int nf = NB + (tpt1 ? MB : 0);
   for (int g0 = 0; g0 < nf; g0 += r.TB) {
     const int nT = min(r.TB, nf - g0);
-    dct2_forward_b(
-        fc, nT, [&](int t, int K) { return r.wc[(size_t)(g0 + t) * P + K]; },
+    dct2_forward_kp(
+        fc, nT,
+        [&](int kp, auto put) {
+          const int K = 2 * kp;
+          double2 v[kMaxTB];
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) v[u] = ldcg2(r.wc + (size_t)(g0 + u) * P + K);
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) put(u, v[u]);
+        },
         [&](int t, int k, double c) {
           const int w = g0 + t;
           if (w < NB) {
@@ -2054,7 +2617,7 @@ __device__ bool objective(const DReq& r, Shared sh, bool fp32 = false) {
   const int nout = r.NB + 2 * r.MB + 1;
   for (int g0 = 0; g0 < nout; g0 += r.TB) {
     const int nT = min(r.TB, nout - g0);
-    dct2_inverse_b(
+    dct2_inverse_kp(
         fc, nT,
         [&](int t, int k) {
           const int w = g0 + t;
@@ -2065,7 +2628,12 @@ __device__ bool objective(const DReq& r, Shared sh, bool fp32 = false) {
           for (int j = 0; j < r.NB; j++) f += r.Cb[(size_t)j * P + k] * r.z[j];
           return f * r.Wcoul[k];
         },
-        [&](int t, int K, double y) { g[(size_t)(g0 + t) * P + K] = y; });
+        [&](int kp, auto get) {
+          const int K = 2 * kp;
+#pragma unroll
+          for (int u = 0; u < kMaxTB; u++)
+            if (u < nT) stcg2(g + (size_t)(g0 + u) * P + K, get(u));
+        });
   }
   const double shift = stage_neutrality(r, sh);
   if (threadIdx.x == 0) g[off_psic(r)] = r.x[off_psic(r)] + shift;

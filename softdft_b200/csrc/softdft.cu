@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <new>
 #include <stdexcept>
 #include <cstdio>
@@ -123,6 +124,7 @@ struct Plan {
   std::vector<int> rad;          // general length: radices, M = their product
   std::vector<int> slot;         // general length: [M] digit-reversed slot of natural index m
   long long n = 0;
+  long long hstride = 0;  // column stride of the Anderson histories (n rounded up to 32)
   bool history = false;
   std::vector<int> bonds;
   std::vector<SpeciesHost> sp;
@@ -228,6 +230,7 @@ int plan_species(const sdft_system_desc* d, Plan& pl) {
   pl.MB = d->mb;
   pl.NS = d->n_species;
   pl.n = (long long)P * (pl.NB + 2 * pl.MB + 1) + 1;
+  pl.hstride = (pl.n + 31) / 32 * 32;
   pl.n_caller = (long long)Pt * (pl.NB + 2 * pl.MB + 1) + 1;
   pl.bonds.assign(d->bond_types, d->bond_types + 2 * pl.MB);
   const int NB = pl.NB;
@@ -445,8 +448,8 @@ void plan_layout(Plan& pl, bool history) {
   pl.o_fbe = lay.take<double>((size_t)4 * MB * P + 1);
   pl.o_elam = lay.take<double>((size_t)NB * P);
   if (history) {
-    pl.o_hx = lay.take<double>((size_t)kMaxAnderson * pl.n);
-    pl.o_hg = lay.take<double>((size_t)kMaxAnderson * pl.n);
+    pl.o_hx = lay.take<double>((size_t)kMaxAnderson * pl.hstride);
+    pl.o_hg = lay.take<double>((size_t)kMaxAnderson * pl.hstride);
     pl.o_u = lay.take<double>(pl.n);
   }
   pl.o_status = lay.take<int>(4);
@@ -607,6 +610,7 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.lB = d->bjerrum_length;
   r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
   r.n = pl.n;
+  r.hstride = pl.hstride;
   r.sig = (const double*)at(pl.o_sig);
   r.z = (const double*)at(pl.o_z);
   r.dmu = (const double*)at(pl.o_dmu);
@@ -732,6 +736,11 @@ struct sdft_request {
   // Picard flag, residual and LSQR warm start; the ring buffers stay in hx / hg
   SolveSlot slot{};
   int slot_m = 0;  // depth of the ring buffers in use (0: fresh)
+  // a prepared request (sdft_request_prepare) holds its plan and the descriptor
+  // values the upload reads until it is placed on the device
+  std::unique_ptr<Plan> pending;
+  sdft_system_desc pdesc{};
+  std::vector<double> pdia, pval, pdmu;
 };
 
 // the state of a solve that has not started (AndersonMixing.jl:80-90)
@@ -768,45 +777,16 @@ extern "C" void sdft_numerics_default(sdft_numerics* o) {
   o->mixed_switch = 0.0;
 }
 
-int request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
-  if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
-  *out = nullptr;
-  if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
-  if (precision != SDFT_PREC_FP64 && precision != SDFT_PREC_MIXED) return set_err(SDFT_ERR_ARG, "unknown precision");
-  Plan pl;
-  pl.prec = precision;
-  int rc = plan_species(d, pl);
-  if (rc) return rc;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(SDFT_ERR_CUDA, "no CUDA device");
-  plan_layout(pl, true);
-  plan_tables(d, pl);
-  auto* q = new sdft_request();
-  cudaGetDevice(&q->device);
-  q->precision = precision;
-  q->NP = pl.P;
-  q->NPt = pl.Pt;
-  q->n_caller = pl.n_caller;
-  q->M = pl.M;
-  q->L = pl.L;
-  q->NB = pl.NB;
-  q->MB = pl.MB;
-  q->NS = pl.NS;
-  q->n = pl.n;
-  q->sp = pl.sp;
-  q->bytes = pl.bytes;
-  cudaError_t e = cudaMalloc(&q->dmem, q->bytes);
+// device placement of a request: one allocation for the plan, its tables
+// uploaded and the initial guess in x; the request's stream exists already
+static int request_place(sdft_request* q, const sdft_system_desc* d, Plan& pl) {
+  cudaError_t e = cudaMalloc(&q->dmem, pl.bytes);
   if (e != cudaSuccess) {
-    delete q;
+    q->dmem = nullptr;
+    cudaGetLastError();  // the failed allocation leaves no sticky error
     return set_err(SDFT_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
   }
-  e = cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) {
-    cudaFree(q->dmem);
-    delete q;
-    return set_err(SDFT_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
-  }
-  cudaError_t ce = cudaMemsetAsync(q->dmem, 0, q->bytes, q->stream);
+  cudaError_t ce = cudaMemsetAsync(q->dmem, 0, pl.bytes, q->stream);
   std::vector<DSpecies> dsp;
   q->h = plan_bind(d, pl, q->dmem, nullptr, nullptr, dsp);
   q->dreq = (DReq*)(q->dmem + pl.o_dreq);
@@ -815,12 +795,101 @@ int request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* ou
   if (ce == cudaSuccess) ce = plan_upload(d, pl, q->dmem, q->h, dsp, q->stream);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(q->stream);
   if (ce != cudaSuccess) {
-    cudaStreamDestroy(q->stream);
     cudaFree(q->dmem);
-    delete q;
+    q->dmem = nullptr;
     return set_err(SDFT_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce));
   }
-  *out = q;
+  return SDFT_OK;
+}
+
+// validated plan and host tables of a request, with its stream; no device memory
+static int request_plan(const sdft_system_desc* d, int32_t precision, std::unique_ptr<sdft_request>& q,
+                        std::unique_ptr<Plan>& pl) {
+  if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
+  if (precision != SDFT_PREC_FP64 && precision != SDFT_PREC_MIXED) return set_err(SDFT_ERR_ARG, "unknown precision");
+  pl.reset(new Plan());
+  pl->prec = precision;
+  int rc = plan_species(d, *pl);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(SDFT_ERR_CUDA, "no CUDA device");
+  plan_layout(*pl, true);
+  plan_tables(d, *pl);
+  q.reset(new sdft_request());
+  cudaGetDevice(&q->device);
+  q->precision = precision;
+  q->NP = pl->P;
+  q->NPt = pl->Pt;
+  q->n_caller = pl->n_caller;
+  q->M = pl->M;
+  q->L = pl->L;
+  q->NB = pl->NB;
+  q->MB = pl->MB;
+  q->NS = pl->NS;
+  q->n = pl->n;
+  q->sp = pl->sp;
+  q->bytes = pl->bytes;
+  cudaError_t e = cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    q->stream = nullptr;
+    return set_err(SDFT_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  return SDFT_OK;
+}
+
+int request_create(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
+  if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
+  *out = nullptr;
+  std::unique_ptr<sdft_request> q;
+  std::unique_ptr<Plan> pl;
+  int rc = request_plan(d, precision, q, pl);
+  if (rc == SDFT_OK) rc = request_place(q.get(), d, *pl);
+  if (rc) {
+    if (q && q->stream) cudaStreamDestroy(q->stream);
+    return rc;
+  }
+  *out = q.release();
+  return SDFT_OK;
+}
+
+// sdft_request_prepare: the plan and the descriptor values its upload reads are
+// kept in the handle; the device memory is taken by request_ensure
+int request_prepare(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
+  if (!d || !out) return set_err(SDFT_ERR_ARG, "null argument");
+  *out = nullptr;
+  std::unique_ptr<sdft_request> q;
+  std::unique_ptr<Plan> pl;
+  int rc = request_plan(d, precision, q, pl);
+  if (rc) {
+    if (q && q->stream) cudaStreamDestroy(q->stream);
+    return rc;
+  }
+  const int NB = pl->NB;
+  q->pdia.assign(d->diameter, d->diameter + NB);
+  q->pval.assign(d->valence, d->valence + NB);
+  q->pdmu.assign(d->delta_muH, d->delta_muH + NB);
+  q->pdesc = *d;  // scalars; the arrays that plan_bind / plan_upload read are the copies above
+  q->pdesc.diameter = q->pdia.data();
+  q->pdesc.valence = q->pval.data();
+  q->pdesc.delta_muH = q->pdmu.data();
+  q->pdesc.species = nullptr;
+  q->pdesc.bond_types = nullptr;
+  q->pdesc.mu_ex_bulk = nullptr;
+  q->pdesc.lng_bulk = nullptr;
+  q->pending = std::move(pl);
+  *out = q.release();
+  return SDFT_OK;
+}
+
+// a prepared request takes its device memory now; SDFT_ERR_OOM leaves it prepared
+static int request_ensure(sdft_handle h) {
+  if (!h->pending) return SDFT_OK;
+  int rc = request_place(h, &h->pdesc, *h->pending);
+  if (rc) return rc;
+  h->pending.reset();
+  h->pdia.clear();
+  h->pval.clear();
+  h->pdmu.clear();
   return SDFT_OK;
 }
 
@@ -835,12 +904,32 @@ extern "C" int sdft_request_create(const sdft_system_desc* d, int32_t precision,
   }
 }
 
+extern "C" int sdft_request_prepare(const sdft_system_desc* d, int32_t precision, sdft_handle* out) {
+  try {
+    return request_prepare(d, precision, out);
+  } catch (const std::bad_alloc&) {
+    return set_err(SDFT_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_err(SDFT_ERR_ARG, e.what());
+  }
+}
+
 extern "C" int sdft_request_destroy(sdft_handle h) {
   if (!h) return SDFT_OK;
   cudaStreamSynchronize(h->stream);
-  cudaFree(h->dmem);
+  if (h->dmem) cudaFree(h->dmem);
   cudaStreamDestroy(h->stream);
   delete h;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_request_resident(sdft_handle h, int32_t* per_device) {
+  if (!h || !per_device) return set_err(SDFT_ERR_ARG, "null argument");
+  int ctas = 0, sms = 0;
+  CUDA_TRY(h->h.gen || (h->pending && h->pending->gen) ? occupancy_solve_gen(smem_bytes(h->M), &ctas)
+                                                      : occupancy_solve_pow2(smem_bytes(h->M), &ctas));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  *per_device = ctas * sms;
   return SDFT_OK;
 }
 
@@ -856,14 +945,12 @@ extern "C" int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* d
   return SDFT_OK;
 }
 
-// transform buffers per CTA: up to kMaxTB within 64 KB, so that three CTAs (the
-// solve kernel's register limit) fit an SM's shared memory; one buffer of M + M/8
-// complex values minimum.  At 444 requests this budget against 96 KB: NP = 1024
-// unchanged (4 buffers either way), NP = 2048 / 4096 26 % / 33 % faster per
-// iteration, odd NP = 1001 / 1029 18 % / 23 % faster
+// transform buffers per CTA: up to kMaxTB within kTransformBudget, so that the
+// solve kernel's occupancy target (kSolveCtasPerSm CTAs) fits an SM's shared
+// memory; one buffer of M + M/8 complex values minimum
 static int tb_for(int M) {
   const size_t buf = sizeof(double2) * (size_t)(M + M / 8);
-  size_t tb = (64 * 1024) / buf;
+  size_t tb = kTransformBudget / buf;
   if (tb < 1) tb = 1;
   if (tb > (size_t)kMaxTB) tb = kMaxTB;
   return (int)tb;
@@ -922,6 +1009,7 @@ static cudaError_t rows_copy(const sdft_request* h, double* dst, const double* s
 extern "C" int sdft_set_state(sdft_handle h, const double* mu_ex_K, const double* lng_K, const double* Psi,
                               const double* PsiC) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  if (int rc_ = request_ensure(h)) return rc_;
   const size_t P = h->NP;
   double* x = h->h.x;
   const cudaMemcpyKind H2D = cudaMemcpyHostToDevice;
@@ -948,11 +1036,13 @@ static int copy_vec_out(sdft_handle h, const double* dv, double* mu_ex_K, double
 
 extern "C" int sdft_get_state(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  if (int rc_ = request_ensure(h)) return rc_;
   return copy_vec_out(h, h->h.x, mu_ex_K, lng_K, Psi, PsiC);
 }
 
 extern "C" int sdft_objective(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  if (int rc_ = request_ensure(h)) return rc_;
   size_t sm = smem_bytes(h->M);
   CUDA_TRY(launch_objective(h->h.gen != 0, h->dreq, sm, h->stream));
   int st = 0;
@@ -985,6 +1075,8 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
                      bool resume = false) {
   int rc = validate_numerics(num);
   if (rc) return rc;
+  for (int i = 0; i < n; i++)
+    if ((rc = request_ensure(hs[i]))) return rc;
   if (resume)
     for (int i = 0; i < n; i++)
       if (hs[i]->slot_m != 0 && hs[i]->slot_m != num->anderm)
@@ -1118,6 +1210,7 @@ static int vec_out(sdft_handle h, const double* dv, double* dst) {
 
 extern "C" int sdft_get_solver_state(sdft_handle h, sdft_solver_state* st, double* hist_x, double* hist_g) {
   if (!h || !st) return set_err(SDFT_ERR_ARG, "null argument");
+  if (int rc_ = request_ensure(h)) return rc_;
   const SolveSlot& s = h->slot_m ? h->slot : fresh_slot();
   std::memset(st, 0, sizeof(*st));
   st->anderm = h->slot_m;
@@ -1127,11 +1220,11 @@ extern "C" int sdft_get_solver_state(sdft_handle h, sdft_solver_state* st, doubl
   for (int c = 0; c + 1 < h->slot_m && c < 15; c++) st->lambdas[c] = s.lam[c];
   for (int c = 0; c < h->slot_m; c++) {
     if (hist_x) {
-      int rc = vec_out(h, h->h.hx + (size_t)c * h->n, hist_x + (size_t)c * h->n_caller);
+      int rc = vec_out(h, h->h.hx + (size_t)c * h->h.hstride, hist_x + (size_t)c * h->n_caller);
       if (rc) return rc;
     }
     if (hist_g) {
-      int rc = vec_out(h, h->h.hg + (size_t)c * h->n, hist_g + (size_t)c * h->n_caller);
+      int rc = vec_out(h, h->h.hg + (size_t)c * h->h.hstride, hist_g + (size_t)c * h->n_caller);
       if (rc) return rc;
     }
   }
@@ -1142,6 +1235,7 @@ extern "C" int sdft_get_solver_state(sdft_handle h, sdft_solver_state* st, doubl
 extern "C" int sdft_set_solver_state(sdft_handle h, const sdft_solver_state* st, const double* hist_x,
                                      const double* hist_g) {
   if (!h || !st) return set_err(SDFT_ERR_ARG, "null argument");
+  if (int rc_ = request_ensure(h)) return rc_;
   if (st->anderm < 2 || st->anderm > kMaxAnderson) return set_err(SDFT_ERR_ARG, "anderm must be in [2, 16]");
   if (st->iter < 0) return set_err(SDFT_ERR_ARG, "negative iteration count");
   SolveSlot s = fresh_slot();
@@ -1150,15 +1244,15 @@ extern "C" int sdft_set_solver_state(sdft_handle h, const sdft_solver_state* st,
   s.err = st->err;
   for (int c = 0; c + 1 < st->anderm; c++) s.lam[c] = st->lambdas[c];
   // the columns hold stride-NP vectors; the pad point of odd grids stays 0
-  CUDA_TRY(cudaMemsetAsync(h->h.hx, 0, sizeof(double) * (size_t)kMaxAnderson * h->n, h->stream));
-  CUDA_TRY(cudaMemsetAsync(h->h.hg, 0, sizeof(double) * (size_t)kMaxAnderson * h->n, h->stream));
+  CUDA_TRY(cudaMemsetAsync(h->h.hx, 0, sizeof(double) * (size_t)kMaxAnderson * h->h.hstride, h->stream));
+  CUDA_TRY(cudaMemsetAsync(h->h.hg, 0, sizeof(double) * (size_t)kMaxAnderson * h->h.hstride, h->stream));
   for (int c = 0; c < st->anderm; c++) {
     if (hist_x) {
-      int rc = vec_in(h, h->h.hx + (size_t)c * h->n, hist_x + (size_t)c * h->n_caller);
+      int rc = vec_in(h, h->h.hx + (size_t)c * h->h.hstride, hist_x + (size_t)c * h->n_caller);
       if (rc) return rc;
     }
     if (hist_g) {
-      int rc = vec_in(h, h->h.hg + (size_t)c * h->n, hist_g + (size_t)c * h->n_caller);
+      int rc = vec_in(h, h->h.hg + (size_t)c * h->h.hstride, hist_g + (size_t)c * h->n_caller);
       if (rc) return rc;
     }
   }
@@ -1171,6 +1265,7 @@ extern "C" int sdft_set_solver_state(sdft_handle h, const sdft_solver_state* st,
 extern "C" int sdft_anderson_step(sdft_handle h, const sdft_numerics* num, const double* g_mu_ex_K,
                                   const double* g_lng_K, const double* g_Psi, const double* g_PsiC, double* err) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  if (int rc_ = request_ensure(h)) return rc_;
   int rc = validate_numerics(num);
   if (rc) return rc;
   if (!g_mu_ex_K || (h->MB && !g_lng_K) || !g_Psi || !g_PsiC) return set_err(SDFT_ERR_ARG, "null G(x) component");
@@ -1244,6 +1339,7 @@ struct sdft_server {
   std::vector<long long> tag;
   std::deque<std::pair<sdft_handle, long long>> queue;
   long long bytes_active = 0;
+  long long reserve = 0;  // device bytes admission leaves free (requests placed at admission)
   int active = 0;
   struct Done {
     long long tag;
@@ -1307,14 +1403,32 @@ extern "C" int sdft_server_submit(sdft_server_t sv, sdft_handle h, int64_t tag) 
 extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active, int32_t* queued) {
   if (!sv) return set_err(SDFT_ERR_ARG, "null server");
   if (iters < 1) return set_err(SDFT_ERR_ARG, "iters must be >= 1");
-  // admission: FIFO into free slots within the byte budget
-  for (int i = 0; i < sv->max_slots && !sv->queue.empty(); i++) {
-    if (sv->owner[i]) continue;
+  // admission: FIFO into free slots within the byte budget; a prepared request
+  // (sdft_request_prepare) is placed on the device here, once the free device
+  // memory less the reserve covers it, else it waits for retirements
+  int slot = 0;
+  while (!sv->queue.empty()) {
+    while (slot < sv->max_slots && sv->owner[slot]) slot++;
+    if (slot >= sv->max_slots) break;
     sdft_handle h = sv->queue.front().first;
+    const long long tag = sv->queue.front().second;
     if (sv->max_bytes > 0 && sv->bytes_active + (long long)h->bytes > sv->max_bytes) break;
+    if (h->pending) {
+      size_t fr = 0, tot = 0;
+      CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+      if ((long long)fr - (long long)h->bytes < sv->reserve) break;
+      const int rc = request_ensure(h);
+      if (rc == SDFT_ERR_OOM) break;  // another allocation took the memory: retry at the next step
+      if (rc) {                       // the request cannot be placed: it completes with that status
+        sv->done.push_back(sdft_server::Done{tag, rc, 0, 0.0, 0.0});
+        sv->queue.pop_front();
+        continue;
+      }
+    }
     CUDA_TRY(cudaStreamSynchronize(h->stream));  // the request's own uploads are complete
+    const int i = slot;
     sv->owner[i] = h;
-    sv->tag[i] = sv->queue.front().second;
+    sv->tag[i] = tag;
     sv->queue.pop_front();
     sv->hreq[i] = h->h;
     SolveSlot s{};
@@ -1370,6 +1484,13 @@ extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active
   return SDFT_OK;
 }
 
+extern "C" int sdft_server_set_reserve(sdft_server_t sv, int64_t reserve_bytes) {
+  if (!sv) return set_err(SDFT_ERR_ARG, "null server");
+  if (reserve_bytes < 0) return set_err(SDFT_ERR_ARG, "reserve must be >= 0");
+  sv->reserve = reserve_bytes;
+  return SDFT_OK;
+}
+
 extern "C" int sdft_server_poll(sdft_server_t sv, int64_t* tags, int32_t* status, int32_t* iters, double* errs,
                                 double* device_ms, int32_t max, int32_t* n) {
   if (!sv || !n) return set_err(SDFT_ERR_ARG, "null argument");
@@ -1390,6 +1511,7 @@ extern "C" int sdft_server_poll(sdft_server_t sv, int64_t* tags, int32_t* status
 
 extern "C" int sdft_get_densities(sdft_handle h, double* const* rho_segments, double* rho_beads_K, double* rho_bonds_K) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
+  if (int rc_ = request_ensure(h)) return rc_;
   if (rho_segments) {
     std::vector<DSpecies> dsp(h->NS);
     CUDA_TRY(cudaMemcpyAsync(dsp.data(), h->h.sp, sizeof(DSpecies) * h->NS, cudaMemcpyDeviceToHost, h->stream));
@@ -1415,6 +1537,7 @@ static int run_omega(sdft_handle h, std::vector<double>& out) {
 
 extern "C" int sdft_grand_potential(sdft_handle h, double* omega) {
   if (!h || !omega) return set_err(SDFT_ERR_ARG, "null argument");
+  if (int rc_ = request_ensure(h)) return rc_;
   std::vector<double> out;
   int rc = run_omega(h, out);
   if (rc) return rc;
@@ -1424,6 +1547,7 @@ extern "C" int sdft_grand_potential(sdft_handle h, double* omega) {
 
 extern "C" int sdft_num_species(sdft_handle h, double* num_species) {
   if (!h || !num_species) return set_err(SDFT_ERR_ARG, "null argument");
+  if (int rc_ = request_ensure(h)) return rc_;
   std::vector<double> out;
   int rc = run_omega(h, out);
   if (rc) return rc;
@@ -1463,6 +1587,9 @@ namespace {
 int objective_noalloc(const sdft_system_desc* d, const double* x_dev, double* g_dev, void* stream_ptr) {
   if (!d || !x_dev || !g_dev) return set_err(SDFT_ERR_ARG, "null argument");
   if (d->abi_version != SDFT_ABI_VERSION) return set_err(SDFT_ERR_ARG, "ABI version mismatch");
+  // G(x) is written as 16-byte grid-point pairs
+  if (reinterpret_cast<uintptr_t>(g_dev) % 16 != 0 || reinterpret_cast<uintptr_t>(x_dev) % 8 != 0)
+    return set_err(SDFT_ERR_ARG, "x_dev must be 8-byte and g_dev 16-byte aligned");
   Plan pl;
   int rc = plan_species(d, pl);
   if (rc) return rc;

@@ -29,7 +29,8 @@ EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_num
            "sdft_server_destroy", "sdft_server_submit", "sdft_server_step", "sdft_server_poll", "sdft_bulk_eval",
            "sdft_grid_supported", "sdft_input_from_yaml", "sdft_input_descriptor", "sdft_input_numerics",
            "sdft_input_bulk_stats", "sdft_input_destroy", "sdft_get_solver_state", "sdft_set_solver_state",
-           "sdft_solve_resume", "sdft_anderson_step"]
+           "sdft_solve_resume", "sdft_anderson_step", "sdft_request_prepare", "sdft_server_set_reserve",
+           "sdft_request_resident"]
 
 
 class SdftError(RuntimeError):
@@ -64,6 +65,8 @@ def lib():
         L.sdft_numerics_default.argtypes = [vp]
         L.sdft_numerics_default.restype = None
         L.sdft_request_create.argtypes = [vp, C.c_int32, C.POINTER(vp)]
+        L.sdft_request_prepare.argtypes = [vp, C.c_int32, C.POINTER(vp)]
+        L.sdft_server_set_reserve.argtypes = [vp, C.c_int64]
         L.sdft_request_destroy.argtypes = [vp]
         L.sdft_request_sizes.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.sdft_set_state.argtypes = [vp, vp, vp, vp, vp]
@@ -105,12 +108,15 @@ def device_count() -> int:
 
 
 class DeviceSystem:
-    """One request on the GPU (the C-ABI handle)."""
+    """One request on the GPU (the C-ABI handle).  With prepare=True the
+    request takes no device memory until it is first used or a server admits
+    it (sdft_request_prepare)."""
 
-    def __init__(self, d: Descriptor, precision: int = 0):
+    def __init__(self, d: Descriptor, precision: int = 0, prepare: bool = False):
         self.d = d
         self.h = C.c_void_p()
-        _check(lib().sdft_request_create(C.byref(d.desc), precision, C.byref(self.h)))
+        make = lib().sdft_request_prepare if prepare else lib().sdft_request_create
+        _check(make(C.byref(d.desc), precision, C.byref(self.h)))
         n = C.c_int64()
         b = C.c_int64()
         lib().sdft_request_sizes(self.h, C.byref(n), C.byref(b))
@@ -155,6 +161,14 @@ class DeviceSystem:
         err = C.c_double()
         rc = _check(lib().sdft_solve(self.h, C.byref(num), C.byref(it), C.byref(err)))
         return int(it.value), float(err.value), rc
+
+    def resident(self) -> int:
+        """Requests of this shape the device runs at once (sdft_request_resident)."""
+        n = C.c_int32()
+        f = lib().sdft_request_resident
+        f.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+        _check(f(self.h, C.byref(n)))
+        return int(n.value)
 
     def solve_resume(self, num: Numerics):
         """Continue the solve from the stored solver state (sdft_solve_resume)."""
@@ -262,6 +276,10 @@ class Server:
             self.close()
         except Exception:
             pass
+
+    def set_reserve(self, reserve_bytes: int) -> None:
+        """Device bytes that admission leaves free (sdft_server_set_reserve)."""
+        _check(lib().sdft_server_set_reserve(self.h, int(reserve_bytes)))
 
     def submit(self, system: "DeviceSystem", tag: int) -> None:
         _check(lib().sdft_server_submit(self.h, system.h, int(tag)))

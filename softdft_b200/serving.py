@@ -5,10 +5,10 @@ between launches the driver hands every arrived request to the server, runs
 one server step (one kernel launch advancing every active request by a
 bounded number of Anderson iterations) and collects the completions.  A
 request's latency is the time from its arrival to the end of the step in
-which it converged; requests are prepared (device memory, bulk state) before
-the stream starts, so latency covers queueing and the GPU solve.
+which it converged, including whatever the backend's submit and poll do at
+arrival and completion (building the request, reading its result).
 
-The backend is any object with submit(system, tag), step(iters) ->
+The backend is any object with submit(request, tag), step(iters) ->
 (active, queued) and poll() -> [(tag, status, iters, err, device_ms)];
 native.Server is the device one.
 """

@@ -21,10 +21,10 @@ vs the CPU oracle, through the C ABI.
   device handle, and both take the same driver iteration with the same G(x)
   (sdft_anderson_step / oracle_anderson_step), so only the arithmetic order of
   the LSQR sweeps differs.  The ring buffers and the residual come out bit for
-  bit.  The first least-squares problems are nearly singular (|lambda| up to
-  6e7 on the acid slit), so x moves with rounding: the device's step is held to
-  100 times the oracle's own spread when its history is perturbed in the last
-  bit.
+  bit, and both least-squares solutions leave the same residual |dG lambda + g|
+  to 1e-8.  The coefficients themselves are ill-determined: the first problems
+  are nearly singular (|lambda| up to 6e7 on the acid slit), so lambda and x
+  move with rounding (measured 1e-10..5e-7) and are held to 1e-5.
 * Checkpoint / resume: a solve stopped, saved and resumed (on the same or on
   another handle) equals the uninterrupted solve bit for bit.
 """
@@ -180,6 +180,18 @@ def _oracle_after_picard(ds, k):
     return dft, o, st, hx, hg, x
 
 
+def _ls_residual(hg, col, lam):
+    """|dG lambda + g_k| of the least-squares problem of AndersonMixing.jl:142,
+    dG[:, c] = G_hist[j_c] - g_k over the columns j_c != col, in extended precision."""
+    m = hg.shape[0]
+    g = hg[col].astype(np.longdouble)
+    r = g.copy()
+    cols = [j for j in range(m) if j != col]
+    for c, j in enumerate(cols):
+        r += (hg[j].astype(np.longdouble) - g) * np.longdouble(lam[c])
+    return float(np.sqrt(np.sum(r * r)))
+
+
 @pytest.mark.parametrize("name", ["plain_slit", "acid_salt", "brush"])
 def test_anderson_steps_from_identical_history(name):
     """The first Anderson steps (LSQR on the ring buffers, warm-started) from
@@ -190,33 +202,28 @@ def test_anderson_steps_from_identical_history(name):
     dft, o, st, hx, hg, x = _oracle_after_picard(ds, m - 1)
     assert st.use_picard == 1 and st.iter == m - 1
     d = native.DeviceSystem(dft.descriptor)
-    rng = np.random.default_rng(3)
     for step in range(4):
         g = o.objective()
         d.set_x(x)
         d.set_solver_state(st, hx, hg)
         err_d = d.anderson_step(num, g)
-        # the oracle's spread: the same step from its history perturbed in the last bit
-        o2 = OracleSystem(dft.descriptor)
-        o2.set_x(x)
-        o2.set_solver_state(st, hx, hg * (1.0 + 2.220446049250313e-16 * rng.choice([-1.0, 1.0], hg.shape)))
-        o2.anderson_step(num, g)
         err_o = o.anderson_step(num, g)
         assert err_d == err_o
         st_d, hx_d, hg_d = d.solver_state()
-        st2, _, _ = o2.solver_state()
         st, hx, hg = o.solver_state()
         assert st.use_picard == 0 and st_d.use_picard == 0 and st_d.iter == st.iter == m + step
         assert np.array_equal(hx_d, hx) and np.array_equal(hg_d, hg)
         x = o.get_x()
-        lam_o, lam_d, lam_2 = (np.array(s_.lambdas[: m - 1]) for s_ in (st, st_d, st2))
-        dx, dx_self = rel(d.get_x(), x), rel(o2.get_x(), x)
-        dl, dl_self = rel(lam_d, lam_o), rel(lam_2, lam_o)
+        col = (st.iter - 1) % m
+        lam_o, lam_d = (np.array(s_.lambdas[: m - 1]) for s_ in (st, st_d))
+        res_o, res_d = _ls_residual(hg, col, lam_o), _ls_residual(hg, col, lam_d)
+        dx, dl = rel(d.get_x(), x), rel(lam_d, lam_o)
+        dres = abs(res_d - res_o) / res_o
         print(f"\n{name} step {m + step}: |lambda| {np.max(np.abs(lam_o)):.3e}; device vs oracle: x {dx:.2e}, "
-              f"lambdas {dl:.2e}; oracle vs its last-bit perturbation: x {dx_self:.2e}, lambdas {dl_self:.2e}")
-        assert dx <= 100.0 * dx_self + 1e-13, (dx, dx_self)
-        assert dl <= 100.0 * dl_self + 1e-13, (dl, dl_self)
-        o2.close()
+              f"lambdas {dl:.2e}, least-squares residual {dres:.2e} (|r| {res_o:.3e} of |g| "
+              f"{float(np.linalg.norm(hg[col])):.3e})")
+        assert dres < 1e-8, dres
+        assert dl < 1e-5 and dx < 1e-5, (dl, dx)
     d.close()
 
 

@@ -74,3 +74,50 @@ def test_byte_budget_limits_admission():
         done += srv.poll()
     assert sorted(t for t, *_ in done) == [0, 1, 2]
     srv.close()
+
+
+def test_admission_follows_free_device_memory():
+    """Prepared requests take device memory only at admission, and only while
+    the free device memory less the server's reserve covers them: with a
+    reserve that leaves room for two requests, at most two are active, the
+    queue waits for retirements (each finished request is destroyed, which
+    returns its memory), and every request ends in the state of its solve alone."""
+    import torch
+
+    cases = [small_slit(np_=4096, dz=0.005, pH=pH, n_chain=6) for pH in (6.0, 7.0, 8.0, 9.0, 7.5)]
+    num = numerics_from_dict(dict(cases[0]["numerical"], tole=1e-8, max_iters=5000))
+    dfts = [descriptor(c) for c in cases]
+    alone = []
+    for d in dfts:
+        s = native.DeviceSystem(d.descriptor)
+        it, err, rc = s.solve(num)
+        assert rc == 0
+        alone.append((s.get_x(), it))
+        s.close()
+    prepared = [native.DeviceSystem(d.descriptor, prepare=True) for d in dfts]
+    one = max(s.device_bytes for s in prepared)
+    assert one > 16 * 2 ** 20  # large against the 2 MiB allocation granularity
+    srv = native.Server(num, max_slots=8)
+    free0, _ = torch.cuda.mem_get_info()
+    srv.set_reserve(int(free0 - 2.5 * one))
+    for i, s in enumerate(prepared):
+        srv.submit(s, i)
+    done = {}
+    most = 0
+    steps = 0
+    while len(done) < len(prepared):
+        active, queued = srv.step(40)
+        most = max(most, active)
+        assert active <= 2
+        for tag, st, it, err, dms in srv.poll():
+            x = prepared[tag].get_x()
+            done[tag] = (st, it, x)
+            prepared[tag].close()  # the finished request's memory returns to the pool of free HBM
+        steps += 1
+        assert steps < 2000
+    assert most == 2
+    for i in range(len(prepared)):
+        st, it, x = done[i]
+        assert st == 0 and it == alone[i][1]
+        assert np.array_equal(x, alone[i][0])
+    srv.close()
