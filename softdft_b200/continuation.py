@@ -27,8 +27,9 @@ whole grid spacings this is the routines' index copy of the near-wall halves.
 
 Grid.  A step with wall separation H and requested spacing dz uses the
 reference's grid NP = cld(H, dz) + 1 whenever the device transform runs it
-(native.grid_supported: NP >= 16 whose FFT length has no prime factor above 61
-and fits one CTA's shared memory); otherwise the spacing is an upper bound and
+(native.grid_supported: NP >= 16 whose FFT length fits one CTA's shared memory,
+by mixed radix or, for a prime factor above 61, by Bluestein's transform);
+otherwise the spacing is an upper bound and
 NP is the next supported size, at spacing H / (NP - 1) (nudged so that the
 reference's rule gives exactly NP).  `grid="pow2"` keeps the earlier policy of
 power-of-two grids, `grid="exact"` the requested spacing as is.

@@ -111,6 +111,15 @@ struct DReq {
   const float2* tw32;     // FP32 copies of tw, twP, twD (mixed precision)
   const float2* twP32;
   const float2* twD32;
+  // Bluestein transform (general length with a prime factor above kMaxGenRadix)
+  int blue;               // 1: the length-M DFTs run as chirp convolutions of length LB
+  int LB, lLB;            // LB = 2^lLB >= 2M - 1 (the transform buffers hold LB points)
+  const double2* bw;      // [M] chirp e^{-i pi n^2 / M}
+  const double2* bB;      // [LB] spectrum of the chirp filter / LB, bit-reversed order
+  const double2* btw;     // [LB/2 + 1] e^{-2 pi i k / LB}
+  const float2* bw32;     // FP32 copies (mixed precision)
+  const float2* bB32;
+  const float2* btw32;
   // state
   double* x;              // [n] unknowns
   double* g;              // [n] G(x) of the last evaluation

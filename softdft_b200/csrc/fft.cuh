@@ -59,6 +59,11 @@ struct FftCtxT {
   const C* __restrict__ tw;   // [M/2] e^{-2 pi i k / M} ([M] for a general length)
   const C* __restrict__ twP;  // [M+1] e^{-2 pi i k / P}
   const C* __restrict__ twD;  // [M+1] e^{-i pi k / 2P}
+  int blue;                   // general length: Bluestein transform (a prime factor above kMaxGenRadix)
+  int LB, lLB;                // Bluestein convolution length 2^lLB >= 2M - 1
+  const C* __restrict__ bw;   // [M] chirp e^{-i pi n^2 / M}
+  const C* __restrict__ bB;   // [LB] chirp filter spectrum / LB, bit-reversed order
+  const C* __restrict__ btw;  // [LB/2] e^{-2 pi i k / LB}
 };
 using FftCtx = FftCtxT<double2>;
 
@@ -76,6 +81,13 @@ __device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
   c.tw = r.tw;
   c.twP = r.twP;
   c.twD = r.twD;
+  c.blue = r.blue;
+  c.LB = r.LB;
+  c.lLB = r.lLB;
+  c.bw = r.bw;
+  c.bB = r.bB;
+  c.btw = r.btw;
+  if (r.blue) c.stride = r.LB + (r.LB >> 3);
   return c;
 }
 
@@ -94,6 +106,13 @@ __device__ __forceinline__ FftCtxT<float2> make_fft32(double2* z, const DReq& r)
   c.tw = r.tw32;
   c.twP = r.twP32;
   c.twD = r.twD32;
+  c.blue = r.blue;
+  c.LB = r.LB;
+  c.lLB = r.lLB;
+  c.bw = r.bw32;
+  c.bB = r.bB32;
+  c.btw = r.btw32;
+  if (r.blue) c.stride = r.LB + (r.LB >> 3);
   return c;
 }
 
@@ -415,69 +434,74 @@ __device__ __noinline__ void fft_gen_inv(const FftCtxT<C> c, int nT) {
   __syncthreads();
 }
 
-// forward FFT of nT buffers: bit-reversed (digit-reversed) input -> natural output
-template <class C>
-__device__ __forceinline__ void fft_fwd_b(const FftCtxT<C>& c, int nT) {
-  if constexpr (SDFT_FFT_GEN != 0) {
-    fft_gen_fwd(c, nT);
-    return;
-  }
-  const int M = c.M, L = c.L;
+// ---- power-of-two pass sets over nT buffers of N = 2^lN points ----------------
+// DIT: bit-reversed input -> natural output; DIF: natural input -> bit-reversed
+// output.  tw[k] = e^{-2 pi i k / N} (k < N/2); CONJ uses the conjugate roots (an
+// unscaled inverse transform).  Three radix-2 stages per pass (radix-8), a
+// radix-4 or radix-2 pass takes the remainder of lN.
+template <class C, bool CONJ>
+__device__ __forceinline__ C tw_at(const C* __restrict__ tw, int k) {
+  const C w = __ldg(&tw[k]);
+  return CONJ ? conj2(w) : w;
+}
+
+template <class C, bool CONJ>
+__device__ __forceinline__ void pow2_dit(C* z, int stride, int nT, int N, int L, const C* __restrict__ tw) {
   for (int s = 0; s < L;) {
     const int rr = min(3, L - s);
     const int h = 1 << s;
     __syncthreads();
     if (rr == 3) {
-      const int per = M >> 3, lper = L - 3;
+      const int per = N >> 3, lper = L - 3;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        C* zb = c.z + (size_t)t * c.stride;
+        C* zb = z + (size_t)t * stride;
         const int p = u & (h - 1);
         const int base = ((u >> s) << (s + 3)) + p;
         C x[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) x[j] = zb[fpad(base + j * h)];
-        const C w1 = __ldg(&c.tw[p << (L - 1 - s)]);
+        const C w1 = tw_at<C, CONJ>(tw, p << (L - 1 - s));
 #pragma unroll
         for (int m = 0; m < 4; m++) bfly(x[2 * m], x[2 * m + 1], w1);
-        const C w2a = __ldg(&c.tw[p << (L - 2 - s)]);
-        const C w2b = __ldg(&c.tw[(p + h) << (L - 2 - s)]);
+        const C w2a = tw_at<C, CONJ>(tw, p << (L - 2 - s));
+        const C w2b = tw_at<C, CONJ>(tw, (p + h) << (L - 2 - s));
         bfly(x[0], x[2], w2a);
         bfly(x[1], x[3], w2b);
         bfly(x[4], x[6], w2a);
         bfly(x[5], x[7], w2b);
 #pragma unroll
-        for (int j = 0; j < 4; j++) bfly(x[j], x[j + 4], __ldg(&c.tw[(p + j * h) << (L - 3 - s)]));
+        for (int j = 0; j < 4; j++) bfly(x[j], x[j + 4], tw_at<C, CONJ>(tw, (p + j * h) << (L - 3 - s)));
 #pragma unroll
         for (int j = 0; j < 8; j++) zb[fpad(base + j * h)] = x[j];
       }
     } else if (rr == 2) {
-      const int per = M >> 2, lper = L - 2;
+      const int per = N >> 2, lper = L - 2;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        C* zb = c.z + (size_t)t * c.stride;
+        C* zb = z + (size_t)t * stride;
         const int p = u & (h - 1);
         const int base = ((u >> s) << (s + 2)) + p;
         C x[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) x[j] = zb[fpad(base + j * h)];
-        const C w1 = __ldg(&c.tw[p << (L - 1 - s)]);
+        const C w1 = tw_at<C, CONJ>(tw, p << (L - 1 - s));
         bfly(x[0], x[1], w1);
         bfly(x[2], x[3], w1);
-        bfly(x[0], x[2], __ldg(&c.tw[p << (L - 2 - s)]));
-        bfly(x[1], x[3], __ldg(&c.tw[(p + h) << (L - 2 - s)]));
+        bfly(x[0], x[2], tw_at<C, CONJ>(tw, p << (L - 2 - s)));
+        bfly(x[1], x[3], tw_at<C, CONJ>(tw, (p + h) << (L - 2 - s)));
 #pragma unroll
         for (int j = 0; j < 4; j++) zb[fpad(base + j * h)] = x[j];
       }
     } else {
-      const int per = M >> 1, lper = L - 1;
+      const int per = N >> 1, lper = L - 1;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        C* zb = c.z + (size_t)t * c.stride;
+        C* zb = z + (size_t)t * stride;
         const int p = u & (h - 1);
         const int base = ((u >> s) << (s + 1)) + p;
         C a = zb[fpad(base)], b = zb[fpad(base + h)];
-        bfly(a, b, __ldg(&c.tw[p << (L - 1 - s)]));
+        bfly(a, b, tw_at<C, CONJ>(tw, p << (L - 1 - s)));
         zb[fpad(base)] = a;
         zb[fpad(base + h)] = b;
       }
@@ -487,70 +511,64 @@ __device__ __forceinline__ void fft_fwd_b(const FftCtxT<C>& c, int nT) {
   __syncthreads();
 }
 
-// inverse FFT of nT buffers (unscaled): natural input -> bit-reversed (digit-reversed) output
-template <class C>
-__device__ __forceinline__ void fft_inv_b(const FftCtxT<C>& c, int nT) {
-  if constexpr (SDFT_FFT_GEN != 0) {
-    fft_gen_inv(c, nT);
-    return;
-  }
-  const int M = c.M, L = c.L;
+template <class C, bool CONJ>
+__device__ __forceinline__ void pow2_dif(C* z, int stride, int nT, int N, int L, const C* __restrict__ tw) {
   for (int top = L; top > 0;) {
     const int rr = min(3, top);
     const int s0 = top - rr;
     const int h = 1 << s0;
     __syncthreads();
     if (rr == 3) {
-      const int per = M >> 3, lper = L - 3;
+      const int per = N >> 3, lper = L - 3;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        C* zb = c.z + (size_t)t * c.stride;
+        C* zb = z + (size_t)t * stride;
         const int p = u & (h - 1);
         const int base = ((u >> s0) << (s0 + 3)) + p;
         C x[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) x[j] = zb[fpad(base + j * h)];
 #pragma unroll
-        for (int j = 0; j < 4; j++) bfly_dif(x[j], x[j + 4], conj2(__ldg(&c.tw[(p + j * h) << (L - 3 - s0)])));
-        const C w2a = conj2(__ldg(&c.tw[p << (L - 2 - s0)]));
-        const C w2b = conj2(__ldg(&c.tw[(p + h) << (L - 2 - s0)]));
+        for (int j = 0; j < 4; j++) bfly_dif(x[j], x[j + 4], tw_at<C, CONJ>(tw, (p + j * h) << (L - 3 - s0)));
+        const C w2a = tw_at<C, CONJ>(tw, p << (L - 2 - s0));
+        const C w2b = tw_at<C, CONJ>(tw, (p + h) << (L - 2 - s0));
         bfly_dif(x[0], x[2], w2a);
         bfly_dif(x[1], x[3], w2b);
         bfly_dif(x[4], x[6], w2a);
         bfly_dif(x[5], x[7], w2b);
-        const C w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
+        const C w1 = tw_at<C, CONJ>(tw, p << (L - 1 - s0));
 #pragma unroll
         for (int m = 0; m < 4; m++) bfly_dif(x[2 * m], x[2 * m + 1], w1);
 #pragma unroll
         for (int j = 0; j < 8; j++) zb[fpad(base + j * h)] = x[j];
       }
     } else if (rr == 2) {
-      const int per = M >> 2, lper = L - 2;
+      const int per = N >> 2, lper = L - 2;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        C* zb = c.z + (size_t)t * c.stride;
+        C* zb = z + (size_t)t * stride;
         const int p = u & (h - 1);
         const int base = ((u >> s0) << (s0 + 2)) + p;
         C x[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) x[j] = zb[fpad(base + j * h)];
-        bfly_dif(x[0], x[2], conj2(__ldg(&c.tw[p << (L - 2 - s0)])));
-        bfly_dif(x[1], x[3], conj2(__ldg(&c.tw[(p + h) << (L - 2 - s0)])));
-        const C w1 = conj2(__ldg(&c.tw[p << (L - 1 - s0)]));
+        bfly_dif(x[0], x[2], tw_at<C, CONJ>(tw, p << (L - 2 - s0)));
+        bfly_dif(x[1], x[3], tw_at<C, CONJ>(tw, (p + h) << (L - 2 - s0)));
+        const C w1 = tw_at<C, CONJ>(tw, p << (L - 1 - s0));
         bfly_dif(x[0], x[1], w1);
         bfly_dif(x[2], x[3], w1);
 #pragma unroll
         for (int j = 0; j < 4; j++) zb[fpad(base + j * h)] = x[j];
       }
     } else {
-      const int per = M >> 1, lper = L - 1;
+      const int per = N >> 1, lper = L - 1;
       for (int it = threadIdx.x; it < nT * per; it += blockDim.x) {
         const int t = it >> lper, u = it & (per - 1);
-        C* zb = c.z + (size_t)t * c.stride;
+        C* zb = z + (size_t)t * stride;
         const int p = u & (h - 1);
         const int base = ((u >> s0) << (s0 + 1)) + p;
         C a = zb[fpad(base)], b = zb[fpad(base + h)];
-        bfly_dif(a, b, conj2(__ldg(&c.tw[p << (L - 1 - s0)])));
+        bfly_dif(a, b, tw_at<C, CONJ>(tw, p << (L - 1 - s0)));
         zb[fpad(base)] = a;
         zb[fpad(base + h)] = b;
       }
@@ -558,6 +576,75 @@ __device__ __forceinline__ void fft_inv_b(const FftCtxT<C>& c, int nT) {
     top = s0;
   }
   __syncthreads();
+}
+
+// ---- Bluestein (chirp-z) transform for lengths with a large prime factor ----
+// X[k] = sum_n x_n W^{nk}, W = e^{-2 pi i / M}, through nk = (n^2 + k^2 - (k-n)^2) / 2:
+// X[k] = w_k sum_n (x_n w_n) conj(w_{k-n}),  w_n = e^{-i pi n^2 / M}
+// (L. Bluestein, IEEE Trans. Audio Electroacoust. 18(4), 1970).  The sum is a
+// cyclic convolution of length L = 2^lL >= 2M - 1: the chirped input, zero
+// padded, goes through a DIF pass set (natural -> bit-reversed), is multiplied by
+// the spectrum of the chirp filter (host table bB, bit-reversed order, divided by
+// L), and comes back through a DIT pass set with the conjugate roots (bit-reversed
+// -> natural).  The inverse DFT is conj(DFT(conj x)).  Input and output are in
+// natural order in buffer slots [0, M).
+template <class C>
+__device__ void bluestein_b(const FftCtxT<C>& c, int nT, bool inverse) {
+  const int M = c.M, LB = c.LB;
+  __syncthreads();
+  for (int it = threadIdx.x; it < nT * LB; it += blockDim.x) {
+    const int t = it >> c.lLB, m = it & (LB - 1);
+    C* zb = c.z + (size_t)t * c.stride;
+    C v = Cx<C>::make(0, 0);
+    if (m < M) {
+      v = zb[fpad(m)];
+      if (inverse) v = conj2(v);
+      v = cmul(v, __ldg(&c.bw[m]));
+    }
+    zb[fpad(m)] = v;
+  }
+  pow2_dif<C, false>(c.z, c.stride, nT, LB, c.lLB, c.btw);
+  for (int it = threadIdx.x; it < nT * LB; it += blockDim.x) {
+    const int t = it >> c.lLB, j = it & (LB - 1);
+    C* zb = c.z + (size_t)t * c.stride;
+    zb[fpad(j)] = cmul(zb[fpad(j)], __ldg(&c.bB[j]));
+  }
+  pow2_dit<C, true>(c.z, c.stride, nT, LB, c.lLB, c.btw);
+  for (int it = threadIdx.x; it < nT * M; it += blockDim.x) {
+    const int t = it / M, k = it - t * M;
+    C* zb = c.z + (size_t)t * c.stride;
+    C v = cmul(zb[fpad(k)], __ldg(&c.bw[k]));
+    zb[fpad(k)] = inverse ? conj2(v) : v;
+  }
+  __syncthreads();
+}
+
+// forward FFT of nT buffers: bit-reversed (digit-reversed) input -> natural output
+template <class C>
+__device__ __forceinline__ void fft_fwd_b(const FftCtxT<C>& c, int nT) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    if (c.blue) {
+      bluestein_b(c, nT, false);
+      return;
+    }
+    fft_gen_fwd(c, nT);
+    return;
+  }
+  pow2_dit<C, false>(c.z, c.stride, nT, c.M, c.L, c.tw);
+}
+
+// inverse FFT of nT buffers (unscaled): natural input -> bit-reversed (digit-reversed) output
+template <class C>
+__device__ __forceinline__ void fft_inv_b(const FftCtxT<C>& c, int nT) {
+  if constexpr (SDFT_FFT_GEN != 0) {
+    if (c.blue) {
+      bluestein_b(c, nT, true);
+      return;
+    }
+    fft_gen_inv(c, nT);
+    return;
+  }
+  pow2_dif<C, true>(c.z, c.stride, nT, c.M, c.L, c.tw);
 }
 
 // ---- pair step ------------------------------------------------------------

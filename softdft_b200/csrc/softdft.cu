@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <memory>
 #include <new>
 #include <stdexcept>
@@ -93,6 +94,28 @@ double filter_k(int k, int N, double dz) {  // apply_filter.jl
   return std::exp(-(t2 * t2));
 }
 double2 cis(long double a) { return make_double2((double)cosl(a), (double)sinl(a)); }
+
+// in-place forward DFT X[k] = sum_m x_m e^{-2 pi i k m / n} of a power-of-two
+// length, radix-2 decimation in time in long double (host tables only)
+void fft_host(std::vector<std::complex<long double>>& a) {
+  const size_t n = a.size();
+  for (size_t i = 1, j = 0; i < n; i++) {  // bit-reversal permutation
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  const long double pi = 3.14159265358979323846264338327950288L;
+  for (size_t len = 2; len <= n; len <<= 1) {
+    for (size_t i = 0; i < n; i += len)
+      for (size_t k = 0; k < len / 2; k++) {
+        const std::complex<long double> w = std::polar(1.0L, -2.0L * pi * (long double)k / (long double)len);
+        const std::complex<long double> u = a[i + k], v = a[i + k + len / 2] * w;
+        a[i + k] = u + v;
+        a[i + k + len / 2] = u - v;
+      }
+  }
+}
 int jround(double x) { return (int)std::nearbyint(x); }
 
 struct Layout {
@@ -146,6 +169,13 @@ struct Plan {
   std::vector<double> Ext, tr, Csurf, Wbond, Wfmt, Wmsa, Wcoul, x0;
   std::vector<double2> tw, twP, twD;
   std::vector<float2> tw32, twP32, twD32;
+  // Bluestein transform: a length with a prime factor above kMaxGenRadix
+  bool blue = false;
+  int LB = 0, lLB = 0;   // convolution length 2^lLB >= 2M - 1
+  int BL = 0;            // points of a transform buffer: M, or LB under Bluestein
+  std::vector<double2> bw, bB, btw;
+  std::vector<float2> bw32, bB32, btw32;
+  size_t o_bw = 0, o_bB = 0, o_btw = 0, o_bw32 = 0, o_bB32 = 0, o_btw32 = 0;
 };
 
 // radices of a general-length FFT of M points (4s, then 2, 3, 5, 7 and larger
@@ -198,12 +228,20 @@ static int plan_grid(int Pt, Plan& pl) {
   const bool odd = (Pt & 1) != 0;
   const int P = odd ? Pt + 1 : Pt;
   const int Mf = odd ? Pt : Pt / 2;
-  if (!fft_radices(Mf, pl.rad))
-    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(Pt) + ": " + (odd ? "NP" : "NP/2") +
-                                             " has a prime factor above " + std::to_string(kMaxGenRadix));
-  pl.gen = (Mf & (Mf - 1)) != 0;
-  if (smem_bytes(Mf) > kMaxSmemBytes)
-    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(Pt) + " needs more shared memory than a CTA has");
+  // a length with a prime factor above kMaxGenRadix runs Bluestein's chirp
+  // convolution of length LB = 2^lLB >= 2M - 1
+  pl.blue = !fft_radices(Mf, pl.rad);
+  pl.LB = pl.lLB = 0;
+  if (pl.blue) {
+    pl.rad.clear();
+    while ((1 << pl.lLB) < 2 * Mf - 1) pl.lLB++;
+    pl.LB = 1 << pl.lLB;
+  }
+  pl.gen = pl.blue || (Mf & (Mf - 1)) != 0;
+  pl.BL = pl.blue ? pl.LB : Mf;
+  if (smem_bytes(pl.BL) > kMaxSmemBytes)
+    return set_err(SDFT_ERR_UNSUPPORTED, "NP = " + std::to_string(Pt) + " needs more shared memory than a CTA has" +
+                                             (pl.blue ? " (Bluestein transform of " + std::to_string(pl.LB) + " points)" : ""));
   pl.P = P;
   pl.Pt = Pt;
   pl.M = Mf;
@@ -424,6 +462,16 @@ void plan_layout(Plan& pl, bool history) {
   pl.o_slot_tab = pl.gen ? lay.take<int>(M) : 0;
   pl.o_twP = lay.take<double2>(M + 1);
   pl.o_twD = lay.take<double2>(M + 1);
+  if (pl.blue) {
+    pl.o_bw = lay.take<double2>(M);
+    pl.o_bB = lay.take<double2>(pl.LB);
+    pl.o_btw = lay.take<double2>(pl.LB / 2 + 1);
+    if (pl.prec == SDFT_PREC_MIXED) {
+      pl.o_bw32 = lay.take<float2>(M);
+      pl.o_bB32 = lay.take<float2>(pl.LB);
+      pl.o_btw32 = lay.take<float2>(pl.LB / 2 + 1);
+    }
+  }
   if (pl.prec == SDFT_PREC_MIXED) {
     pl.o_tw32 = lay.take<float2>(ntw);
     pl.o_twP32 = lay.take<float2>(M + 1);
@@ -535,7 +583,36 @@ void plan_tables(const sdft_system_desc* d, Plan& pl) {
   pl.twP.resize(M + 1);
   pl.twD.resize(M + 1);
   for (size_t k = 0; k < pl.tw.size(); k++) pl.tw[k] = cis(-2.0L * PI_L * (long double)k / M);
-  if (pl.gen) fft_digit_slots(M, pl.rad, pl.slot);
+  if (pl.blue) {  // natural order in and out; the chirp tables
+    pl.slot.resize(M);
+    for (int m = 0; m < M; m++) pl.slot[m] = m;
+    const int LB = pl.LB;
+    pl.bw.resize(M);
+    for (int m = 0; m < M; m++) {
+      const long long q = ((long long)m * m) % (2LL * M);  // e^{-i pi m^2 / M} with the argument reduced mod 2 pi
+      pl.bw[m] = cis(-PI_L * (long double)q / M);
+    }
+    // filter b[m] = conj(w_m) for |m| < M on the cyclic grid of LB points, and its DFT
+    std::vector<std::complex<long double>> b(LB, 0.0L);
+    for (int m = 0; m < M; m++) {
+      const long long q = ((long long)m * m) % (2LL * M);
+      const std::complex<long double> v = std::polar(1.0L, PI_L * (long double)q / M);
+      b[m] = v;
+      if (m) b[LB - m] = v;
+    }
+    fft_host(b);
+    pl.bB.resize(LB);
+    for (int j = 0; j < LB; j++) {
+      int k = 0;
+      for (int bit = 0; bit < pl.lLB; bit++) k |= ((j >> bit) & 1) << (pl.lLB - 1 - bit);
+      const std::complex<long double> v = b[k] / (long double)LB;
+      pl.bB[j] = make_double2((double)v.real(), (double)v.imag());
+    }
+    pl.btw.resize(LB / 2 + 1);
+    for (int k = 0; k <= LB / 2; k++) pl.btw[k] = cis(-2.0L * PI_L * k / LB);
+  } else if (pl.gen) {
+    fft_digit_slots(M, pl.rad, pl.slot);
+  }
   for (int k = 0; k <= M; k++) pl.twP[k] = cis(-2.0L * PI_L * k / Pt);
   for (int k = 0; k <= M; k++) pl.twD[k] = cis(-PI_L * k / (2.0L * Pt));
   if (pl.prec == SDFT_PREC_MIXED) {
@@ -546,6 +623,14 @@ void plan_tables(const sdft_system_desc* d, Plan& pl) {
     for (size_t k = 0; k < pl.tw.size(); k++) pl.tw32[k] = f2(pl.tw[k]);
     for (size_t k = 0; k < pl.twP.size(); k++) pl.twP32[k] = f2(pl.twP[k]);
     for (size_t k = 0; k < pl.twD.size(); k++) pl.twD32[k] = f2(pl.twD[k]);
+    if (pl.blue) {
+      pl.bw32.resize(pl.bw.size());
+      pl.bB32.resize(pl.bB.size());
+      pl.btw32.resize(pl.btw.size());
+      for (size_t k = 0; k < pl.bw.size(); k++) pl.bw32[k] = f2(pl.bw[k]);
+      for (size_t k = 0; k < pl.bB.size(); k++) pl.bB32[k] = f2(pl.bB[k]);
+      for (size_t k = 0; k < pl.btw.size(); k++) pl.btw32[k] = f2(pl.btw[k]);
+    }
   }
   if (pl.history) {
     pl.x0.assign(pl.n, 0.0);
@@ -603,7 +688,7 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.NS = pl.NS;
   r.funcs = (int)d->functionals;
   // odd grids pack two real transforms into each buffer
-  r.TB = pl.P != pl.Pt ? std::min(kMaxTB, 2 * tb_for(pl.M)) : tb_for(pl.M);
+  r.TB = pl.P != pl.Pt ? std::min(kMaxTB, 2 * tb_for(pl.BL)) : tb_for(pl.BL);
   r.ngrp = (int)pl.grp_sig.size();
   r.prec = pl.prec;
   r.dz = d->bin_width;
@@ -632,6 +717,15 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.nrad = pl.gen ? (int)pl.rad.size() : 0;
   for (int i = 0; i < r.nrad; i++) r.rad[i] = pl.rad[i];
   r.slot = pl.gen ? (const int*)at(pl.o_slot_tab) : nullptr;
+  r.blue = pl.blue ? 1 : 0;
+  r.LB = pl.LB;
+  r.lLB = pl.lLB;
+  r.bw = pl.blue ? (const double2*)at(pl.o_bw) : nullptr;
+  r.bB = pl.blue ? (const double2*)at(pl.o_bB) : nullptr;
+  r.btw = pl.blue ? (const double2*)at(pl.o_btw) : nullptr;
+  r.bw32 = pl.blue && pl.o_bw32 ? (const float2*)at(pl.o_bw32) : nullptr;
+  r.bB32 = pl.blue && pl.o_bB32 ? (const float2*)at(pl.o_bB32) : nullptr;
+  r.btw32 = pl.blue && pl.o_btw32 ? (const float2*)at(pl.o_btw32) : nullptr;
   r.twP = (const double2*)at(pl.o_twP);
   r.twD = (const double2*)at(pl.o_twD);
   const bool mixed = pl.prec == SDFT_PREC_MIXED;
@@ -703,6 +797,16 @@ cudaError_t plan_upload(const sdft_system_desc* d, const Plan& pl, char* base, c
   up(pl.o_Wcoul, pl.Wcoul.data(), sizeof(double) * P);
   up(pl.o_tw, pl.tw.data(), sizeof(double2) * pl.tw.size());
   if (pl.gen) up(pl.o_slot_tab, pl.slot.data(), sizeof(int) * pl.slot.size());
+  if (pl.blue) {
+    up(pl.o_bw, pl.bw.data(), sizeof(double2) * pl.bw.size());
+    up(pl.o_bB, pl.bB.data(), sizeof(double2) * pl.bB.size());
+    up(pl.o_btw, pl.btw.data(), sizeof(double2) * pl.btw.size());
+    if (pl.o_bw32) {
+      up(pl.o_bw32, pl.bw32.data(), sizeof(float2) * pl.bw32.size());
+      up(pl.o_bB32, pl.bB32.data(), sizeof(float2) * pl.bB32.size());
+      up(pl.o_btw32, pl.btw32.data(), sizeof(float2) * pl.btw32.size());
+    }
+  }
   up(pl.o_twP, pl.twP.data(), sizeof(double2) * pl.twP.size());
   up(pl.o_twD, pl.twD.data(), sizeof(double2) * pl.twD.size());
   if (pl.prec == SDFT_PREC_MIXED) {
@@ -722,6 +826,7 @@ struct sdft_request {
   cudaStream_t stream = nullptr;
   int precision = SDFT_PREC_FP64;
   int NP = 0, M = 0, L = 0, NB = 0, MB = 0, NS = 0;
+  int BL = 0;             // points of a transform buffer (M, or the Bluestein length)
   int NPt = 0;            // grid points (NP: stride of the device arrays)
   long long n = 0;
   long long n_caller = 0;  // unknowns in the caller's layout
@@ -822,6 +927,7 @@ static int request_plan(const sdft_system_desc* d, int32_t precision, std::uniqu
   q->NPt = pl->Pt;
   q->n_caller = pl->n_caller;
   q->M = pl->M;
+  q->BL = pl->BL;
   q->L = pl->L;
   q->NB = pl->NB;
   q->MB = pl->MB;
@@ -926,8 +1032,8 @@ extern "C" int sdft_request_destroy(sdft_handle h) {
 extern "C" int sdft_request_resident(sdft_handle h, int32_t* per_device) {
   if (!h || !per_device) return set_err(SDFT_ERR_ARG, "null argument");
   int ctas = 0, sms = 0;
-  CUDA_TRY(h->h.gen || (h->pending && h->pending->gen) ? occupancy_solve_gen(smem_bytes(h->M), &ctas)
-                                                      : occupancy_solve_pow2(smem_bytes(h->M), &ctas));
+  CUDA_TRY(h->h.gen || (h->pending && h->pending->gen) ? occupancy_solve_gen(smem_bytes(h->BL), &ctas)
+                                                      : occupancy_solve_pow2(smem_bytes(h->BL), &ctas));
   CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
   *per_device = ctas * sms;
   return SDFT_OK;
@@ -1043,7 +1149,7 @@ extern "C" int sdft_get_state(sdft_handle h, double* mu_ex_K, double* lng_K, dou
 extern "C" int sdft_objective(sdft_handle h, double* mu_ex_K, double* lng_K, double* Psi, double* PsiC) {
   if (!h) return set_err(SDFT_ERR_ARG, "null handle");
   if (int rc_ = request_ensure(h)) return rc_;
-  size_t sm = smem_bytes(h->M);
+  size_t sm = smem_bytes(h->BL);
   CUDA_TRY(launch_objective(h->h.gen != 0, h->dreq, sm, h->stream));
   int st = 0;
   CUDA_TRY(cudaMemcpyAsync(&st, h->h.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1085,7 +1191,7 @@ static int run_batch(sdft_handle* hs, int32_t n, const sdft_numerics* num, int32
   size_t sm = 0;
   bool any_pow2 = false, any_gen = false;
   for (int i = 0; i < n; i++) {
-    sm = std::max(sm, smem_bytes(hs[i]->M));
+    sm = std::max(sm, smem_bytes(hs[i]->BL));
     (hs[i]->h.gen ? any_gen : any_pow2) = true;
   }
   // device arrays and events of this batch, released on every return path
@@ -1446,7 +1552,7 @@ extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active
   for (int i = 0; i < sv->max_slots; i++)
     if (sv->owner[i]) {
       hi = i + 1;
-      sm = std::max(sm, smem_bytes(sv->owner[i]->M));
+      sm = std::max(sm, smem_bytes(sv->owner[i]->BL));
       (sv->owner[i]->h.gen ? any_gen : any_pow2) = true;
     }
   if (hi > 0) {
@@ -1527,7 +1633,7 @@ extern "C" int sdft_get_densities(sdft_handle h, double* const* rho_segments, do
 }
 
 static int run_omega(sdft_handle h, std::vector<double>& out) {
-  size_t sm = smem_bytes(h->M);
+  size_t sm = smem_bytes(h->BL);
   CUDA_TRY(launch_omega(h->h.gen != 0, h->dreq, h->dout, sm, h->stream));
   out.assign(1 + h->NS, 0.0);
   CUDA_TRY(cudaMemcpyAsync(out.data(), h->dout, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, h->stream));
@@ -1606,13 +1712,12 @@ int objective_noalloc(const sdft_system_desc* d, const double* x_dev, double* g_
   if (rc) return rc;
   char* base = static_cast<char*>(base_v);
   plan_tables(d, pl);
-  const int M = pl.M;
   std::vector<DSpecies> dsp;
   DReq r = plan_bind(d, pl, base, const_cast<double*>(x_dev), g_dev, dsp);  // x is read only in G(x)
   // the array keeps the previous call's contents: clear the region this call uses
   CUDA_TRY(cudaMemsetAsync(base, 0, pl.bytes, stream));
   CUDA_TRY(plan_upload(d, pl, base, r, dsp, stream));
-  size_t sm = smem_bytes(M);
+  size_t sm = smem_bytes(pl.BL);
   CUDA_TRY(launch_objective(pl.gen, (const DReq*)(base + pl.o_dreq), sm, stream));
   int st = 0;
   CUDA_TRY(cudaMemcpyAsync(&st, r.status, sizeof(int), cudaMemcpyDeviceToHost, stream));

@@ -20,34 +20,39 @@ def test_pow2_bin_width_gives_power_of_two_grids():
 
 
 def test_grid_supported_matches_the_device_rule():
-    """sdft_grid_supported (host-only): NP >= 16 whose FFT length (NP/2 for
-    even NP, NP for odd NP) has no prime factor above 61 and fits one CTA."""
+    """sdft_grid_supported (host-only): NP >= 16 whose FFT length M (NP/2 for
+    even NP, NP for odd NP) fits one CTA's shared memory: directly when M has no
+    prime factor above 61, else through Bluestein's chirp convolution of length
+    2^k >= 2M - 1 (at most 8192 points, so M <= 4096)."""
     from softdft_b200 import native
     ok = native.grid_supported
     assert [n for n in (8, 15, 16, 17, 1000, 1001, 1024, 16384) if ok(n)] == [16, 17, 1000, 1001, 1024, 16384]
-    assert not ok(1009)            # prime
-    assert not ok(2018)            # NP/2 = 1009
-    assert not ok(1002)            # NP/2 = 3 * 167
-    assert ok(2 * 61 * 64) and not ok(2 * 67 * 64)
+    assert ok(1009)                # prime: Bluestein over 2048 points
+    assert ok(2018)                # NP/2 = 1009
+    assert ok(1002)                # NP/2 = 3 * 167: Bluestein over 1024 points
+    assert ok(2 * 61 * 64)         # mixed radix
+    assert not ok(2 * 67 * 64)     # M = 4288 = 67 * 64: Bluestein over 16384 points, beyond one CTA
+    assert not ok(4099) and not ok(8198)  # M = 4099 (prime): the same
+    assert b"Bluestein transform of 16384 points" in native.lib().sdft_last_error()
     assert ok(24910) and not ok(32768)  # shared memory of one CTA
-    assert b"prime factor above 61" in native.lib().sdft_last_error() or not ok(1009)
 
 
 def test_supported_bin_width_keeps_the_reference_grid():
     # H = 20 sigma at dz = 0.02: the reference's NP = 1001 runs as is
     assert ct.supported_bin_width(20.0, 0.02) == 0.02
-    for H, dz in [(20.0, 0.02), (19.97, 0.05), (40.0, 40.0 / 8191), (10.16, 0.01)]:
+    for H, dz in [(20.0, 0.02), (19.97, 0.05), (40.0, 40.0 / 8191), (10.16, 0.01), (workloads.slit_length(4099, 0.01), 0.01)]:
         w = ct.supported_bin_width(H, dz)
         NP = cld(H, w) + 1
         from softdft_b200 import native
         assert native.grid_supported(NP) and w <= dz
         NP0 = cld(H, dz) + 1
         assert all(not native.grid_supported(n) for n in range(NP0, NP))
-    # 1009 points (prime) move to the next supported size, 1012 (NP/2 = 2 * 11 * 23)
-    H = 1008 * 0.01
-    assert cld(H, 0.01) + 1 == 1009
+    # 4099 points (prime, beyond a Bluestein transform in one CTA) move to the
+    # next supported size, 4100 (NP/2 = 2 * 5^2 * 41)
+    H = workloads.slit_length(4099, 0.01)
+    assert cld(H, 0.01) + 1 == 4099
     w = ct.supported_bin_width(H, 0.01)
-    assert cld(H, w) + 1 == 1012 and w < 0.01
+    assert cld(H, w) + 1 == 4100 and w < 0.01
 
 
 def test_set_distance_grid_policies():

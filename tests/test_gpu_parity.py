@@ -77,6 +77,10 @@ def _diblock_odd():
 
 
 CASES["diblock_1001"] = _diblock_odd()
+# lengths with a prime factor above 61: Bluestein's chirp convolution
+CASES["grid_1009_bluestein"] = small_slit(np_=1009, dz=0.02)        # M = 1009 (prime), 2048-point convolution
+CASES["grid_1002_bluestein"] = small_slit(np_=1002, dz=0.02)        # M = 501 = 3 * 167, 1024 points
+CASES["grid_2026_bluestein_mfmt_msa"] = small_slit(np_=2026, dz=0.01, models=["ideal", "mfmt", "msa"])  # M = 1013
 
 
 # branched chains (parse_topology.jl syntax: a parenthesised run is a side branch)
@@ -142,7 +146,7 @@ def test_picard_trajectory_matches():
 
 
 @pytest.mark.parametrize("name", ["acid_salt", "brush", "grid_1000", "brush_600", "grid_1001", "brush_999",
-                                  "branched_acid_mix5e-4", "branched_brush"])
+                                  "branched_acid_mix5e-4", "branched_brush", "grid_1009_bluestein"])
 def test_converged_state_matches(name):
     ds = copy.deepcopy(CASES[name])
     ds["numerical"]["tole"] = 1e-10
@@ -214,8 +218,8 @@ def test_batch_mixes_grid_kinds():
         assert rel(b.get_x(), x) == 0.0
 
 
-@pytest.mark.parametrize("np_,why", [(1009, "NP has a prime factor above 61"),
-                                     (1002, "NP/2 has a prime factor above 61")])
+@pytest.mark.parametrize("np_,why", [(4099, "Bluestein transform of 16384 points"),
+                                     (8198, "Bluestein transform of 16384 points")])
 def test_unsupported_grids_are_refused(np_, why):
     dft = descriptor(small_slit(np_=np_, dz=0.02))
     with pytest.raises(native.SdftError) as e:

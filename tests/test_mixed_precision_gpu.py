@@ -33,6 +33,8 @@ CASES = {
     "grid_1000": small_slit(np_=1000, dz=0.02),
     "grid_1001": small_slit(np_=1001, dz=0.02),
     "brush_999": workloads.grafted_brush(999, 0.05, 10, 0.05, 4.5, 7.0, 0.01),
+    # FP32 Bluestein transforms (M = 1009, prime)
+    "grid_1009_bluestein": small_slit(np_=1009, dz=0.02),
 }
 
 
