@@ -100,6 +100,150 @@ __device__ __forceinline__ void lsqr_pass(const double* __restrict__ gk, const d
   }
 }
 
+// Streams element pairs p = tid, tid + bd, ... < n2 through shared memory: each
+// thread copies its own pairs of up to A arrays (src(a) gives array a as double2,
+// nullptr: not read) into its own stage slots with cp.async, D pairs ahead, and
+// body(p, slots) reads them back as slots[a * blockDim.x].  A thread reads only
+// what it copied, so no barrier is needed, and the copies of the next D pairs
+// are in flight while the current one is combined (plain loads hold registers
+// until their first use, which caps them at about two pairs a thread here).
+// stage: D * A * blockDim.x double2 slots.
+template <int A, int D, class Src, class Body>
+__device__ __forceinline__ void staged_pairs(long long n2, double2* stage, Src src, Body body) {
+  const int bd = blockDim.x, tid = threadIdx.x;
+  auto issue = [&](long long p, int s) {
+    if (p < n2) {
+      double2* b = stage + (size_t)s * A * bd + tid;
+#pragma unroll
+      for (int a = 0; a < A; a++) {
+        const double2* g = src(a);
+        if (g) cp_async16(b + (size_t)a * bd, g + p);
+      }
+    }
+    cp_async_commit();  // an empty group past the end keeps the group count uniform
+  };
+#pragma unroll
+  for (int s = 0; s < D; s++) issue(tid + (long long)s * bd, s);
+  int s = 0;
+  for (long long p = tid; p < n2; p += bd) {
+    cp_async_wait<D - 1>();
+    body(p, static_cast<const double2*>(stage + (size_t)s * A * bd + tid));
+    // the slots of stage s were read and used by body
+    issue(p + (long long)D * bd, s);
+    s = s + 1 == D ? 0 : s + 1;
+  }
+  cp_async_wait<0>();
+}
+
+// lsqr_pass with its operands streamed through shared memory (staged_pairs):
+// slots g_k, u, the history columns
+template <int NC, int D>
+__device__ __forceinline__ void lsqr_pass_staged(const double* __restrict__ gk, const double* const* hc,
+                                                 double* __restrict__ u, long long n, int nc, const double* v,
+                                                 double coef, double* acc, double2* stage) {
+  const long long n2 = n >> 1;
+  double2* u2 = reinterpret_cast<double2*>(u);
+  const int bd = blockDim.x;
+  staged_pairs<NC + 2, D>(
+      n2, stage,
+      [&](int a) -> const double2* {
+        if (a == 0) return reinterpret_cast<const double2*>(gk);
+        if (a == 1) return u2;
+        return a - 2 < nc ? reinterpret_cast<const double2*>(hc[a - 2]) : nullptr;
+      },
+      [&](long long p, const double2* b) {
+        const double2 g = b[0];
+        double2 uu = b[bd];
+        double2 h[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          if (c < nc) h[c] = b[(size_t)(2 + c) * bd];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const double gq = e ? g.y : g.x;
+          const double uq = e ? uu.y : uu.x;
+          double aq[NC];
+          double av = 0.0;
+#pragma unroll
+          for (int c = 0; c < NC; c++)
+            if (c < nc) {
+              aq[c] = (e ? h[c].y : h[c].x) - gq;
+              av += aq[c] * v[c];
+            }
+          const double wq = coef * uq + av;
+          if (e) uu.y = wq;
+          else uu.x = wq;
+          acc[NC] += wq * wq;
+#pragma unroll
+          for (int c = 0; c < NC; c++)
+            if (c < nc) acc[c] += aq[c] * wq;
+        }
+        __stcg(u2 + p, uu);
+      });
+  if ((n & 1) && threadIdx.x == 0) {  // the last element of an odd length
+    const long long q = n - 1;
+    const double gq = gk[q];
+    double aq[NC];
+    double av = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) {
+        aq[c] = hc[c][q] - gq;
+        av += aq[c] * v[c];
+      }
+    const double wq = coef * u[q] + av;
+    u[q] = wq;
+    acc[NC] += wq * wq;
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      if (c < nc) acc[c] += aq[c] * wq;
+  }
+}
+
+// u = b - A x with b = -g_k and A[:, c] = G_hist[j_c] - g_k, its squared norm
+// (acc[NC]) and A^T u (acc[c]).  Thread t takes the elements t, t + bd, t + 2 bd,
+// ... in that order, U of them per round with every load issued before the first
+// use; the order of every sum is that of one element per round.
+template <int NC>
+__device__ __forceinline__ void lsqr_init_pass(const double* __restrict__ gk, const double* const* hc,
+                                               double* __restrict__ u, long long n, int nc, const double* x,
+                                               double* acc) {
+  constexpr int U = 4;
+  const int bd = blockDim.x;
+  for (long long q0 = threadIdx.x; q0 < n; q0 += (long long)U * bd) {
+    double g[U], h[U][NC];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const long long q = q0 + (long long)k * bd;
+      if (q >= n) continue;
+      g[k] = __ldcg(gk + q);
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        if (c < nc) h[k][c] = __ldcg(hc[c] + q);
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const long long q = q0 + (long long)k * bd;
+      if (q >= n) continue;
+      const double gq = g[k];
+      double aq[NC];
+      double ax = 0.0;
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        if (c < nc) {
+          aq[c] = h[k][c] - gq;
+          ax += aq[c] * x[c];
+        }
+      const double uq = -gq - ax;
+      __stcg(u + q, uq);
+      acc[NC] += uq * uq;
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        if (c < nc) acc[c] += aq[c] * uq;
+    }
+  }
+}
+
 // One sweep over the history serves each LSQR iteration: the next vector
 // w = A v - alpha u is stored unnormalised (u_true = uscale * u_stored) while
 // ||w||^2 and A^T w are accumulated in the same pass; A^T u_{i+1} = A^T w / beta
@@ -107,7 +251,8 @@ __device__ __forceinline__ void lsqr_pass(const double* __restrict__ gk, const d
 // order of the divisions by beta differs.  NC bounds the column count at
 // compile time so that the per-thread column values stay in registers.
 template <int NC>
-__device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, double* lam, double* red) {
+__device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, double* lam, double* red,
+                                              double2* stage, size_t stage_bytes) {
   const long long n = r.n, hs = r.hstride;
   const double* gk = r.hg + (size_t)col * hs;
   const double* hc[NC];
@@ -119,28 +264,15 @@ __device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, d
   const long long maxiter = n > nc ? n : nc;
   const double ctol = conlim > 0 ? 1.0 / conlim : 0.0;
   double v[NC], w[NC], acc[NC + 1], x[NC];
+  // pipeline depth of the staged passes that the shared-memory stage holds
+  const size_t per_stage = (size_t)(NC + 2) * blockDim.x * sizeof(double2);
+  const int depth = stage_bytes >= 3 * per_stage ? 3 : stage_bytes >= 2 * per_stage ? 2 : 0;
 #pragma unroll
   for (int c = 0; c < NC; c++) x[c] = c < nc ? lam[c] : 0.0;
   // u = b - A x with b = -g_k and A[:, c] = G_hist[j_c] - g_k; ||u||^2 and A^T u
 #pragma unroll
   for (int c = 0; c <= NC; c++) acc[c] = 0.0;
-  for (long long q = threadIdx.x; q < n; q += blockDim.x) {
-    const double gq = gk[q];
-    double aq[NC];
-    double ax = 0.0;
-#pragma unroll
-    for (int c = 0; c < NC; c++)
-      if (c < nc) {
-        aq[c] = hc[c][q] - gq;
-        ax += aq[c] * x[c];
-      }
-    const double uq = -gq - ax;
-    u[q] = uq;
-    acc[NC] += uq * uq;
-#pragma unroll
-    for (int c = 0; c < NC; c++)
-      if (c < nc) acc[c] += aq[c] * uq;
-  }
+  lsqr_init_pass<NC>(gk, hc, u, n, nc, x, acc);
   block_sum_vec<NC + 1>(acc, NC + 1, red);
   double beta = sqrt(acc[NC]);
   double uscale = beta > 0 ? 1.0 / beta : 1.0;
@@ -175,7 +307,9 @@ __device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, d
     const double coef = alpha * uscale;
 #pragma unroll
     for (int c = 0; c <= NC; c++) acc[c] = 0.0;
-    lsqr_pass<NC>(gk, hc, u, n, nc, v, -coef, acc);
+    if (depth == 3) lsqr_pass_staged<NC, 3>(gk, hc, u, n, nc, v, -coef, acc, stage);
+    else if (depth == 2) lsqr_pass_staged<NC, 2>(gk, hc, u, n, nc, v, -coef, acc, stage);
+    else lsqr_pass<NC>(gk, hc, u, n, nc, v, -coef, acc);
     block_sum_vec<NC + 1>(acc, NC + 1, red);
     beta = sqrt(acc[NC]);
     if (beta > 0) {
@@ -243,11 +377,12 @@ __device__ __noinline__ void lsqr_sweep_device(const DReq& r, int nc, int col, d
     if (c < nc) lam[c] = x[c];
 }
 
-__device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* red) {
+__device__ void lsqr_device(const DReq& r, int m, int col, double* lam, double* red, double2* stage,
+                            size_t stage_bytes) {
   const int nc = m - 1;
-  if (nc <= 4) lsqr_sweep_device<4>(r, nc, col, lam, red);
-  else if (nc <= 9) lsqr_sweep_device<9>(r, nc, col, lam, red);
-  else lsqr_sweep_device<kMaxAnderson - 1>(r, nc, col, lam, red);
+  if (nc <= 4) lsqr_sweep_device<4>(r, nc, col, lam, red, stage, stage_bytes);
+  else if (nc <= 9) lsqr_sweep_device<9>(r, nc, col, lam, red, stage, stage_bytes);
+  else lsqr_sweep_device<kMaxAnderson - 1>(r, nc, col, lam, red, stage, stage_bytes);
 }
 
 // x <- X_k + dX lambda + amix (g_k + dG lambda) over element pairs (AndersonMixing.jl:144),
@@ -313,9 +448,10 @@ __device__ __noinline__ void anderson_mix(const DReq& r, int nc, int col, const 
 }
 
 // One Anderson update after r.g = G(x).  Returns ST_RUNNING, ST_OK (converged
-// after this update) or ST_NONFINITE.
+// after this update) or ST_NONFINITE.  stage: shared memory free during the
+// update (the transform buffers), stage_bytes of it; 0 when there is none.
 __device__ int anderson_step(const DReq& r, const SolveCfg& cfg, int iter, AndersonState& st, double* red,
-                             double* err_out) {
+                             double2* stage, size_t stage_bytes, double* err_out) {
   const long long n = r.n, hs = r.hstride, n2 = n >> 1;
   const int m = cfg.anderm;
   const int col = (iter - 1) % m;
@@ -325,16 +461,26 @@ __device__ int anderson_step(const DReq& r, const SolveCfg& cfg, int iter, Ander
   const double* __restrict__ gv = r.g;
   double mx = 0.0;
   int bad = 0;
-  // ring-buffer column col: x and G(x) - x (AndersonMixing.jl:102-111), element pairs
-  for (long long p = threadIdx.x; p < n2; p += blockDim.x) {
-    const double2 xq = __ldcg(reinterpret_cast<const double2*>(xv) + p);
-    const double2 g2 = __ldcg(reinterpret_cast<const double2*>(gv) + p);
+  // ring-buffer column col: x and G(x) - x (AndersonMixing.jl:102-111), element
+  // pairs, streamed through the stage when it holds four rounds (the maximum and
+  // the finite test do not depend on the order)
+  auto column = [&](long long p, double2 xq, double2 g2) {
     const double2 gq = make_double2(g2.x - xq.x, g2.y - xq.y);
     __stcg(reinterpret_cast<double2*>(hxc) + p, xq);
     __stcg(reinterpret_cast<double2*>(hgc) + p, gq);
     const double a0 = fabs(gq.x), a1 = fabs(gq.y);
     if (!isfinite(a0) || !isfinite(a1)) bad = 1;
     mx = fmax(mx, fmax(a0, a1));
+  };
+  if (stage_bytes >= (size_t)4 * 2 * blockDim.x * sizeof(double2)) {
+    const int bd = blockDim.x;
+    staged_pairs<2, 4>(
+        n2, stage,
+        [&](int a) { return reinterpret_cast<const double2*>(a == 0 ? xv : gv); },
+        [&](long long p, const double2* b) { column(p, b[0], b[bd]); });
+  } else {
+    for (long long p = threadIdx.x; p < n2; p += blockDim.x)
+      column(p, __ldcg(reinterpret_cast<const double2*>(xv) + p), __ldcg(reinterpret_cast<const double2*>(gv) + p));
   }
   if ((n & 1) && threadIdx.x == 0) {
     const long long q = n - 1;
@@ -357,15 +503,23 @@ __device__ int anderson_step(const DReq& r, const SolveCfg& cfg, int iter, Ander
   if (iter < m || (err > cfg.switch_tole && st.use_picard)) {
     const double c1 = 1.0 - amix, c2 = amix;
     double* __restrict__ x = r.x;
-    for (long long p = threadIdx.x; p < n2; p += blockDim.x) {
-      const double2 xq = __ldcg(reinterpret_cast<const double2*>(x) + p);
-      const double2 gq = __ldcg(reinterpret_cast<const double2*>(gv) + p);
+    auto picard = [&](long long p, double2 xq, double2 gq) {
       __stcg(reinterpret_cast<double2*>(x) + p, make_double2(c1 * xq.x + c2 * gq.x, c1 * xq.y + c2 * gq.y));
+    };
+    if (stage_bytes >= (size_t)4 * 2 * blockDim.x * sizeof(double2)) {
+      const int bd = blockDim.x;
+      staged_pairs<2, 4>(
+          n2, stage,
+          [&](int a) { return reinterpret_cast<const double2*>(a == 0 ? x : gv); },
+          [&](long long p, const double2* b) { picard(p, b[0], b[bd]); });
+    } else {
+      for (long long p = threadIdx.x; p < n2; p += blockDim.x)
+        picard(p, __ldcg(reinterpret_cast<const double2*>(x) + p), __ldcg(reinterpret_cast<const double2*>(gv) + p));
     }
     if ((n & 1) && threadIdx.x == 0) x[n - 1] = c1 * x[n - 1] + c2 * gv[n - 1];
   } else {
     st.use_picard = 0;
-    lsqr_device(r, m, col, st.lam, red);
+    lsqr_device(r, m, col, st.lam, red, stage, stage_bytes);
     const int nc = m - 1;
     if (nc <= 4) anderson_mix<4>(r, nc, col, st.lam, amix);
     else if (nc <= 9) anderson_mix<9>(r, nc, col, st.lam, amix);

@@ -86,6 +86,7 @@ struct DReq {
   double dz, lB, total_charge;
   long long n;        // Anderson unknowns
   long long hstride;  // column stride of the Anderson histories: n rounded up to 32 (256-byte columns)
+  long long zbytes;   // shared memory of the transform buffers (free while the Anderson update runs)
   // per-bead / per-bond constants
   const double* sig;  // [NB]
   const double* z;    // [NB]
@@ -237,6 +238,19 @@ __device__ __forceinline__ void block_max2(double* a, double* b, double* red) {
   }
   *a = x;
   *b = y;
+}
+
+// 16-byte asynchronous global -> shared copies, completed per thread by commit
+// groups (cp.async.cg: cached in L2 only, as __ldcg); both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's commit groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // k sums at once (k <= 16): vals[k] in/out

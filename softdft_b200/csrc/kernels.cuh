@@ -64,6 +64,8 @@ extern "C" __global__ void __launch_bounds__(kThreads, kSolveCtasPerSm)
   AndersonState st;
   st.use_picard = sl->use_picard;
   for (int c = 0; c < kMaxAnderson; c++) st.lam[c] = sl->lam[c];
+  // the request's transform buffers, free while the Anderson update runs
+  const size_t zbytes = (size_t)r.zbytes;
   int iter = sl->iter;
   int status = ST_RUNNING;
   double err = sl->err;
@@ -76,7 +78,7 @@ extern "C" __global__ void __launch_bounds__(kThreads, kSolveCtasPerSm)
       status = ST_NORM;
       break;
     }
-    int s = anderson_step(r, cfg, iter, st, sh.red, &err);
+    int s = anderson_step(r, cfg, iter, st, sh.red, sh.z, zbytes, &err);
     if (s != ST_RUNNING) {
       status = s;
       break;
@@ -108,7 +110,7 @@ extern "C" __global__ void __launch_bounds__(kThreads) SDFT_KNAME(sdft_k_anderso
   for (int c = 0; c < kMaxAnderson; c++) st.lam[c] = sl->lam[c];
   const int iter = sl->iter + 1;
   double err = sl->err;
-  const int s = anderson_step(r, cfg, iter, st, smem, &err);
+  const int s = anderson_step(r, cfg, iter, st, smem, nullptr, 0, &err);  // launched without transform buffers
   if (threadIdx.x == 0) {
     sl->iter = iter;
     sl->status = s;

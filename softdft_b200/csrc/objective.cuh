@@ -411,8 +411,10 @@ struct FuseT {             // one transform of a fused chain step (shared memory
   const double* w;         // filtered bond kernel in C-space
   void* out;               // propagator slot written (R)
   int sweep;               // 0: child recursion, 1: parent recursion
-  int pad;
+  int sum;                 // register slot of the source sum (child jj, parent SM + jj), | kSumReused when an
+                           // earlier transform of the same pass set forms it
 };
+constexpr int kSumReused = 0x100;
 constexpr int kFuseOffset = 64;  // FuseT table position in Shared::red (doubles), after the reduction slots
 
 // exponent of the power of two that brings mx into [0.5, 1) when mx leaves
@@ -484,6 +486,7 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
         d.w = r.Wbond + (size_t)bond * P;
         d.out = gC + ((size_t)(p * S + ii) * S + jj) * P;
         d.sweep = 0;
+        d.sum = jj | (ii > 0 && jj / r.TB == q / r.TB ? kSumReused : 0);  // transform jj (ii = 0) sums it
       } else {  // parent pair (ii of c2, jj of p2)
         const int qq = q - nC, ii = qq / npP, jj = qq - ii * npP;
         const int si = s.states[c2 * S + ii], sj = s.states[p2 * S + jj];
@@ -495,8 +498,8 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
         d.w = r.Wbond + (size_t)bond * P;
         d.out = gP + ((size_t)(c2 * S + ii) * S + jj) * P;
         d.sweep = 1;
+        d.sum = (SM + jj) | (ii > 0 && (nC + jj) / r.TB == q / r.TB ? kSumReused : 0);
       }
-      d.pad = 0;
       fd[q] = d;
     }
     double mxC = 0.0, mxP = 0.0;  // largest output of each recursion at this step (this thread)
@@ -586,6 +589,7 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
           [&](int kp, auto put) {
             const int K = 2 * kp;
             double2 f[kMaxTB];
+            double2 qs[2 * SM];  // the source sums of this pair, by slot
 #pragma unroll
             for (int u = 0; u < kMaxTB; u++)
               if (u < nb) {
@@ -595,14 +599,26 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
                 const R2 fv = ldca2(reinterpret_cast<const R*>(d.fin) + K);
                 f[u] = make_double2((double)fv.x, (double)fv.y);
                 if (d.src) {
+                  // transforms (ii, jj) of one recursion share the source sum of jj:
+                  // it is formed once per pass set (the same sum, in the same order)
+                  const int slot = d.sum & (kSumReused - 1);
                   double2 q2 = make_double2(0.0, 0.0);
+                  if (d.sum & kSumReused) {
 #pragma unroll
-                  for (int q = 0; q < SM; q++)
-                    if (q < S) {
-                      const R2 v = ldcg2(reinterpret_cast<const R*>(d.src) + (size_t)q * P + K);
-                      q2.x += v.x;
-                      q2.y += v.y;
-                    }
+                    for (int k = 0; k < 2 * SM; k++)
+                      if (k == slot) q2 = qs[k];
+                  } else {
+#pragma unroll
+                    for (int q = 0; q < SM; q++)
+                      if (q < S) {
+                        const R2 v = ldcg2(reinterpret_cast<const R*>(d.src) + (size_t)q * P + K);
+                        q2.x += v.x;
+                        q2.y += v.y;
+                      }
+#pragma unroll
+                    for (int k = 0; k < 2 * SM; k++)
+                      if (k == slot) qs[k] = q2;
+                  }
                   f[u].x *= q2.x;
                   f[u].y *= q2.y;
                 }

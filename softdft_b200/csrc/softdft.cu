@@ -696,6 +696,7 @@ DReq plan_bind(const sdft_system_desc* d, const Plan& pl, char* base, double* x,
   r.total_charge = d->charged_walls ? d->wall_charge[0] + d->wall_charge[1] : 0.0;
   r.n = pl.n;
   r.hstride = pl.hstride;
+  r.zbytes = (long long)(smem_bytes(pl.BL) - sizeof(double) * kRedDoubles);
   r.sig = (const double*)at(pl.o_sig);
   r.z = (const double*)at(pl.o_z);
   r.dmu = (const double*)at(pl.o_dmu);
