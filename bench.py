@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling case: only batched solves capped at --max-iters, one short line out")
     ap.add_argument("--max-iters", type=int, default=0)
+    ap.add_argument("--profile-launches", type=int, default=1,
+                    help="profiling case through the serving loop: this many launches of --max-iters "
+                         "iterations each, so that a capture of a later launch sees the Anderson phase")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--workload", default="plain", choices=["plain", "uneven"],
@@ -313,6 +316,18 @@ def run_profile_case(args):
     num = numerics_from_dict(nd)
     B = args.batch if args.batch > 0 else 148
     systems = [native.DeviceSystem(dft.descriptor) for _ in range(B)]
+    if args.profile_launches > 1:
+        # one solve kernel launch per server step, each advancing every request
+        # by --max-iters iterations (the requests' own max_iters stays as specified)
+        srv = native.Server(numerics_from_dict(dict(ds["numerical"])), max_slots=B)
+        for i, s_ in enumerate(systems):
+            srv.submit(s_, i)
+        for _ in range(args.profile_launches):
+            active, _ = srv.step(args.max_iters)
+        srv.close()
+        print(json.dumps({"profile_case": name, "batch": B, "launches": args.profile_launches,
+                          "iters_per_launch": args.max_iters, "active_after": active}), flush=True)
+        return
     for _ in range(args.warmup + args.steps):
         iters, errs, status = native.solve_batch(systems, num)
     ms, nl, _ = native.last_batch_stats(B)

@@ -45,15 +45,35 @@ __device__ __forceinline__ double dist2_grid(int K, int c, double dz) {
 // ---------------------------------------------------------------------------
 // lambda_K = mu_ex_K + (Psi + PsiC) z + Ext + dmuH
 // ---------------------------------------------------------------------------
+// lambda and e^{-lambda}; each thread takes four elements a round, every load of
+// the round issued before the first use
 __device__ void stage_lambda(const DReq& r) {
-  const int P = r.NP;
+  constexpr int U = 4;
+  const int P = r.NP, total = r.NB * P, bd = blockDim.x;
   const double* mu = xs_mu(r, r.x);
   const double* psi = xs_psi(r, r.x);
   const double psic = r.x[off_psic(r)];
-  for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) {
-    int j = idx / P, K = idx - j * P;
-    double p = psi[K] + psic;
-    r.lambda[idx] = mu[idx] + p * r.z[j] + r.Ext[idx] + r.dmu[j];
+  for (int i0 = threadIdx.x; i0 < total; i0 += U * bd) {
+    double m[U], ps[U], ex[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const int idx = i0 + k * bd;
+      if (idx >= total) continue;
+      const int K = idx - (idx / P) * P;
+      m[k] = mu[idx];
+      ps[k] = psi[K];
+      ex[k] = r.Ext[idx];
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const int idx = i0 + k * bd;
+      if (idx >= total) continue;
+      const int j = idx / P;
+      const double p = ps[k] + psic;
+      const double lam = m[k] + p * r.z[j] + ex[k] + r.dmu[j];
+      r.lambda[idx] = lam;
+      r.elam[idx] = exp(-lam);
+    }
   }
   __syncthreads();
 }
@@ -72,25 +92,35 @@ __device__ void stage_lambda(const DReq& r) {
 // (its outputs are the true propagators times 2^-(sc+so); the grafted
 // segment's local sums are shifted to match).
 __device__ void stage_bond_factors(const DReq& r, Shared sh, bool fp32) {
-  const int P = r.NP, nbe = 2 * r.MB;
+  constexpr int U = 4;  // elements a round per thread, loads issued before the first use
+  const int P = r.NP, nbe = 2 * r.MB, total = nbe * P, bd = blockDim.x, Pt = grid_points(r);
   const double* lng = xs_lng(r, r.x);
-  double mx = 0.0;
-  for (int idx = threadIdx.x; idx < nbe * P; idx += blockDim.x) {
-    const int be = idx / P, K = idx - be * P;
-    const int j = r.bonds[be];
-    const double l = lng[idx];
-    const double fin = exp(-r.lambda[(size_t)j * P + K] + l / 2.0) * r.trapez[(size_t)j * P + K];
-    r.fbe[idx] = fin;
-    r.fbe[(size_t)nbe * P + idx] = exp(l / 2.0);
-    if (K < grid_points(r) && isfinite(fin)) mx = fmax(mx, fin);
+  double mx = 0.0, mo = 0.0;  // largest input factor and output factor e^{lng/2}
+  for (int i0 = threadIdx.x; i0 < total; i0 += U * bd) {
+    double l[U], lam[U], tr[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const int idx = i0 + k * bd;
+      if (idx >= total) continue;
+      const int be = idx / P, K = idx - be * P;
+      const int j = r.bonds[be];
+      l[k] = lng[idx];
+      lam[k] = r.lambda[(size_t)j * P + K];
+      tr[k] = r.trapez[(size_t)j * P + K];
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const int idx = i0 + k * bd;
+      if (idx >= total) continue;
+      const int K = idx - (idx / P) * P;
+      const double fin = exp(-lam[k] + l[k] / 2.0) * tr[k];
+      const double fo = exp(l[k] / 2.0);
+      r.fbe[idx] = fin;
+      r.fbe[(size_t)nbe * P + idx] = fo;
+      if (K < Pt && isfinite(fin)) mx = fmax(mx, fin);
+      if (K < Pt && isfinite(fo)) mo = fmax(mo, fo);
+    }
   }
-  double mo = 0.0;  // largest output factor e^{lng/2}
-  for (int idx = threadIdx.x; idx < nbe * P; idx += blockDim.x) {
-    const int K = idx - (idx / P) * P;
-    const double fo = r.fbe[(size_t)nbe * P + idx];
-    if (K < grid_points(r) && isfinite(fo)) mo = fmax(mo, fo);
-  }
-  for (int idx = threadIdx.x; idx < r.NB * P; idx += blockDim.x) r.elam[idx] = exp(-r.lambda[idx]);
   if (fp32 && r.fbe32) {
     block_max2(&mx, &mo, sh.red);
     int sc = 0, so = 0;
@@ -411,10 +441,8 @@ struct FuseT {             // one transform of a fused chain step (shared memory
   const double* w;         // filtered bond kernel in C-space
   void* out;               // propagator slot written (R)
   int sweep;               // 0: child recursion, 1: parent recursion
-  int sum;                 // register slot of the source sum (child jj, parent SM + jj), | kSumReused when an
-                           // earlier transform of the same pass set forms it
+  int pad;
 };
-constexpr int kSumReused = 0x100;
 constexpr int kFuseOffset = 64;  // FuseT table position in Shared::red (doubles), after the reduction slots
 
 // exponent of the power of two that brings mx into [0.5, 1) when mx leaves
@@ -486,7 +514,6 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
         d.w = r.Wbond + (size_t)bond * P;
         d.out = gC + ((size_t)(p * S + ii) * S + jj) * P;
         d.sweep = 0;
-        d.sum = jj | (ii > 0 && jj / r.TB == q / r.TB ? kSumReused : 0);  // transform jj (ii = 0) sums it
       } else {  // parent pair (ii of c2, jj of p2)
         const int qq = q - nC, ii = qq / npP, jj = qq - ii * npP;
         const int si = s.states[c2 * S + ii], sj = s.states[p2 * S + jj];
@@ -498,8 +525,8 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
         d.w = r.Wbond + (size_t)bond * P;
         d.out = gP + ((size_t)(c2 * S + ii) * S + jj) * P;
         d.sweep = 1;
-        d.sum = (SM + jj) | (ii > 0 && (nC + jj) / r.TB == q / r.TB ? kSumReused : 0);
       }
+      d.pad = 0;
       fd[q] = d;
     }
     double mxC = 0.0, mxP = 0.0;  // largest output of each recursion at this step (this thread)
@@ -589,7 +616,6 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
           [&](int kp, auto put) {
             const int K = 2 * kp;
             double2 f[kMaxTB];
-            double2 qs[2 * SM];  // the source sums of this pair, by slot
 #pragma unroll
             for (int u = 0; u < kMaxTB; u++)
               if (u < nb) {
@@ -599,26 +625,14 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
                 const R2 fv = ldca2(reinterpret_cast<const R*>(d.fin) + K);
                 f[u] = make_double2((double)fv.x, (double)fv.y);
                 if (d.src) {
-                  // transforms (ii, jj) of one recursion share the source sum of jj:
-                  // it is formed once per pass set (the same sum, in the same order)
-                  const int slot = d.sum & (kSumReused - 1);
                   double2 q2 = make_double2(0.0, 0.0);
-                  if (d.sum & kSumReused) {
 #pragma unroll
-                    for (int k = 0; k < 2 * SM; k++)
-                      if (k == slot) q2 = qs[k];
-                  } else {
-#pragma unroll
-                    for (int q = 0; q < SM; q++)
-                      if (q < S) {
-                        const R2 v = ldcg2(reinterpret_cast<const R*>(d.src) + (size_t)q * P + K);
-                        q2.x += v.x;
-                        q2.y += v.y;
-                      }
-#pragma unroll
-                    for (int k = 0; k < 2 * SM; k++)
-                      if (k == slot) qs[k] = q2;
-                  }
+                  for (int q = 0; q < SM; q++)
+                    if (q < S) {
+                      const R2 v = ldcg2(reinterpret_cast<const R*>(d.src) + (size_t)q * P + K);
+                      q2.x += v.x;
+                      q2.y += v.y;
+                    }
                   f[u].x *= q2.x;
                   f[u].y *= q2.y;
                 }
