@@ -409,6 +409,7 @@ def run_serving(native, slots: int, n_requests: int, rate: float, iters_per_step
     pick = [int(k) for k in rng.integers(0, len(pts), size=n_requests)]
     arrivals = poisson_arrivals(n_requests, rate, seed + 2)
     srv = native.Server(num, max_slots=slots)
+    srv.set_pipeline(True)  # host work between steps overlaps the launch in flight
     backend = StreamBackend(native, srv, [dft.descriptor for _, dft in pts])
     res = serve_stream(backend, pick, arrivals, iters_per_step)
     srv.close()

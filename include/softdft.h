@@ -129,6 +129,16 @@ void sdft_numerics_default(sdft_numerics* out);
  * (src/iDFT/setup/setup_steps/process_guess.jl:5-54) on the device. */
 int sdft_request_create(const sdft_system_desc* desc, int32_t precision, sdft_handle* out);
 int sdft_request_destroy(sdft_handle h);
+/* Device memory of destroyed requests is cached by the library for later
+ * requests of a size it covers (a cudaFree synchronises the whole device, and a
+ * server retires and admits requests at every step).  A request takes the
+ * smallest cached block of its device that holds it with at most a quarter to
+ * spare; a failed device allocation releases the device's cache and is tried
+ * once more.  sdft_release_cached_memory returns the cached blocks of the
+ * current device to the driver and *bytes (may be NULL) says how many bytes
+ * that was.  No reference counterpart (Julia's GC owns the reference's
+ * arrays). */
+int sdft_release_cached_memory(int64_t* bytes);
 /* A request without device memory yet: the descriptor is validated and the
  * host tables are built as by sdft_request_create, and the handle keeps them;
  * the device memory (sdft_request_sizes' device_bytes) is taken when the
@@ -250,6 +260,13 @@ int sdft_server_step(sdft_server_t server, int32_t iters, int32_t* active, int32
 int sdft_server_poll(sdft_server_t server, int64_t* tags, int32_t* status, int32_t* iters, double* errs,
                      double* device_ms, int32_t max, int32_t* n);
 int sdft_server_set_reserve(sdft_server_t server, int64_t reserve_bytes);
+/* sdft_server_set_pipeline: with on != 0, sdft_server_step returns once its
+ * launch is queued, and the requests that finish in that launch are retired
+ * (and reported by sdft_server_poll) at the next sdft_server_step, so that the
+ * caller's host work between steps (preparing arrivals, reading results back)
+ * overlaps the GPU.  A request's state does not depend on the mode.  Off by
+ * default; turning it off collects the launch in flight. */
+int sdft_server_set_pipeline(sdft_server_t server, int32_t on);
 
 /* ---- bulk (iLST) state evaluation on the host --------------------------------
  * One evaluation of the bulk residual's expensive steps, for the host solve of

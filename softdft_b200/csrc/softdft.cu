@@ -16,6 +16,8 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -822,6 +824,54 @@ cudaError_t plan_upload(const sdft_system_desc* d, const Plan& pl, char* base, c
 
 }  // namespace
 
+// ---- device blocks of destroyed requests ----
+// Kept for later requests instead of going back through cudaFree, which
+// synchronises the whole device (a server that retires and admits requests at
+// every step would stall the GPU once per request); cudaMalloc can synchronise
+// too.  Keyed by device; a request takes the smallest cached block that holds it
+// with at most a quarter to spare.
+namespace {
+struct BlockCache {
+  std::mutex mu;
+  std::map<int, std::multimap<size_t, char*>> blocks;  // device -> (bytes, block)
+};
+BlockCache& block_cache() {
+  static BlockCache c;
+  return c;
+}
+bool block_fits(size_t have, size_t need) { return have >= need && have - need <= need / 4; }
+// a cached block of dev for need bytes (its size in *got), or nullptr; take=false only looks
+char* cache_find(int dev, size_t need, size_t* got, bool take) {
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  auto& m = c.blocks[dev];
+  auto it = m.lower_bound(need);
+  if (it == m.end() || !block_fits(it->first, need)) return nullptr;
+  char* p = it->second;
+  if (got) *got = it->first;
+  if (take) m.erase(it);
+  return p;
+}
+void cache_put(int dev, char* p, size_t bytes) {
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  c.blocks[dev].emplace(bytes, p);
+}
+// frees the cached blocks of dev (the current device); returns their bytes
+size_t cache_release(int dev) {
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  size_t total = 0;
+  auto& m = c.blocks[dev];
+  for (auto& kv : m) {
+    cudaFree(kv.second);
+    total += kv.first;
+  }
+  m.clear();
+  return total;
+}
+}  // namespace
+
 struct sdft_request {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -834,6 +884,7 @@ struct sdft_request {
   std::vector<SpeciesHost> sp;
   char* dmem = nullptr;
   size_t bytes = 0;
+  size_t dbytes = 0;       // size of the device block (a cached block may be larger than bytes)
   DReq h{};            // host copy of the device descriptor
   DReq* dreq = nullptr;
   SolveSlot* dslot = nullptr;
@@ -886,11 +937,23 @@ extern "C" void sdft_numerics_default(sdft_numerics* o) {
 // device placement of a request: one allocation for the plan, its tables
 // uploaded and the initial guess in x; the request's stream exists already
 static int request_place(sdft_request* q, const sdft_system_desc* d, Plan& pl) {
-  cudaError_t e = cudaMalloc(&q->dmem, pl.bytes);
-  if (e != cudaSuccess) {
-    q->dmem = nullptr;
-    cudaGetLastError();  // the failed allocation leaves no sticky error
-    return set_err(SDFT_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  size_t got = 0;
+  q->dmem = cache_find(q->device, pl.bytes, &got, true);
+  if (q->dmem) {
+    q->dbytes = got;
+  } else {
+    cudaError_t e = cudaMalloc(&q->dmem, pl.bytes);
+    if (e != cudaSuccess) {  // give the cached blocks back to the driver and try once more
+      cudaGetLastError();    // the failed allocation leaves no sticky error
+      cache_release(q->device);
+      e = cudaMalloc(&q->dmem, pl.bytes);
+    }
+    if (e != cudaSuccess) {
+      q->dmem = nullptr;
+      cudaGetLastError();
+      return set_err(SDFT_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    q->dbytes = pl.bytes;
   }
   cudaError_t ce = cudaMemsetAsync(q->dmem, 0, pl.bytes, q->stream);
   std::vector<DSpecies> dsp;
@@ -1023,10 +1086,26 @@ extern "C" int sdft_request_prepare(const sdft_system_desc* d, int32_t precision
 
 extern "C" int sdft_request_destroy(sdft_handle h) {
   if (!h) return SDFT_OK;
-  cudaStreamSynchronize(h->stream);
-  if (h->dmem) cudaFree(h->dmem);
+  // the request's own work is complete (batch solves and server steps
+  // synchronise their streams before they return): its block is idle
+  const cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (h->dmem) {
+    if (e == cudaSuccess) cache_put(h->device, h->dmem, h->dbytes);
+    else cudaFree(h->dmem);
+  }
   cudaStreamDestroy(h->stream);
   delete h;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_release_cached_memory(int64_t* bytes) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(SDFT_ERR_CUDA, "no CUDA device");
+  }
+  const size_t b = cache_release(dev);
+  if (bytes) *bytes = (int64_t)b;
   return SDFT_OK;
 }
 
@@ -1448,6 +1527,13 @@ struct sdft_server {
   long long bytes_active = 0;
   long long reserve = 0;  // device bytes admission leaves free (requests placed at admission)
   int active = 0;
+  // pipelined stepping: a step returns once its launch is queued; the launch's
+  // slot states come back into pin (pinned, so that the copy is asynchronous)
+  // and are collected at the next step
+  bool pipeline = false;
+  bool inflight = false;
+  int hi_launched = 0;
+  SolveSlot* pin = nullptr;
   struct Done {
     long long tag;
     int status, iters;
@@ -1473,8 +1559,10 @@ extern "C" int sdft_server_create(const sdft_numerics* num, int32_t max_slots, i
   cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&sv->dreqs, sizeof(DReq) * max_slots);
   if (e == cudaSuccess) e = cudaMalloc(&sv->dslots, sizeof(SolveSlot) * max_slots);
+  if (e == cudaSuccess) e = cudaMallocHost(&sv->pin, sizeof(SolveSlot) * max_slots);
   if (e != cudaSuccess) {
     if (sv->dreqs) cudaFree(sv->dreqs);
+    if (sv->dslots) cudaFree(sv->dslots);
     if (sv->stream) cudaStreamDestroy(sv->stream);
     delete sv;
     return set_err(SDFT_ERR_OOM, std::string("server allocation: ") + cudaGetErrorString(e));
@@ -1494,6 +1582,7 @@ extern "C" int sdft_server_destroy(sdft_server_t sv) {
   cudaStreamSynchronize(sv->stream);
   cudaFree(sv->dreqs);
   cudaFree(sv->dslots);
+  cudaFreeHost(sv->pin);
   cudaStreamDestroy(sv->stream);
   delete sv;
   return SDFT_OK;
@@ -1507,9 +1596,46 @@ extern "C" int sdft_server_submit(sdft_server_t sv, sdft_handle h, int64_t tag) 
   return SDFT_OK;
 }
 
+// waits for the launch in flight and retires the requests that finished in it
+static int server_collect(sdft_server* sv) {
+  if (!sv->inflight) return SDFT_OK;
+  sv->inflight = false;
+  CUDA_TRY(cudaStreamSynchronize(sv->stream));
+  const int hi = sv->hi_launched;
+  std::memcpy(sv->hslot.data(), sv->pin, sizeof(SolveSlot) * hi);
+  for (int i = 0; i < hi; i++) {
+    if (!sv->owner[i] || sv->hslot[i].status == ST_RUNNING) continue;
+    sdft_server::Done d;
+    d.tag = sv->tag[i];
+    d.status = slot_status_to_rc(sv->hslot[i].status);
+    d.iters = sv->hslot[i].iter;
+    d.err = sv->hslot[i].err;
+    d.device_ms = (double)(sv->hslot[i].t1 - sv->hslot[i].t0) * 1e-6;
+    sv->done.push_back(d);
+    sv->bytes_active -= (long long)sv->owner[i]->bytes;
+    sv->owner[i] = nullptr;
+    sv->hslot[i].status = -1;
+    sv->active--;
+  }
+  return SDFT_OK;
+}
+
+extern "C" int sdft_server_set_pipeline(sdft_server_t sv, int32_t on) {
+  if (!sv) return set_err(SDFT_ERR_ARG, "null server");
+  if (!on) {
+    const int rc = server_collect(sv);
+    if (rc) return rc;
+  }
+  sv->pipeline = on != 0;
+  return SDFT_OK;
+}
+
 extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active, int32_t* queued) {
   if (!sv) return set_err(SDFT_ERR_ARG, "null server");
   if (iters < 1) return set_err(SDFT_ERR_ARG, "iters must be >= 1");
+  // the previous launch of a pipelined server finishes first
+  int rc0 = server_collect(sv);
+  if (rc0) return rc0;
   // admission: FIFO into free slots within the byte budget; a prepared request
   // (sdft_request_prepare) is placed on the device here, once the free device
   // memory less the reserve covers it, else it waits for retirements
@@ -1520,10 +1646,13 @@ extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active
     sdft_handle h = sv->queue.front().first;
     const long long tag = sv->queue.front().second;
     if (sv->max_bytes > 0 && sv->bytes_active + (long long)h->bytes > sv->max_bytes) break;
-    if (h->pending) {
+    if (h->pending && !cache_find(h->device, h->bytes, nullptr, false)) {
+      // a cached block would take no free device memory; a new one must leave the reserve
       size_t fr = 0, tot = 0;
       CUDA_TRY(cudaMemGetInfo(&fr, &tot));
       if ((long long)fr - (long long)h->bytes < sv->reserve) break;
+    }
+    if (h->pending) {
       const int rc = request_ensure(h);
       if (rc == SDFT_ERR_OOM) break;  // another allocation took the memory: retry at the next step
       if (rc) {                       // the request cannot be placed: it completes with that status
@@ -1569,21 +1698,12 @@ extern "C" int sdft_server_step(sdft_server_t sv, int32_t iters, int32_t* active
     cfg.mixed_switch = mixed_switch(&sv->num);
     int launched = 0;
     CUDA_TRY(launch_solve(any_pow2, any_gen, sv->dreqs, sv->dslots, cfg, iters, hi, sm, sv->stream, &launched));
-    CUDA_TRY(cudaMemcpyAsync(sv->hslot.data(), sv->dslots, sizeof(SolveSlot) * hi, cudaMemcpyDeviceToHost, sv->stream));
-    CUDA_TRY(cudaStreamSynchronize(sv->stream));
-    for (int i = 0; i < hi; i++) {
-      if (!sv->owner[i] || sv->hslot[i].status == ST_RUNNING) continue;
-      sdft_server::Done d;
-      d.tag = sv->tag[i];
-      d.status = slot_status_to_rc(sv->hslot[i].status);
-      d.iters = sv->hslot[i].iter;
-      d.err = sv->hslot[i].err;
-      d.device_ms = (double)(sv->hslot[i].t1 - sv->hslot[i].t0) * 1e-6;
-      sv->done.push_back(d);
-      sv->bytes_active -= (long long)sv->owner[i]->bytes;
-      sv->owner[i] = nullptr;
-      sv->hslot[i].status = -1;
-      sv->active--;
+    CUDA_TRY(cudaMemcpyAsync(sv->pin, sv->dslots, sizeof(SolveSlot) * hi, cudaMemcpyDeviceToHost, sv->stream));
+    sv->hi_launched = hi;
+    sv->inflight = true;
+    if (!sv->pipeline) {  // retire now; a pipelined server retires at the next step
+      const int rc = server_collect(sv);
+      if (rc) return rc;
     }
   }
   if (active) *active = sv->active;

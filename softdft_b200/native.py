@@ -30,13 +30,21 @@ EXPORTS = ["sdft_abi_version", "sdft_last_error", "sdft_device_count", "sdft_num
            "sdft_grid_supported", "sdft_input_from_yaml", "sdft_input_descriptor", "sdft_input_numerics",
            "sdft_input_bulk_stats", "sdft_input_destroy", "sdft_get_solver_state", "sdft_set_solver_state",
            "sdft_solve_resume", "sdft_anderson_step", "sdft_request_prepare", "sdft_server_set_reserve",
-           "sdft_request_resident"]
+           "sdft_request_resident", "sdft_release_cached_memory", "sdft_server_set_pipeline"]
 
 
 class SdftError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
         self.code = code
+
+
+def release_cached_memory() -> int:
+    """Return the device blocks that the library caches from destroyed requests
+    to the driver (sdft_release_cached_memory); the number of bytes released."""
+    b = C.c_int64()
+    _check(lib().sdft_release_cached_memory(C.byref(b)))
+    return int(b.value)
 
 
 def grid_supported(np_: int) -> bool:
@@ -67,6 +75,8 @@ def lib():
         L.sdft_request_create.argtypes = [vp, C.c_int32, C.POINTER(vp)]
         L.sdft_request_prepare.argtypes = [vp, C.c_int32, C.POINTER(vp)]
         L.sdft_server_set_reserve.argtypes = [vp, C.c_int64]
+        L.sdft_server_set_pipeline.argtypes = [vp, C.c_int32]
+        L.sdft_release_cached_memory.argtypes = [C.POINTER(C.c_int64)]
         L.sdft_request_destroy.argtypes = [vp]
         L.sdft_request_sizes.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.sdft_set_state.argtypes = [vp, vp, vp, vp, vp]
@@ -280,6 +290,12 @@ class Server:
     def set_reserve(self, reserve_bytes: int) -> None:
         """Device bytes that admission leaves free (sdft_server_set_reserve)."""
         _check(lib().sdft_server_set_reserve(self.h, int(reserve_bytes)))
+
+    def set_pipeline(self, on: bool) -> None:
+        """Pipelined stepping (sdft_server_set_pipeline): a step returns once its
+        launch is queued, and that launch's finished requests are reported after
+        the next step."""
+        _check(lib().sdft_server_set_pipeline(self.h, 1 if on else 0))
 
     def submit(self, system: "DeviceSystem", tag: int) -> None:
         _check(lib().sdft_server_submit(self.h, system.h, int(tag)))

@@ -24,7 +24,8 @@ def _cases():
     return [small_slit(pH=pH, salt=salt, n_chain=n) for pH, salt, n in pts]
 
 
-def test_results_alone_equal_results_in_the_mix():
+@pytest.mark.parametrize("pipelined", [False, True])
+def test_results_alone_equal_results_in_the_mix(pipelined):
     cases = _cases()
     numd = dict(cases[0]["numerical"], tole=1e-8, max_iters=5000)
     num = numerics_from_dict(numd)
@@ -40,6 +41,7 @@ def test_results_alone_equal_results_in_the_mix():
         alone.append((s.get_x(), it, rc))
     assert sum(a[2] == 0 for a in alone) >= 3, [a[1:] for a in alone]
     srv = native.Server(num, max_slots=3)
+    srv.set_pipeline(pipelined)
     systems = [native.DeviceSystem(d.descriptor) for d in dfts]
     # staggered submission: two now, the rest while those run
     srv.submit(systems[0], 0)
@@ -88,8 +90,9 @@ def test_admission_follows_free_device_memory():
     """Prepared requests take device memory only at admission, and only while
     the free device memory less the server's reserve covers them: with a
     reserve that leaves room for two requests, at most two are active, the
-    queue waits for retirements (each finished request is destroyed, which
-    returns its memory), and every request ends in the state of its solve alone."""
+    queue waits for retirements (each finished request is destroyed, and its
+    block, kept in the library's cache, serves the next one), and every
+    request ends in the state of its solve alone."""
     import torch
 
     cases = [small_slit(np_=4096, dz=0.005, pH=pH, n_chain=6) for pH in (6.0, 7.0, 8.0, 9.0, 7.5)]
@@ -110,6 +113,7 @@ def test_admission_follows_free_device_memory():
     one = max(s.device_bytes for s in prepared)
     assert one > 16 * 2 ** 20  # large against the 2 MiB allocation granularity
     srv = native.Server(num, max_slots=8)
+    native.release_cached_memory()  # the solves above left their blocks in the library's cache
     free0, _ = torch.cuda.mem_get_info()
     srv.set_reserve(int(free0 - 2.5 * one))
     for i, s in enumerate(prepared):
