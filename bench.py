@@ -61,12 +61,15 @@ def parse():
                          "iterations each, so that a capture of a later launch sees the Anderson phase")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
-    ap.add_argument("--workload", default="plain", choices=["plain", "uneven"],
-                    help="uneven: a seeded batch of slits of different grids and chains in one launch sequence")
+    ap.add_argument("--workload", default="plain", choices=["plain", "uneven", "serving-mixed"],
+                    help="uneven: a seeded batch of slits of different grids and chains in one launch sequence; "
+                         "serving-mixed: a Poisson stream of slits of different grids and chain lengths, each "
+                         "built on the host at arrival")
     ap.add_argument("--uneven-n", type=int, default=148)
     ap.add_argument("--uneven-np", type=str, default="1024,4096", help="log-uniform grid range (powers of two)")
     ap.add_argument("--uneven-chain", type=str, default="10,60", help="uniform chain-length range")
-    ap.add_argument("--uneven-dump", type=str, default="", help="write per-request status and iterations (JSON)")
+    ap.add_argument("--uneven-dump", type=str, default="",
+                    help="uneven and serving-mixed: write per-request status and iterations (JSON)")
     ap.add_argument("--serve-requests", type=int, default=1500)
     ap.add_argument("--serve-rate", type=float, default=100.0, help="offered requests/s of the serving stream")
     ap.add_argument("--serve-iters", type=int, default=25, help="Anderson iterations per server launch")
@@ -426,6 +429,84 @@ def run_serving(native, slots: int, n_requests: int, rate: float, iters_per_step
                    "state per distinct point computed once"}
 
 
+class ArrivalBackend(StreamBackend):
+    """StreamBackend whose requests are built at arrival: the bulk state
+    (iLST), the descriptor and the host tables are made when the request
+    arrives, so that a request's latency covers its whole host setup."""
+
+    def __init__(self, native, srv, dss):
+        super().__init__(native, srv, [])
+        self.dss = dss
+
+    def submit(self, point: int, tag: int):
+        from softdft_b200.api import setup_request
+        dft = setup_request(copy.deepcopy(self.dss[point]))
+        s = self.native.DeviceSystem(dft.descriptor, prepare=True)
+        self.held[tag] = s
+        self.srv.submit(s, tag)
+
+
+def run_serving_mixed(args):
+    """A stream shaped like the mixed-request serving configuration, within the
+    grids one CTA holds: weak-polyacid slits with NP log-uniform over
+    {1024, 2048, 4096} (dz = 0.02), chain length log-uniform in [10, 200],
+    pH U(5, 9) and salt log-U(10 mM, 0.3 M), arriving as a Poisson stream.
+    Every request is a distinct parameter point built at arrival; requests
+    that the reference driver does not bring to the tolerance end with their
+    status and are counted, not dropped."""
+    import numpy as np
+
+    from softdft_b200 import native, workloads
+    from softdft_b200.host.descriptor import numerics_from_dict
+    from softdft_b200.serving import poisson_arrivals, serve_stream
+    rng = np.random.default_rng(17)
+    n = args.serve_requests
+    dss, nps, chains = [], [], []
+    for _ in range(n):
+        np_ = int(2 ** rng.integers(10, 13))
+        n_chain = int(round(10 ** rng.uniform(1.0, np.log10(200.0))))
+        pH = float(rng.uniform(5.0, 9.0))
+        salt = float(10 ** rng.uniform(-2.0, np.log10(0.3)))
+        dss.append(workloads.weak_acid_slit(np_, 0.02, n_chain, 4.5, pH, salt, 0.3))
+        nps.append(np_)
+        chains.append(n_chain)
+    nd = dict(dss[0]["numerical"], max_iters=args.max_iters if args.max_iters > 0 else 3000)
+    for ds in dss:
+        ds["numerical"] = dict(nd)
+    num = numerics_from_dict(nd)
+    arrivals = poisson_arrivals(n, args.serve_rate, 19)
+    srv = native.Server(num, max_slots=296)
+    srv.set_pipeline(True)
+    backend = ArrivalBackend(native, srv, dss)
+    res = serve_stream(backend, list(range(n)), arrivals, args.serve_iters)
+    srv.close()
+    st = res["status"]
+    ok = st == 0
+    lat = res["latency_ms"]
+    out = {"metric": "serving stream of mixed slits: converged solves/s and latency", "workload": "serving-mixed",
+           "requests": n, "offered_rate": args.serve_rate, "solves_per_s": float(np.sum(ok)) / res["wall_s"],
+           "requests_per_s": res["solves_per_s"], "wall_s": res["wall_s"], "launches": res["steps"],
+           "status": {"converged": int(np.sum(ok)), "max_iters": int(np.sum(st == 1)),
+                      "non_finite": int(np.sum(st == 7)), "other": int(np.sum((st != 0) & (st != 1) & (st != 7)))},
+           "latency_ms_converged": {"p50": float(np.percentile(lat[ok], 50)) if ok.any() else None,
+                                    "p99": float(np.percentile(lat[ok], 99)) if ok.any() else None},
+           "latency_ms_all": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+           "iterations_converged": {"min": int(res["iters"][ok].min()) if ok.any() else None,
+                                    "max": int(res["iters"][ok].max()) if ok.any() else None,
+                                    "mean": float(res["iters"][ok].mean()) if ok.any() else None},
+           "mix": {"np": sorted(set(nps)), "n_chain": [min(chains), max(chains)], "max_iters": nd["max_iters"],
+                   "iters_per_step": args.serve_iters, "slots": 296},
+           "latency_covers": "host bulk state and request build at arrival, queueing, device placement, solve, "
+                             "density readback",
+           "dtype": "f64", "data": "synthetic", "n_gpus": 1}
+    if args.uneven_dump:
+        rows = [{"np": nps[i], "n_chain": chains[i], "status": int(st[i]), "iters": int(res["iters"][i]),
+                 "latency_ms": float(lat[i])} for i in range(n)]
+        with open(args.uneven_dump, "w") as fh:
+            json.dump({"seed": 17, "rows": rows}, fh)
+    print(json.dumps(out), flush=True)
+
+
 def run_uneven(args):
     """Uneven batch: independent slits with NP log-uniform (rounded to powers of
     two), chain length, pH U(2,12), salt log-U(1 mM, 1 M) and packing U(0.1,0.4)
@@ -652,6 +733,8 @@ def main():
             run_profile_case(args)
         elif args.workload == "uneven" and args.impl == "ours":
             run_uneven(args)
+        elif args.workload == "serving-mixed" and args.impl == "ours":
+            run_serving_mixed(args)
         elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:

@@ -137,3 +137,32 @@ def test_admission_follows_free_device_memory():
         assert st == alone[i][2] and it == alone[i][1]
         assert np.array_equal(x, alone[i][0], equal_nan=True)
     srv.close()
+
+
+def test_destroyed_request_blocks_are_reused_and_released():
+    """A destroyed request's device block serves the next request of its size
+    without new device memory, a request on a reused block solves to the same
+    state bit for bit, and sdft_release_cached_memory hands the blocks back."""
+    import torch
+
+    d = descriptor(small_slit(np_=4096, dz=0.005, n_chain=6)).descriptor
+    num = numerics_from_dict(dict(small_slit()["numerical"], tole=1e-8, max_iters=200))
+    native.release_cached_memory()
+    a = native.DeviceSystem(d)
+    one = a.device_bytes
+    assert one > 16 * 2 ** 20  # large against the 2 MiB allocation granularity
+    it_a, _, _ = a.solve(num)
+    x_a = a.get_x()
+    a.close()  # its block goes to the cache
+    free1, _ = torch.cuda.mem_get_info()
+    b = native.DeviceSystem(d)  # on that block
+    free2, _ = torch.cuda.mem_get_info()
+    assert free1 - free2 < one // 2
+    it_b, _, _ = b.solve(num)
+    assert it_b == it_a and np.array_equal(b.get_x(), x_a)
+    b.close()
+    released = native.release_cached_memory()
+    assert released >= one
+    free3, _ = torch.cuda.mem_get_info()
+    assert free3 - free2 >= 0.9 * one
+    assert native.release_cached_memory() == 0
