@@ -156,7 +156,7 @@ int sdft_request_resident(sdft_handle h, int32_t* per_device);
  * SDFT_ERR_UNSUPPORTED with the reason in sdft_last_error().  No reference
  * counterpart (FFTW plans any length): the device transform takes np >= 16
  * whose FFT length M (np/2 for even np, np for odd np) fits one CTA's shared
- * memory: mixed radix when M has no prime factor above 61 (M up to 12459),
+ * memory: mixed radix when M has no prime factor above 61 (M up to 12288),
  * else Bluestein's chirp convolution of 2^k >= 2M - 1 points (M up to 4096).
  * Host-only: needs no GPU. */
 int sdft_grid_supported(int32_t np);

@@ -299,6 +299,14 @@ constexpr int kSolveCtasPerSm = SDFT_SOLVE_CTAS;
 constexpr size_t kTransformBudget = kSolveCtasPerSm >= 3 ? 64 * 1024 : 96 * 1024;
 constexpr size_t kMaxSmemBytes = 227 * 1024;   // dynamic shared memory a CTA may opt into
 
+// Padded position of complex index i in a transform buffer: one spare slot
+// after every 8 and after every 64 values.  The strided radix passes then meet
+// no bank conflicts, and the bit-reversed slots that the Makhoul reorder
+// writes and reads spread over the banks (with one spare per 8 alone, the 16
+// slots a warp touches there fall on two bank groups).
+__host__ __device__ constexpr int fpad(int i) { return i + (i >> 3) + (i >> 6); }
+// slots of a transform buffer of n complex values
+__host__ __device__ constexpr int fft_buffer_len(int n) { return n > 0 ? fpad(n - 1) + 1 : 0; }
 // ---- kernel launches ----
 // The kernels are compiled twice (kernels_pow2.cu, kernels_gen.cu): once with
 // the power-of-two FFT passes and once with the general-length ones, so that

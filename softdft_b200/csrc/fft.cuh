@@ -41,8 +41,6 @@
 namespace sdft {
 namespace {  // internal linkage: each kernel build (kernels.cuh) has its own copy
 
-__device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
-
 __device__ __forceinline__ int brev_bits(int m, int L) {
   return L == 0 ? 0 : (int)(__brev((unsigned)m) >> (32 - L));
 }
@@ -74,7 +72,7 @@ __device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
   c.L = r.L;
   c.P = r.NPt;
   c.H = r.M >> 1;
-  c.stride = r.M + (r.M >> 3);
+  c.stride = fft_buffer_len(r.M);
   c.nrad = r.nrad;
   c.rad = r.rad;
   c.slot = r.slot;
@@ -87,7 +85,7 @@ __device__ __forceinline__ FftCtx make_fft(double2* z, const DReq& r) {
   c.bw = r.bw;
   c.bB = r.bB;
   c.btw = r.btw;
-  if (r.blue) c.stride = r.LB + (r.LB >> 3);
+  if (r.blue) c.stride = fft_buffer_len(r.LB);
   return c;
 }
 
@@ -99,7 +97,7 @@ __device__ __forceinline__ FftCtxT<float2> make_fft32(double2* z, const DReq& r)
   c.L = r.L;
   c.P = r.NPt;
   c.H = r.M >> 1;
-  c.stride = r.M + (r.M >> 3);
+  c.stride = fft_buffer_len(r.M);
   c.nrad = r.nrad;
   c.rad = r.rad;
   c.slot = r.slot;
@@ -112,7 +110,7 @@ __device__ __forceinline__ FftCtxT<float2> make_fft32(double2* z, const DReq& r)
   c.bw = r.bw32;
   c.bB = r.bB32;
   c.btw = r.btw32;
-  if (r.blue) c.stride = r.LB + (r.LB >> 3);
+  if (r.blue) c.stride = fft_buffer_len(r.LB);
   return c;
 }
 

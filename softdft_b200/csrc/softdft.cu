@@ -1133,16 +1133,16 @@ extern "C" int sdft_request_sizes(sdft_handle h, int64_t* n_unknowns, int64_t* d
 
 // transform buffers per CTA: up to kMaxTB within kTransformBudget, so that the
 // solve kernel's occupancy target (kSolveCtasPerSm CTAs) fits an SM's shared
-// memory; one buffer of M + M/8 complex values minimum
+// memory; one buffer of fft_buffer_len(M) complex values minimum
 static int tb_for(int M) {
-  const size_t buf = sizeof(double2) * (size_t)(M + M / 8);
+  const size_t buf = sizeof(double2) * (size_t)fft_buffer_len(M);
   size_t tb = kTransformBudget / buf;
   if (tb < 1) tb = 1;
   if (tb > (size_t)kMaxTB) tb = kMaxTB;
   return (int)tb;
 }
 static size_t smem_bytes(int M) {
-  return sizeof(double) * kRedDoubles + sizeof(double2) * (size_t)(M + M / 8) * (size_t)tb_for(M);
+  return sizeof(double) * kRedDoubles + sizeof(double2) * (size_t)fft_buffer_len(M) * (size_t)tb_for(M);
 }
 
 // launches of the kernel build that matches the request (power-of-two or general FFT length)

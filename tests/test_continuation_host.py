@@ -34,7 +34,7 @@ def test_grid_supported_matches_the_device_rule():
     assert not ok(2 * 67 * 64)     # M = 4288 = 67 * 64: Bluestein over 16384 points, beyond one CTA
     assert not ok(4099) and not ok(8198)  # M = 4099 (prime): the same
     assert b"Bluestein transform of 16384 points" in native.lib().sdft_last_error()
-    assert ok(24910) and not ok(32768)  # shared memory of one CTA
+    assert ok(24576) and not ok(24696) and not ok(32768)  # one CTA's shared memory: M = 12288 fits, 12348 does not
 
 
 def test_supported_bin_width_keeps_the_reference_grid():
