@@ -61,7 +61,7 @@ def parse():
                          "iterations each, so that a capture of a later launch sees the Anderson phase")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
-    ap.add_argument("--workload", default="plain", choices=["plain", "uneven", "serving-mixed"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "uneven", "serving-mixed", "continuation"],
                     help="uneven: a seeded batch of slits of different grids and chains in one launch sequence; "
                          "serving-mixed: a Poisson stream of slits of different grids and chain lengths, each "
                          "built on the host at arrival")
@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--uneven-chain", type=str, default="10,60", help="uniform chain-length range")
     ap.add_argument("--uneven-dump", type=str, default="",
                     help="uneven and serving-mixed: write per-request status and iterations (JSON)")
+    ap.add_argument("--cont-steps", type=int, default=4,
+                    help="continuation: wall-separation steps run (of the 400 of the full sweep)")
     ap.add_argument("--serve-requests", type=int, default=1500)
     ap.add_argument("--serve-rate", type=float, default=100.0, help="offered requests/s of the serving stream")
     ap.add_argument("--serve-iters", type=int, default=25, help="Anderson iterations per server launch")
@@ -507,6 +509,46 @@ def run_serving_mixed(args):
     print(json.dumps(out), flush=True)
 
 
+def run_continuation(args):
+    """The batched wall-separation continuation at its specified shape: 64
+    branches of weak-polyacid brushes (N = 100, grafting density 0.05, pKa 4.5,
+    pH U(3, 9) per branch, 10 mM salt) grafted on both walls, swept from
+    H = 40 sigma towards 2 sigma in 400 equal steps on the grid of 8192 points
+    at H = 40 sigma (the spacing kept as H shrinks), every step warm-started
+    from the branch's previous solution and all branches solved in one batch
+    per step.  The first --cont-steps steps are run and timed."""
+    import numpy as np
+
+    from softdft_b200 import native, workloads
+    from softdft_b200.continuation import batched_distance_sweep
+    from softdft_b200.host.descriptor import numerics_from_dict
+    rng = np.random.default_rng(23)
+    dz = 40.0 / 8191.0
+    branches = [workloads.grafted_brush(8192, dz, 100, 0.05, 4.5, float(rng.uniform(3.0, 9.0)), 0.010)
+                for _ in range(64)]
+    nd = dict(branches[0]["numerical"], max_iters=args.max_iters if args.max_iters > 0 else 3000)
+    for b in branches:
+        b["numerical"] = dict(nd)
+    distances = [float(x) for x in np.linspace(40.0, 2.0, 401)[1:]][: args.cont_steps]
+    t0 = time.perf_counter()
+    out = batched_distance_sweep(branches, distances, dz=dz, num=numerics_from_dict(nd))
+    wall = time.perf_counter() - t0
+    steps = []
+    for k in range(len(distances)):
+        rows = [o[k] for o in out]
+        st = np.array([r_["status"] for r_ in rows])
+        it = np.array([r_["iterations"] for r_ in rows])
+        steps.append({"H": distances[k], "device_ms": rows[0]["batch_device_ms"],
+                      "converged": int(np.sum(st == 0)), "iterations": {"min": int(it.min()), "max": int(it.max()),
+                                                                         "mean": float(it.mean())}})
+    dev_s = sum(s_["device_ms"] for s_ in steps) / 1000.0
+    print(json.dumps({"metric": "batched wall-separation continuation: branch-steps/s", "workload": "continuation",
+                      "branches": 64, "steps_run": len(distances), "steps_full_sweep": 400,
+                      "value": 64 * len(distances) / wall, "unit": "branch-steps/s", "wall_s": wall,
+                      "device_s": dev_s, "host_s": wall - dev_s, "per_step": steps, "dtype": "f64",
+                      "data": "synthetic", "n_gpus": 1}), flush=True)
+
+
 def run_uneven(args):
     """Uneven batch: independent slits with NP log-uniform (rounded to powers of
     two), chain length, pH U(2,12), salt log-U(1 mM, 1 M) and packing U(0.1,0.4)
@@ -735,6 +777,8 @@ def main():
             run_uneven(args)
         elif args.workload == "serving-mixed" and args.impl == "ours":
             run_serving_mixed(args)
+        elif args.workload == "continuation" and args.impl == "ours":
+            run_continuation(args)
         elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:
