@@ -620,9 +620,9 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
             for (int u = 0; u < kMaxTB; u++)
               if (u < nb) {
                 const FuseT& d = fd[g0 + u];
-                // the bond-end factors repeat across the two recursions and the
-                // steps of a chain: L1-cached loads
-                const R2 fv = ldca2(reinterpret_cast<const R*>(d.fin) + K);
+                // the bond-end factors (4 MB P values) exceed L1 beside the
+                // twiddles and bond kernels that every pass rereads: L2 only
+                const R2 fv = ldcg2(reinterpret_cast<const R*>(d.fin) + K);
                 f[u] = make_double2((double)fv.x, (double)fv.y);
                 if (d.src) {
                   double2 q2 = make_double2(0.0, 0.0);
@@ -647,7 +647,7 @@ __device__ bool chain_sweeps(const DReq& r, const DSpecies& s, Shared sh) {
             R2 fo[kMaxTB];
 #pragma unroll
             for (int u = 0; u < kMaxTB; u++)
-              if (u < nb) fo[u] = ldca2(reinterpret_cast<const R*>(fd[g0 + u].fout) + K);
+              if (u < nb) fo[u] = ldcg2(reinterpret_cast<const R*>(fd[g0 + u].fout) + K);
             const bool cut = s.fixed >= 0;
 #pragma unroll
             for (int u = 0; u < kMaxTB; u++)
